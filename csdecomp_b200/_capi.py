@@ -1,0 +1,166 @@
+"""ctypes binding of libcsdecomp_b200.so (declared in include/csd_capi.h).
+
+The library is the product: this module raises if it has not been built
+(there is no CPU fallback).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Dict
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcsdecomp_b200.so")
+
+CSD_OK, CSD_ERR_INVALID, CSD_ERR_CAPACITY, CSD_ERR_NOT_CONTAINED, CSD_ERR_CUDA, CSD_ERR_UNSUPPORTED, \
+    CSD_ERR_DIMENSION, CSD_ERR_NO_DEVICE = range(8)
+CSD_PTR_HOST, CSD_PTR_DEVICE = 0, 1
+CSD_EDGE_L2_REF, CSD_EDGE_LINF, CSD_EDGE_VG = 0, 1, 2
+
+_P = ctypes.c_void_p
+
+
+class PlantDesc(ctypes.Structure):
+    _fields_ = [
+        ("num_joints", ctypes.c_int32),
+        ("num_links", ctypes.c_int32),
+        ("num_configuration_variables", ctypes.c_int32),
+        ("num_geometries", ctypes.c_int32),
+        ("num_collision_pairs", ctypes.c_int32),
+        ("joint_type", _P),
+        ("joint_parent_link", _P),
+        ("joint_child_link", _P),
+        ("joint_idx_to_config_idx", _P),
+        ("joint_traversal_sequence", _P),
+        ("joint_X_PL_J", _P),
+        ("joint_axis", _P),
+        ("geom_type", _P),
+        ("geom_link_index", _P),
+        ("geom_group", _P),
+        ("geom_dimensions", _P),
+        ("geom_X_L_B", _P),
+        ("collision_pairs_flat", _P),
+    ]
+
+
+class PlantInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in (
+        "dim", "num_links", "num_fk_joints", "num_moving", "num_static", "num_tile_pairs",
+        "num_generic_pairs", "always_colliding")]
+
+
+class EizoOptionsC(ctypes.Structure):
+    _fields_ = [
+        ("configuration_margin", ctypes.c_float),
+        ("tau", ctypes.c_float),
+        ("delta", ctypes.c_float),
+        ("epsilon", ctypes.c_float),
+        ("bisection_steps", ctypes.c_uint32),
+        ("num_particles", ctypes.c_uint32),
+        ("max_hyperplanes_per_iteration", ctypes.c_uint32),
+        ("max_iterations", ctypes.c_uint32),
+        ("mixing_steps", ctypes.c_uint32),
+        ("seed", ctypes.c_uint64),
+        ("verbose", ctypes.c_int32),
+        ("track_iteration_information", ctypes.c_int32),
+    ]
+
+
+class EizoIterC(ctypes.Structure):
+    _fields_ = [
+        ("iteration_index", ctypes.c_int32),
+        ("num_samples_drawn", ctypes.c_int32),
+        ("collisions_threshold", ctypes.c_int32),
+        ("num_collisions_unadaptive", ctypes.c_int32),
+        ("num_collisions_updated", ctypes.c_int32),
+        ("num_faces_placed", ctypes.c_int32),
+        ("iteration_time_ms", ctypes.c_float),
+    ]
+
+
+# every entry point declared in include/csd_capi.h
+EXPORTS = (
+    "csd_last_error", "csd_version", "csd_plant_create", "csd_plant_destroy", "csd_plant_info", "csd_fk",
+    "csd_check_points", "csd_check_edges", "csd_pair_collision_free", "csd_uniform_sample_hpolyhedra",
+    "csd_inflator_create", "csd_inflator_inflate", "csd_inflator_destroy", "csd_eizo",
+    "csd_num_samples_unadaptive",
+)
+
+_lib = None
+
+
+class CsdError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: the CUDA library has not been built "
+                "(run `python -c 'import __graft_entry__; __graft_entry__.build()'`).")
+        L = ctypes.CDLL(LIB_PATH)
+        L.csd_last_error.restype = ctypes.c_char_p
+        L.csd_num_samples_unadaptive.restype = ctypes.c_uint32
+        L.csd_num_samples_unadaptive.argtypes = [ctypes.c_float] * 3
+        for name in EXPORTS:
+            f = getattr(L, name)
+            if name not in ("csd_last_error", "csd_num_samples_unadaptive"):
+                f.restype = ctypes.c_int32
+        _lib = L
+    return _lib
+
+
+def check(code: int) -> None:
+    if code == CSD_OK:
+        return
+    msg = lib().csd_last_error().decode(errors="replace")
+    if code == CSD_ERR_INVALID:
+        raise ValueError(msg)
+    raise CsdError(code, msg)
+
+
+def ptr(a) -> ctypes.c_void_p:
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return ctypes.c_void_p(a)
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class PlantHandle:
+    """Device-resident plant tables (csd_plant_create / csd_plant_destroy)."""
+
+    def __init__(self, arrays: Dict[str, np.ndarray], num_joints: int, num_links: int, dim: int,
+                 num_geoms: int, num_pairs: int):
+        self._arrays = arrays
+        d = PlantDesc(num_joints, num_links, dim, num_geoms, num_pairs,
+                      *[ptr(arrays[k]) for k in (
+                          "joint_type", "joint_parent_link", "joint_child_link", "joint_idx_to_config_idx",
+                          "joint_traversal_sequence", "joint_X_PL_J", "joint_axis", "geom_type",
+                          "geom_link_index", "geom_group", "geom_dimensions", "geom_X_L_B",
+                          "collision_pairs_flat")])
+        h = ctypes.c_void_p()
+        check(lib().csd_plant_create(ctypes.byref(d), ctypes.byref(h)))
+        self.handle = h
+        self.dim = dim
+        self.num_links = num_links
+
+    def info(self) -> dict:
+        i = PlantInfo()
+        check(lib().csd_plant_info(self.handle, ctypes.byref(i)))
+        return {k: getattr(i, k) for k, _ in PlantInfo._fields_}
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h and _lib is not None:
+            try:
+                _lib.csd_plant_destroy(h)
+            except Exception:  # pragma: no cover - interpreter shutdown
+                pass
+        self.handle = None

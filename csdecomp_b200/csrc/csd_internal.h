@@ -1,0 +1,101 @@
+// csd_internal.h -- host-side handle types, error plumbing and device buffers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/csd_capi.h"
+#include "csd_device.cuh"
+
+namespace csd {
+
+void set_error(const std::string& msg);
+
+struct Status {
+  csd_status_t code;
+  std::string msg;
+};
+
+#define CSD_CUDA_TRY(expr)                                                               \
+  do {                                                                                   \
+    cudaError_t _e = (expr);                                                             \
+    if (_e != cudaSuccess) {                                                             \
+      ::csd::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e));              \
+      return CSD_ERR_CUDA;                                                               \
+    }                                                                                    \
+  } while (0)
+
+#define CSD_CHECK(cond, code, msg)   \
+  do {                               \
+    if (!(cond)) {                   \
+      ::csd::set_error(msg);         \
+      return (code);                 \
+    }                                \
+  } while (0)
+
+// Grow-only device buffer (no allocation once warm).
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  csd_status_t reserve(size_t n);
+  ~DevBuf();
+  template <typename T>
+  T* as() const { return reinterpret_cast<T*>(ptr); }
+};
+
+struct HostPlant {  // host copies kept for host-side checks and voxel tables
+  int dim = 0;
+  int num_links = 0;
+  std::vector<int> moving_of_geom;  // geometry -> moving index or -1
+  std::vector<int> static_of_geom;  // geometry -> static index or -1
+  std::vector<int> geom_type;
+  std::vector<MovingGeom> moving;
+  std::vector<float> statics;       // [S][16]
+  std::vector<int> static_type;
+  int num_tile_pairs = 0;
+};
+
+}  // namespace csd
+
+struct csd_plant_s {
+  int device = 0;
+  csd::DevPlant dp{};
+  csd::HostPlant host;
+  void* blob = nullptr;  // device tables
+  // scratch for host-pointer calls and per-call voxel tables
+  csd::DevBuf in_buf, in_buf2, out_buf, out_buf2, vox_buf, vox_tab, counter;
+  ~csd_plant_s();
+};
+
+namespace csd {
+
+// Per-call voxel tables derived from robot geometry ids.
+struct VoxelTables {
+  const float* vox = nullptr;     // [V][3] device
+  int nv = 0;
+  float vr = 0.f;
+  const uint32_t* tile_mask = nullptr;  // [num_tiles] lanes of each sphere tile checked against voxels
+  const uint32_t* other = nullptr;      // geometry refs (bit31 = static) checked lane-over-voxels
+  int num_other = 0;
+};
+
+csd_status_t build_voxel_tables(csd_plant_s* p, const int32_t* robot_ids, int nr, std::vector<uint32_t>* tab,
+                                int* num_other);
+
+// kernels (check.cu)
+csd_status_t launch_check_points(const csd_plant_s* p, const float* q, int64_t n, const VoxelTables& vt,
+                                 uint8_t* out, cudaStream_t st);
+csd_status_t launch_fk(const csd_plant_s* p, const float* q, int64_t n, float* tf, cudaStream_t st);
+csd_status_t launch_check_edges(const csd_plant_s* p, const float* s, const float* e, int64_t n, float step,
+                                int mode, uint8_t* out, int64_t* pts, unsigned int* counter, cudaStream_t st);
+// sampler.cu
+csd_status_t launch_hit_and_run(const float* A, const float* b, const int32_t* face_off, int num_poly, int dim,
+                                const float* starts, int samples_per_poly, int mixing, uint64_t seed,
+                                uint32_t stream_base, int fail_keep, float* out, int* num_failed,
+                                const int* num_faces_dev, cudaStream_t st);
+
+int device_sm_count();
+
+}  // namespace csd

@@ -1,0 +1,521 @@
+// eizo.cu -- EI-ZO edge inflation on the device.
+//
+// Reference: executeEizo (csdecomp/src/planning/cuda_edge_inflation_zero_order.cu:94-339)
+// drives each iteration from the host with ~12 + 3*faces launches and
+// blocking copies: sample, FK, pair check, pool, atomicAdd compaction (D2H),
+// first-M count (D2H), projection, 9 x (midpoint, FK, check, pool, bounds,
+// store), distances, then per face a thrust::min_element, a <<<1,1>>>
+// maybePlaceFace with two memcpys and a redundancy kernel.
+//
+// Here an iteration is five launches and one 16-byte device-to-host read:
+//   1. hit_and_run_kernel           M_k chains in the current region
+//   2. check_points_kernel          fused FK + pair sweep, one verdict byte each
+//   3. compact_kernel               one block: ordered prefix scan of the
+//                                    colliding samples (the reference's atomicAdd
+//                                    slot order is scheduling dependent,
+//                                    cuda_set_builder_utils.cu:168-186) and the
+//                                    first-M collision count
+//   -- host reads the counts, applies the admissibility test --
+//   4. bisect_kernel                projection onto the segment and all
+//                                    bisection steps, each step a fused FK +
+//                                    check of the 32 midpoints a warp owns
+//   5. faces_kernel                 one block: greedy argmin (first index on
+//                                    ties, as thrust::min_element), face
+//                                    placement with the segment relaxation
+//                                    (cuda_set_builder_utils.cu:359-401) and
+//                                    redundancy marking (:402-424), all faces
+//                                    of the iteration in one launch.
+#include <algorithm>
+#include <cfloat>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "check_core.cuh"
+
+namespace csd {
+
+struct EizoCounters {
+  uint32_t total;     // colliding samples
+  uint32_t first_m;   // colliding samples among the first M
+  uint32_t placed;    // faces placed by the last faces_kernel
+  int32_t status;     // 0 ok, 2 face capacity exceeded
+};
+
+__global__ void compact_kernel(const uint8_t* __restrict__ flags, const float* __restrict__ samples, int N, int M,
+                               int max_keep, int dim, float* __restrict__ cols, EizoCounters* cnt) {
+  __shared__ uint32_t warp_sums[32];
+  __shared__ uint32_t running;
+  __shared__ uint32_t first_m;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  if (tid == 0) {
+    running = 0;
+    first_m = 0;
+  }
+  __syncthreads();
+  for (int base = 0; base < N; base += blockDim.x) {
+    int i = base + tid;
+    uint32_t f = (i < N && !flags[i]) ? 1u : 0u;
+    uint32_t ballot = __ballot_sync(0xffffffffu, f);
+    uint32_t pre = __popc(ballot & ((1u << lane) - 1u));
+    uint32_t fm = __popc(__ballot_sync(0xffffffffu, f && i < M));
+    if (lane == 0) warp_sums[warp] = __popc(ballot);
+    if (lane == 0 && fm) atomicAdd(&first_m, fm);
+    __syncthreads();
+    uint32_t off = 0;
+    for (int w = 0; w < warp; ++w) off += warp_sums[w];
+    uint32_t pos = running + off + pre;
+    if (f && pos < (uint32_t)max_keep)
+      for (int k = 0; k < dim; ++k) cols[(size_t)pos * dim + k] = samples[(size_t)i * dim + k];
+    __syncthreads();
+    if (tid == 0) {
+      uint32_t tot = 0;
+      for (int w = 0; w < nw; ++w) tot += warp_sums[w];
+      running += tot;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    cnt->total = running;
+    cnt->first_m = first_m;
+  }
+}
+
+
+__global__ void __launch_bounds__(128) bisect_kernel(DevPlant p, int K, int dim, int steps,
+                                                     const float* __restrict__ ls, const float* __restrict__ le,
+                                                     VoxArgs va, float* __restrict__ cols, float* __restrict__ proj,
+                                                     float* __restrict__ dist) {
+  extern __shared__ float4 smem4[];
+  float* smem = reinterpret_cast<float*>(smem4);
+  const int wpb = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* tf = smem + warp * per_warp_floats(p);
+  float* qbuf = warp_qbuf(p, tf);
+  float* pose = warp_pose(p, tf);
+  const int nbatch = (K + 31) / 32;
+  for (int b = blockIdx.x * wpb + warp; b < nbatch; b += gridDim.x * wpb) {
+    const int i = b * 32 + lane;
+    const int cnt = min(32, K - b * 32);
+    const bool valid = lane < cnt;
+    float c[kMaxDim], pr[kMaxDim], lo[kMaxDim], hi[kMaxDim];
+    if (valid) {
+      float seg2 = 0.f, a = 0.f;
+      for (int k = 0; k < dim; ++k) {
+        float dk = __fsub_rn(le[k], ls[k]);
+        c[k] = cols[(size_t)i * dim + k];
+        seg2 = __fmaf_rn(dk, dk, seg2);
+        a = __fmaf_rn(__fsub_rn(c[k], ls[k]), dk, a);
+      }
+      float t = fminf(fmaxf(__fdiv_rn(a, seg2), 0.0f), 1.0f);
+      float omt = __fsub_rn(1.0f, t);
+      for (int k = 0; k < dim; ++k) {
+        pr[k] = __fmaf_rn(t, le[k], __fmul_rn(omt, ls[k]));
+        lo[k] = pr[k];
+        hi[k] = c[k];
+      }
+    }
+    for (int s = 0; s < steps; ++s) {
+      float mid[kMaxDim];
+      if (valid) {
+        for (int k = 0; k < dim; ++k) {
+          mid[k] = __fmul_rn(0.5f, __fadd_rn(lo[k], hi[k]));
+          qbuf[k * kRow + lane] = mid[k];
+        }
+        fk_lane(p, qbuf, tf, lane);
+      }
+      __syncwarp();
+      bool mine = false;
+      for (int cc = 0; cc < cnt; ++cc) {
+        bool h = check_config(p, tf, pose, cc, lane, va);
+        if (lane == cc) mine = h;
+      }
+      if (valid) {
+        for (int k = 0; k < dim; ++k) {
+          if (mine) {
+            hi[k] = mid[k];
+            c[k] = mid[k];
+          } else {
+            lo[k] = mid[k];
+          }
+        }
+      }
+      __syncwarp();
+    }
+    if (valid) {
+      float s2 = 0.f;
+      for (int k = 0; k < dim; ++k) {
+        float x = __fsub_rn(c[k], pr[k]);
+        s2 = __fmaf_rn(x, x, s2);
+        cols[(size_t)i * dim + k] = c[k];
+        proj[(size_t)i * dim + k] = pr[k];
+      }
+      dist[i] = __fsqrt_rn(s2);
+    }
+  }
+}
+
+// One block places up to max_faces faces (greedy, nearest collision first).
+__global__ void __launch_bounds__(1024) faces_kernel(int K, int dim, int max_faces, int capacity, float margin,
+                                                     const float* __restrict__ ls, const float* __restrict__ le,
+                                                     const float* __restrict__ cols, const float* __restrict__ proj,
+                                                     float* __restrict__ dist, float* __restrict__ A,
+                                                     float* __restrict__ b, int* __restrict__ num_faces,
+                                                     EizoCounters* cnt) {
+  __shared__ float red_v[32];
+  __shared__ int red_i[32];
+  __shared__ float face[kMaxDim + 1];
+  __shared__ int best_s;
+  __shared__ float best_v;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  int nf = *num_faces;
+  int placed = 0;
+  int status = 0;
+  for (; placed < max_faces; ++placed) {
+    float bv = FLT_MAX;
+    int bi = 0x7fffffff;
+    for (int i = tid; i < K; i += blockDim.x) {
+      float v = dist[i];
+      if (v < bv || (v == bv && i < bi)) {
+        bv = v;
+        bi = i;
+      }
+    }
+    for (int o = 16; o; o >>= 1) {
+      float ov = __shfl_down_sync(0xffffffffu, bv, o);
+      int oi = __shfl_down_sync(0xffffffffu, bi, o);
+      if (ov < bv || (ov == bv && oi < bi)) {
+        bv = ov;
+        bi = oi;
+      }
+    }
+    if (lane == 0) {
+      red_v[warp] = bv;
+      red_i[warp] = bi;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      float v = FLT_MAX;
+      int ix = 0x7fffffff;
+      for (int w = 0; w < nw; ++w)
+        if (red_v[w] < v || (red_v[w] == v && red_i[w] < ix)) {
+          v = red_v[w];
+          ix = red_i[w];
+        }
+      best_v = v;
+      best_s = ix;
+    }
+    __syncthreads();
+    if (!(best_v < FLT_MAX)) break;
+    if (nf >= capacity) {
+      status = 2;
+      break;
+    }
+    if (tid == 0) {
+      const int s = best_s;
+      const float* c = cols + (size_t)s * dim;
+      const float* pr = proj + (size_t)s * dim;
+      float a[kMaxDim];
+      float n2 = 0.f;
+      for (int k = 0; k < dim; ++k) {
+        a[k] = __fsub_rn(c[k], pr[k]);
+        n2 = __fmaf_rn(a[k], a[k], n2);
+      }
+      float nrm = __fsqrt_rn(n2);
+      for (int k = 0; k < dim; ++k) a[k] = __fdiv_rn(a[k], nrm);
+      float bb = 0.f, v1 = 0.f, v2 = 0.f;
+      for (int k = 0; k < dim; ++k) {
+        bb = __fmaf_rn(a[k], c[k], bb);
+        v1 = __fmaf_rn(a[k], ls[k], v1);
+        v2 = __fmaf_rn(a[k], le[k], v2);
+      }
+      bb = __fsub_rn(bb, margin);
+      v1 = __fsub_rn(v1, bb);
+      v2 = __fsub_rn(v2, bb);
+      float relax = v2 > v1 ? v2 : v1;
+      relax = relax > 0 ? relax : 0;
+      bb = __fadd_rn(bb, relax);
+      for (int k = 0; k < dim; ++k) {
+        A[(size_t)nf * dim + k] = a[k];
+        face[k] = a[k];
+      }
+      b[nf] = bb;
+      face[dim] = bb;
+      dist[s] = FLT_MAX;
+    }
+    __syncthreads();
+    const float bb = face[dim];
+    for (int i = tid; i < K; i += blockDim.x) {
+      if (dist[i] == FLT_MAX) continue;
+      float v = 0.f;
+      for (int k = 0; k < dim; ++k) v = __fmaf_rn(face[k], cols[(size_t)i * dim + k], v);
+      if (__fsub_rn(v, bb) > 0.f) dist[i] = FLT_MAX;
+    }
+    ++nf;
+    __syncthreads();
+  }
+  if (tid == 0) {
+    *num_faces = nf;
+    cnt->placed = (uint32_t)placed;
+    cnt->status = status;
+  }
+}
+
+}  // namespace csd
+
+// ------------------------------------------------------------------- handle
+struct csd_inflator_s {
+  csd_plant_s* plant = nullptr;
+  int device = 0;
+  int dim = 0;
+  csd_eizo_options_t opt{};
+  int domain_faces = 0;
+  int capacity = 0;
+  int max_voxels = 0;
+  int max_configs = 0;
+  std::vector<float> domain_A, domain_b;
+  std::vector<uint32_t> vtab_host;
+  int num_other = 0;
+  csd::DevBuf A, b, nf, samples, flags, cols, proj, dist, seg, vox, vtab, cnt;
+  csd::EizoCounters* host_cnt = nullptr;  // pinned
+  int* host_nf = nullptr;                 // pinned
+  ~csd_inflator_s() {
+    if (host_cnt) cudaFreeHost(host_cnt);
+    if (host_nf) cudaFreeHost(host_nf);
+  }
+};
+
+namespace csd {
+
+static bool point_in_set(const std::vector<float>& A, const std::vector<float>& b, int F, int d, const float* x) {
+  for (int f = 0; f < F; ++f) {
+    float ax = 0.f;
+    for (int k = 0; k < d; ++k) ax += A[(size_t)f * d + k] * x[k];
+    if (!(ax <= b[f] + 1e-9f)) return false;
+  }
+  return true;
+}
+
+static csd_status_t launch_bisect(const csd_plant_s* p, int K, int dim, int steps, const float* ls, const float* le,
+                                  const VoxArgs& va, float* cols, float* proj, float* dist, cudaStream_t st) {
+  if (K <= 0) return CSD_OK;
+  const int wpb = 4;
+  size_t smem = smem_bytes(p, wpb);
+  int grid = 0;
+  csd_status_t s = grid_for(bisect_kernel, smem, (K + 31) / 32, &grid, wpb);
+  if (s) return s;
+  bisect_kernel<<<grid, 32 * wpb, smem, st>>>(p->dp, K, dim, steps, ls, le, va, cols, proj, dist);
+  CSD_CUDA_TRY(cudaGetLastError());
+  return CSD_OK;
+}
+
+}  // namespace csd
+
+using namespace csd;
+
+extern "C" {
+
+csd_status_t csd_inflator_create(csd_plant_t plant, const int32_t* ids, int32_t nr, const csd_eizo_options_t* o,
+                                 const float* dA, const float* db, int32_t F0, int32_t max_voxels, int32_t capacity,
+                                 csd_inflator_t* out) {
+  CSD_CHECK(plant && o && out && (F0 == 0 || (dA && db)) && (nr == 0 || ids), CSD_ERR_INVALID, "null argument");
+  CSD_CHECK(F0 >= 0 && nr >= 0 && max_voxels >= 0, CSD_ERR_INVALID, "negative size");
+  *out = nullptr;
+  const int d = plant->dp.dim;
+  CSD_CHECK(d >= 1 && d <= kMaxDim, CSD_ERR_DIMENSION, "plant dimension must be in [1, 16]");
+  CSD_CHECK(capacity >= F0 && capacity > 0, CSD_ERR_CAPACITY, "face capacity smaller than the domain");
+  CSD_CHECK(o->num_particles >= 1 && o->max_iterations >= 1, CSD_ERR_INVALID, "num_particles and max_iterations must be positive");
+  CSD_CHECK(o->tau > 0.f && o->tau < 1.f && o->epsilon > 0.f && o->delta > 0.f, CSD_ERR_INVALID, "bad epsilon/delta/tau");
+  // EizoGpuMemory sizing, cuda_edge_inflation_zero_order.cu:448-494
+  double delta_min = 6 * o->delta / (M_PI * M_PI * (double)o->max_iterations * (double)o->max_iterations);
+  uint32_t mmax = csd_num_samples_unadaptive(o->epsilon, (float)delta_min, o->tau);
+  if (o->num_particles > mmax) {
+    set_error("Current required particle count exceeds buffer size. There were " + std::to_string(o->num_particles) +
+              " num_particles requested, and " + std::to_string(mmax) +
+              " max_num_configurations space provided by the unadaptive test.");
+    return CSD_ERR_CAPACITY;
+  }
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != plant->device) cudaSetDevice(plant->device);
+  std::unique_ptr<csd_inflator_s> h(new csd_inflator_s());
+  h->plant = plant;
+  h->device = plant->device;
+  h->dim = d;
+  h->opt = *o;
+  h->domain_faces = F0;
+  h->capacity = capacity;
+  h->max_voxels = max_voxels;
+  h->max_configs = (int)std::max<uint32_t>(mmax, o->num_particles);
+  h->domain_A.assign(dA, dA + (size_t)F0 * d);
+  h->domain_b.assign(db, db + F0);
+  csd_status_t s;
+  if ((s = build_voxel_tables(plant, ids, nr, &h->vtab_host, &h->num_other))) return s;
+  const size_t np = o->num_particles, mc = (size_t)h->max_configs;
+  if ((s = h->A.reserve((size_t)capacity * d * 4)) || (s = h->b.reserve((size_t)capacity * 4)) ||
+      (s = h->nf.reserve(16)) || (s = h->samples.reserve(mc * d * 4)) || (s = h->flags.reserve(mc + 16)) ||
+      (s = h->cols.reserve(np * d * 4)) || (s = h->proj.reserve(np * d * 4)) || (s = h->dist.reserve(np * 4)) ||
+      (s = h->seg.reserve(2 * d * 4)) || (s = h->vox.reserve((size_t)std::max(1, max_voxels) * 12)) ||
+      (s = h->vtab.reserve((h->vtab_host.size() + 1) * 4)) || (s = h->cnt.reserve(sizeof(EizoCounters))))
+    return s;
+  if (F0) {
+    CSD_CUDA_TRY(cudaMemcpy(h->A.ptr, dA, (size_t)F0 * d * 4, cudaMemcpyHostToDevice));
+    CSD_CUDA_TRY(cudaMemcpy(h->b.ptr, db, (size_t)F0 * 4, cudaMemcpyHostToDevice));
+  }
+  if (!h->vtab_host.empty())
+    CSD_CUDA_TRY(cudaMemcpy(h->vtab.ptr, h->vtab_host.data(), h->vtab_host.size() * 4, cudaMemcpyHostToDevice));
+  CSD_CUDA_TRY(cudaMallocHost((void**)&h->host_cnt, sizeof(EizoCounters)));
+  CSD_CUDA_TRY(cudaMallocHost((void**)&h->host_nf, sizeof(int) * 4));
+  if (cur != plant->device) cudaSetDevice(cur);
+  *out = h.release();
+  return CSD_OK;
+}
+
+csd_status_t csd_inflator_destroy(csd_inflator_t h) {
+  if (!h) return CSD_OK;
+  int cur = 0, dev = h->device;
+  cudaGetDevice(&cur);
+  if (cur != dev) cudaSetDevice(dev);
+  delete h;
+  if (cur != dev) cudaSetDevice(cur);
+  return CSD_OK;
+}
+
+csd_status_t csd_inflator_inflate(csd_inflator_t h, const float* ls, const float* le, const float* voxels, int32_t nv,
+                                  float vr, float* A_out, float* b_out, int32_t* num_faces,
+                                  csd_eizo_iteration_info_t* info, int32_t info_cap, int32_t* num_iters, void* stream) {
+  CSD_CHECK(h && ls && le && A_out && b_out && num_faces, CSD_ERR_INVALID, "null argument");
+  CSD_CHECK(nv >= 0 && (nv == 0 || voxels), CSD_ERR_INVALID, "null voxels");
+  CSD_CHECK(nv <= h->max_voxels, CSD_ERR_CAPACITY, "more voxels than the inflator was created for");
+  const int d = h->dim;
+  CSD_CHECK(point_in_set(h->domain_A, h->domain_b, h->domain_faces, d, ls) &&
+                point_in_set(h->domain_A, h->domain_b, h->domain_faces, d, le),
+            CSD_ERR_NOT_CONTAINED, "line segment endpoints must lie in the domain");
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != h->device) cudaSetDevice(h->device);
+  struct Restore {
+    int cur, dev;
+    ~Restore() {
+      if (cur != dev) cudaSetDevice(cur);
+    }
+  } restore{cur, h->device};
+  cudaStream_t st = (cudaStream_t)stream;
+  const csd_eizo_options_t& o = h->opt;
+  csd_plant_s* p = h->plant;
+  // reset the region to the domain and upload the segment and voxels
+  h->host_nf[0] = h->domain_faces;
+  CSD_CUDA_TRY(cudaMemcpyAsync(h->nf.ptr, h->host_nf, sizeof(int), cudaMemcpyHostToDevice, st));
+  std::vector<float> seg(2 * d);
+  std::memcpy(seg.data(), ls, d * 4);
+  std::memcpy(seg.data() + d, le, d * 4);
+  CSD_CUDA_TRY(cudaMemcpyAsync(h->seg.ptr, seg.data(), 2 * d * 4, cudaMemcpyHostToDevice, st));
+  if (nv) CSD_CUDA_TRY(cudaMemcpyAsync(h->vox.ptr, voxels, (size_t)nv * 12, cudaMemcpyHostToDevice, st));
+  const float* ls_d = h->seg.as<float>();
+  const float* le_d = ls_d + d;
+  VoxelTables vt;
+  if (nv > 0 && !h->vtab_host.empty()) {
+    vt.vox = h->vox.as<float>();
+    vt.nv = nv;
+    vt.vr = vr;
+    vt.tile_mask = h->vtab.as<uint32_t>();
+    vt.other = h->vtab.as<uint32_t>() + p->dp.num_tiles;
+    vt.num_other = h->num_other;
+  }
+  VoxArgs va{vt.vox, vt.nv, vt.vr, vt.tile_mask, vt.other, vt.num_other};
+  EizoCounters* cnt = h->cnt.as<EizoCounters>();
+  csd_status_t s;
+  int nit = 0;
+  int last_with_faces = -1;
+  auto t_prev = std::chrono::high_resolution_clock::now();
+  for (uint32_t it = 0; it < o.max_iterations; ++it) {
+    auto t0 = std::chrono::high_resolution_clock::now();
+    float delta_k = (float)(6 * o.delta / (M_PI * M_PI * (it + 1) * (it + 1)));
+    uint32_t M = csd_num_samples_unadaptive(o.epsilon, delta_k, o.tau);
+    uint32_t N = std::max(M, o.num_particles);
+    if ((s = launch_hit_and_run(h->A.as<float>(), h->b.as<float>(), nullptr, 1, d, ls_d, (int)N, (int)o.mixing_steps,
+                                o.seed, 0u, 1, h->samples.as<float>(), nullptr, h->nf.as<int>(), st)))
+      return s;
+    if ((s = launch_check_points(p, h->samples.as<float>(), N, vt, h->flags.as<uint8_t>(), st))) return s;
+    compact_kernel<<<1, 1024, 0, st>>>(h->flags.as<uint8_t>(), h->samples.as<float>(), (int)N, (int)M,
+                                       (int)o.num_particles, d, h->cols.as<float>(), cnt);
+    CSD_CUDA_TRY(cudaGetLastError());
+    CSD_CUDA_TRY(cudaMemcpyAsync(h->host_cnt, cnt, sizeof(EizoCounters), cudaMemcpyDeviceToHost, st));
+    CSD_CUDA_TRY(cudaStreamSynchronize(st));
+    if (last_with_faces >= 0) {
+      if (info && last_with_faces < info_cap) info[last_with_faces].num_faces_placed = (int32_t)h->host_cnt->placed;
+      if (h->host_cnt->status == 2) {
+        set_error("Max face count exceeded.");
+        return CSD_ERR_CAPACITY;
+      }
+      last_with_faces = -1;
+    }
+    const uint32_t total = h->host_cnt->total, first_m = h->host_cnt->first_m;
+    const float thr = (1 - o.tau) * o.epsilon * M;
+    csd_eizo_iteration_info_t rec{};
+    rec.iteration_index = (int32_t)it;
+    rec.num_samples_drawn = (int32_t)N;
+    rec.collisions_threshold = (int32_t)thr;
+    rec.num_collisions_unadaptive = (int32_t)first_m;
+    if (o.verbose)
+      printf("iter %u, num collisions found in first M samples %u, thresh %f\n", it, first_m, (double)thr);
+    if ((float)first_m <= thr) {
+      auto t1 = std::chrono::high_resolution_clock::now();
+      rec.iteration_time_ms = std::chrono::duration<float, std::milli>(t1 - t0).count();
+      if (info && nit < info_cap) info[nit] = rec;
+      ++nit;
+      break;
+    }
+    const uint32_t K = std::min(total, o.num_particles);
+    if ((s = launch_bisect(p, (int)K, d, (int)o.bisection_steps, ls_d, le_d, va, h->cols.as<float>(),
+                           h->proj.as<float>(), h->dist.as<float>(), st)))
+      return s;
+    faces_kernel<<<1, 1024, 0, st>>>((int)K, d, (int)o.max_hyperplanes_per_iteration, h->capacity,
+                                     o.configuration_margin, ls_d, le_d, h->cols.as<float>(), h->proj.as<float>(),
+                                     h->dist.as<float>(), h->A.as<float>(), h->b.as<float>(), h->nf.as<int>(), cnt);
+    CSD_CUDA_TRY(cudaGetLastError());
+    rec.num_collisions_updated = (int32_t)K;
+    auto t1 = std::chrono::high_resolution_clock::now();
+    rec.iteration_time_ms = std::chrono::duration<float, std::milli>(t1 - t0).count();
+    if (info && nit < info_cap) info[nit] = rec;
+    last_with_faces = nit;
+    ++nit;
+    (void)t_prev;
+  }
+  CSD_CUDA_TRY(cudaMemcpyAsync(h->host_cnt, cnt, sizeof(EizoCounters), cudaMemcpyDeviceToHost, st));
+  CSD_CUDA_TRY(cudaMemcpyAsync(h->host_nf, h->nf.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CSD_CUDA_TRY(cudaStreamSynchronize(st));
+  if (last_with_faces >= 0) {
+    if (info && last_with_faces < info_cap) info[last_with_faces].num_faces_placed = (int32_t)h->host_cnt->placed;
+    if (h->host_cnt->status == 2) {
+      set_error("Max face count exceeded.");
+      return CSD_ERR_CAPACITY;
+    }
+  }
+  const int F = h->host_nf[0];
+  CSD_CUDA_TRY(cudaMemcpyAsync(A_out, h->A.ptr, (size_t)F * d * 4, cudaMemcpyDeviceToHost, st));
+  CSD_CUDA_TRY(cudaMemcpyAsync(b_out, h->b.ptr, (size_t)F * 4, cudaMemcpyDeviceToHost, st));
+  CSD_CUDA_TRY(cudaStreamSynchronize(st));
+  *num_faces = F;
+  if (num_iters) *num_iters = nit;
+  return CSD_OK;
+}
+
+csd_status_t csd_eizo(csd_plant_t plant, const float* ls, const float* le, const float* voxels, int32_t nv, float vr,
+                      const float* dA, const float* db, int32_t F0, const int32_t* ids, int32_t nr,
+                      const csd_eizo_options_t* o, int32_t capacity, float* A_out, float* b_out, int32_t* num_faces,
+                      csd_eizo_iteration_info_t* info, int32_t info_cap, int32_t* num_iters) {
+  CSD_CHECK(plant && o, CSD_ERR_INVALID, "null argument");
+  // EizoCuda argument checks, cuda_edge_inflation_zero_order.cu:355-386
+  CSD_CHECK(F0 <= 0.9 * capacity, CSD_ERR_CAPACITY,
+            "The domain polyhedron is already reserving almost all of the allocated faces.");
+  csd_inflator_t h = nullptr;
+  csd_status_t s = csd_inflator_create(plant, ids, nr, o, dA, db, F0, nv, capacity, &h);
+  if (s) return s;
+  s = csd_inflator_inflate(h, ls, le, voxels, nv, vr, A_out, b_out, num_faces, info, info_cap, num_iters, nullptr);
+  csd_inflator_destroy(h);
+  return s;
+}
+
+}  // extern "C"

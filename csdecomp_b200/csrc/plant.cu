@@ -1,0 +1,519 @@
+// plant.cu -- host preprocessing of a MinimalPlant into the device layout of
+// csd_device.cuh, and the plant handle's lifetime.
+//
+// Reference: the MinimalPlant is copied whole to the GPU on every call
+// (csdecomp/src/plant/cuda_collision_checker.cu:458-462) and FK walks every
+// joint, fixed ones included (cuda_forward_kinematics.cu:14-57). Here the
+// tree is flattened once: fixed-joint chains are pre-composed in FP64,
+// world-fixed geometry is posed once, and the pair list is split into
+// moving-sphere x static tiles (lane masks) and a generic remainder.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+
+#include "csd_internal.h"
+
+namespace csd {
+
+static thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+
+csd_status_t DevBuf::reserve(size_t n) {
+  if (n <= bytes && ptr) return CSD_OK;
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+  size_t nb = std::max<size_t>(n, 256);
+  CSD_CUDA_TRY(cudaMalloc(&ptr, nb));
+  bytes = nb;
+  return CSD_OK;
+}
+
+DevBuf::~DevBuf() {
+  if (ptr) cudaFree(ptr);
+}
+
+int device_sm_count() {
+  static std::mutex mu;
+  static int cache[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 0 || dev >= 64) return 148;
+  if (!cache[dev]) {
+    int n = 0;
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    cache[dev] = n > 0 ? n : 148;
+  }
+  return cache[dev];
+}
+
+namespace {
+
+struct X4 {  // rigid transform in FP64: R column-major, t
+  double R[9];
+  double t[3];
+};
+
+X4 ident() {
+  X4 x{};
+  x.R[0] = x.R[4] = x.R[8] = 1.0;
+  return x;
+}
+
+X4 from_colmajor(const float* m) {
+  X4 x;
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) x.R[c * 3 + r] = m[c * 4 + r];
+  for (int r = 0; r < 3; ++r) x.t[r] = m[12 + r];
+  return x;
+}
+
+X4 mul(const X4& a, const X4& b) {
+  X4 o;
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += a.R[k * 3 + r] * b.R[c * 3 + k];
+      o.R[c * 3 + r] = s;
+    }
+  for (int r = 0; r < 3; ++r) {
+    double s = a.t[r];
+    for (int k = 0; k < 3; ++k) s += a.R[k * 3 + r] * b.t[k];
+    o.t[r] = s;
+  }
+  return o;
+}
+
+// World-format (16 floats) pose of a geometry from its FP64 world transform.
+void world_pose(int type, const float* dims, const X4& X, float* out) {
+  for (int i = 0; i < 16; ++i) out[i] = 0.f;
+  if (type == G_SPHERE) {
+    for (int r = 0; r < 3; ++r) out[r] = (float)X.t[r];
+    out[3] = dims[0];
+  } else if (type == G_CAPSULE) {
+    for (int r = 0; r < 3; ++r) {
+      out[r] = (float)X.t[r];
+      out[4 + r] = (float)X.R[6 + r];
+    }
+    out[3] = dims[0];
+    out[7] = 0.5f * dims[1];
+  } else {
+    for (int a = 0; a < 3; ++a) {
+      double q = 0;
+      for (int r = 0; r < 3; ++r) {
+        out[4 * a + r] = (float)X.R[a * 3 + r];
+        q += X.R[a * 3 + r] * X.t[r];
+      }
+      out[4 * a + 3] = (float)(-q);
+      out[12 + a] = 0.5f * dims[a];
+    }
+  }
+}
+
+// FP64 collision test of two world-fixed geometries (evaluated once).
+struct DGeom {
+  int type;
+  double c[3], ax[3][3], h[3], r, hl;
+};
+
+DGeom dgeom(int type, const float* dims, const X4& X) {
+  DGeom g{};
+  g.type = type;
+  for (int r = 0; r < 3; ++r) g.c[r] = X.t[r];
+  for (int a = 0; a < 3; ++a)
+    for (int r = 0; r < 3; ++r) g.ax[a][r] = X.R[a * 3 + r];
+  g.r = dims[0];
+  g.hl = 0.5 * dims[1];
+  for (int a = 0; a < 3; ++a) g.h[a] = 0.5 * dims[a];
+  return g;
+}
+
+double dot(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+double point_box_d2(const double* p, const DGeom& B) {
+  double d[3] = {p[0] - B.c[0], p[1] - B.c[1], p[2] - B.c[2]};
+  double s = 0;
+  for (int a = 0; a < 3; ++a) {
+    double e = std::max(std::fabs(dot(B.ax[a], d)) - B.h[a], 0.0);
+    s += e * e;
+  }
+  return s;
+}
+
+double point_seg_d2(const double* p, const DGeom& C) {
+  double d[3] = {p[0] - C.c[0], p[1] - C.c[1], p[2] - C.c[2]};
+  double t = std::max(-C.hl, std::min(dot(d, C.ax[2]), C.hl));
+  double e[3] = {d[0] - t * C.ax[2][0], d[1] - t * C.ax[2][1], d[2] - t * C.ax[2][2]};
+  return dot(e, e);
+}
+
+// distance^2 from a capsule segment to a geometry by dense sampling refined
+// with a golden-section search (convex in t); exact enough for a one-off test.
+double seg_to_d2(const DGeom& C, const DGeom& O) {
+  auto f = [&](double t) {
+    double p[3] = {C.c[0] + t * C.ax[2][0], C.c[1] + t * C.ax[2][1], C.c[2] + t * C.ax[2][2]};
+    if (O.type == G_SPHERE) {
+      double d[3] = {p[0] - O.c[0], p[1] - O.c[1], p[2] - O.c[2]};
+      return dot(d, d);
+    }
+    if (O.type == G_BOX) return point_box_d2(p, O);
+    return point_seg_d2(p, O);
+  };
+  double lo = -C.hl, hi = C.hl;
+  for (int it = 0; it < 200; ++it) {
+    double m1 = lo + (hi - lo) / 3, m2 = hi - (hi - lo) / 3;
+    if (f(m1) < f(m2))
+      hi = m2;
+    else
+      lo = m1;
+  }
+  return f(0.5 * (lo + hi));
+}
+
+bool static_pair_hit(const DGeom& A, const DGeom& B) {
+  if (A.type == G_SPHERE && B.type == G_SPHERE) {
+    double d[3] = {A.c[0] - B.c[0], A.c[1] - B.c[1], A.c[2] - B.c[2]};
+    return dot(d, d) < (A.r + B.r) * (A.r + B.r);
+  }
+  if (A.type == G_SPHERE && B.type == G_BOX) return point_box_d2(A.c, B) < A.r * A.r;
+  if (A.type == G_BOX && B.type == G_SPHERE) return point_box_d2(B.c, A) < B.r * B.r;
+  if (A.type == G_CAPSULE) {
+    double rr = A.r + (B.type == G_BOX ? 0.0 : B.r);
+    return seg_to_d2(A, B) < rr * rr;
+  }
+  if (B.type == G_CAPSULE) return static_pair_hit(B, A);
+  // box-box SAT
+  double axes[15][3];
+  int n = 0;
+  for (int a = 0; a < 3; ++a) {
+    for (int r = 0; r < 3; ++r) axes[n][r] = A.ax[a][r];
+    ++n;
+    for (int r = 0; r < 3; ++r) axes[n][r] = B.ax[a][r];
+    ++n;
+  }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      const double* a = A.ax[i];
+      const double* b = B.ax[j];
+      axes[n][0] = a[1] * b[2] - a[2] * b[1];
+      axes[n][1] = a[2] * b[0] - a[0] * b[2];
+      axes[n][2] = a[0] * b[1] - a[1] * b[0];
+      ++n;
+    }
+  double d[3] = {A.c[0] - B.c[0], A.c[1] - B.c[1], A.c[2] - B.c[2]};
+  for (int s = 0; s < 15; ++s) {
+    double lhs = std::fabs(dot(d, axes[s]));
+    double rhs = 0;
+    for (int a = 0; a < 3; ++a) rhs += A.h[a] * std::fabs(dot(A.ax[a], axes[s])) + B.h[a] * std::fabs(dot(B.ax[a], axes[s]));
+    if (lhs > rhs) return false;
+  }
+  return true;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+}  // namespace csd
+
+csd_plant_s::~csd_plant_s() {
+  if (blob) cudaFree(blob);
+}
+
+using namespace csd;
+
+extern "C" {
+
+const char* csd_last_error(void) { return csd::g_err.c_str(); }
+
+int32_t csd_version(void) { return 10000; }
+
+csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
+  CSD_CHECK(d && out, CSD_ERR_INVALID, "null argument");
+  *out = nullptr;
+  const int J = d->num_joints, L = d->num_links, D = d->num_configuration_variables, G = d->num_geometries,
+            P = d->num_collision_pairs;
+  CSD_CHECK(J >= 0 && L >= 1 && D >= 0 && G >= 0 && P >= 0, CSD_ERR_INVALID, "negative plant sizes");
+  CSD_CHECK(D <= kMaxDim, CSD_ERR_CAPACITY, "more than 16 configuration variables");
+  CSD_CHECK(J == 0 || (d->joint_type && d->joint_parent_link && d->joint_child_link && d->joint_idx_to_config_idx &&
+                       d->joint_traversal_sequence && d->joint_X_PL_J && d->joint_axis),
+            CSD_ERR_INVALID, "null joint table");
+  CSD_CHECK(G == 0 || (d->geom_type && d->geom_link_index && d->geom_dimensions && d->geom_X_L_B), CSD_ERR_INVALID,
+            "null geometry table");
+  CSD_CHECK(P == 0 || d->collision_pairs_flat, CSD_ERR_INVALID, "null pair table");
+  int dev_count = 0;
+  if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) {
+    set_error("no CUDA device");
+    return CSD_ERR_NO_DEVICE;
+  }
+
+  // ---- tree flattening
+  std::vector<int> slot(L, -2);
+  std::vector<X4> X(L, ident());
+  slot[0] = -1;
+  std::vector<FkJoint> fk;
+  std::vector<char> seen(J, 0);
+  for (int t = 0; t < J; ++t) {
+    int j = d->joint_traversal_sequence[t];
+    CSD_CHECK(j >= 0 && j < J && !seen[j], CSD_ERR_INVALID, "bad joint traversal sequence");
+    seen[j] = 1;
+    int pl = d->joint_parent_link[j], cl = d->joint_child_link[j], ty = d->joint_type[j];
+    CSD_CHECK(pl >= 0 && pl < L && cl >= 0 && cl < L, CSD_ERR_INVALID, "joint link index out of range");
+    CSD_CHECK(ty >= J_FIXED && ty <= J_PRISMATIC, CSD_ERR_INVALID, "bad joint type");
+    CSD_CHECK(slot[pl] != -2, CSD_ERR_INVALID, "traversal visits a child before its parent");
+    X4 xp = mul(X[pl], from_colmajor(d->joint_X_PL_J + 16 * j));
+    if (ty == J_FIXED) {
+      slot[cl] = slot[pl];
+      X[cl] = xp;
+      continue;
+    }
+    int qi = d->joint_idx_to_config_idx[j];
+    CSD_CHECK(qi >= 0 && qi < D, CSD_ERR_INVALID, "joint configuration index out of range");
+    CSD_CHECK((int)fk.size() < kMaxSlots, CSD_ERR_CAPACITY, "more than 32 moving joints");
+    FkJoint f{};
+    f.type = ty;
+    f.parent = slot[pl];
+    f.child = (int)fk.size();
+    f.qidx = qi;
+    double a[3] = {d->joint_axis[3 * j], d->joint_axis[3 * j + 1], d->joint_axis[3 * j + 2]};
+    double Ra[3];
+    for (int r = 0; r < 3; ++r) Ra[r] = xp.R[r] * a[0] + xp.R[3 + r] * a[1] + xp.R[6 + r] * a[2];
+    if (ty == J_REVOLUTE) {
+      // R(q) = Rp (c I + s [a]x + (1-c) a a^T) = c (Rp - Ra a^T) + s Rp [a]x + Ra a^T
+      double K[9] = {0, a[2], -a[1], -a[2], 0, a[0], a[1], -a[0], 0};  // [a]x column-major
+      for (int c = 0; c < 3; ++c)
+        for (int r = 0; r < 3; ++r) {
+          double T = Ra[r] * a[c];
+          double S = 0;
+          for (int k = 0; k < 3; ++k) S += xp.R[k * 3 + r] * K[c * 3 + k];
+          f.P[c * 3 + r] = (float)(xp.R[c * 3 + r] - T);
+          f.S[c * 3 + r] = (float)S;
+          f.T[c * 3 + r] = (float)T;
+        }
+    } else {
+      for (int i = 0; i < 9; ++i) f.P[i] = (float)xp.R[i];
+      for (int r = 0; r < 3; ++r) f.v[r] = (float)Ra[r];
+    }
+    for (int r = 0; r < 3; ++r) f.t[r] = (float)xp.t[r];
+    fk.push_back(f);
+    slot[cl] = f.child;
+    X[cl] = ident();
+  }
+
+  // ---- geometries
+  std::unique_ptr<csd_plant_s> h(new csd_plant_s());
+  cudaGetDevice(&h->device);
+  HostPlant& hp = h->host;
+  hp.dim = D;
+  hp.num_links = L;
+  hp.moving_of_geom.assign(G, -1);
+  hp.static_of_geom.assign(G, -1);
+  hp.geom_type.resize(G);
+  std::vector<X4> gX(G);
+  std::vector<int> mov_sph, mov_cap, mov_box, st_sph, st_box, st_cap;
+  for (int g = 0; g < G; ++g) {
+    int ty = d->geom_type[g], l = d->geom_link_index[g];
+    if (ty == G_CYLINDER) {
+      set_error("Cylinders are not supported (collision_checker.cpp:104-107).");
+      return CSD_ERR_UNSUPPORTED;
+    }
+    CSD_CHECK(ty == G_BOX || ty == G_SPHERE || ty == G_CAPSULE, CSD_ERR_INVALID, "bad geometry type");
+    CSD_CHECK(l >= 0 && l < L && slot[l] != -2, CSD_ERR_INVALID, "geometry on an unknown or unreachable link");
+    hp.geom_type[g] = ty;
+    gX[g] = mul(X[l], from_colmajor(d->geom_X_L_B + 16 * g));
+    bool moving = slot[l] >= 0;
+    auto& lst = moving ? (ty == G_SPHERE ? mov_sph : ty == G_CAPSULE ? mov_cap : mov_box)
+                       : (ty == G_SPHERE ? st_sph : ty == G_BOX ? st_box : st_cap);
+    lst.push_back(g);
+  }
+  std::vector<int> mov_order(mov_sph);
+  mov_order.insert(mov_order.end(), mov_cap.begin(), mov_cap.end());
+  mov_order.insert(mov_order.end(), mov_box.begin(), mov_box.end());
+  std::vector<int> st_order(st_sph);
+  st_order.insert(st_order.end(), st_box.begin(), st_box.end());
+  st_order.insert(st_order.end(), st_cap.begin(), st_cap.end());
+  int pose_words = 0;
+  for (size_t m = 0; m < mov_order.size(); ++m) {
+    int g = mov_order[m];
+    const float* dm = d->geom_dimensions + 3 * g;
+    MovingGeom mg{};
+    mg.type = d->geom_type[g];
+    mg.slot = slot[d->geom_link_index[g]];
+    mg.pose_off = pose_words;
+    pose_words += mg.type == G_SPHERE ? 4 : mg.type == G_CAPSULE ? 8 : 16;
+    mg.r = dm[0];
+    mg.hl = 0.5f * dm[1];
+    for (int r = 0; r < 3; ++r) {
+      mg.p[r] = (float)gX[g].t[r];
+      mg.z[r] = (float)gX[g].R[6 + r];
+      mg.h[r] = 0.5f * dm[r];
+    }
+    for (int i = 0; i < 9; ++i) mg.R[i] = (float)gX[g].R[i];
+    hp.moving.push_back(mg);
+    hp.moving_of_geom[g] = (int)m;
+  }
+  hp.statics.assign(st_order.size() * 16, 0.f);
+  for (size_t s = 0; s < st_order.size(); ++s) {
+    int g = st_order[s];
+    world_pose(d->geom_type[g], d->geom_dimensions + 3 * g, gX[g], hp.statics.data() + 16 * s);
+    hp.static_type.push_back(d->geom_type[g]);
+    hp.static_of_geom[g] = (int)s;
+  }
+
+  // ---- pairs
+  const int S = (int)st_order.size();
+  const int nmsph = (int)mov_sph.size();
+  const int T = (nmsph + kWarp - 1) / kWarp;
+  std::vector<uint32_t> masks((size_t)T * S, 0u);
+  std::vector<GenericPair> generic;
+  int always = 0, tile_pairs = 0;
+  for (int k = 0; k < P; ++k) {
+    int a = d->collision_pairs_flat[2 * k], b = d->collision_pairs_flat[2 * k + 1];
+    CSD_CHECK(a >= 0 && a < G && b >= 0 && b < G, CSD_ERR_INVALID, "collision pair index out of range");
+    int ma = hp.moving_of_geom[a], mb = hp.moving_of_geom[b];
+    if (ma < 0 && mb < 0) {
+      const float* da = d->geom_dimensions + 3 * a;
+      const float* db = d->geom_dimensions + 3 * b;
+      if (static_pair_hit(dgeom(d->geom_type[a], da, gX[a]), dgeom(d->geom_type[b], db, gX[b]))) always = 1;
+      continue;
+    }
+    if ((ma >= 0 && mb < 0 && ma < nmsph) || (mb >= 0 && ma < 0 && mb < nmsph)) {
+      int m = ma >= 0 ? ma : mb;
+      int s = ma >= 0 ? hp.static_of_geom[b] : hp.static_of_geom[a];
+      uint32_t& w = masks[(size_t)(m / kWarp) * S + s];
+      if (!(w & (1u << (m % kWarp)))) ++tile_pairs;
+      w |= 1u << (m % kWarp);
+      continue;
+    }
+    auto ref = [&](int g) -> uint32_t {
+      int m = hp.moving_of_geom[g];
+      return m >= 0 ? (uint32_t)m : (0x80000000u | (uint32_t)hp.static_of_geom[g]);
+    };
+    generic.push_back({ref(a), ref(b)});
+  }
+  auto type_of_ref = [&](uint32_t r) {
+    return (r & 0x80000000u) ? hp.static_type[r & 0x7fffffffu] : hp.moving[r].type;
+  };
+  std::stable_sort(generic.begin(), generic.end(), [&](const GenericPair& x, const GenericPair& y) {
+    int kx = type_of_ref(x.a) * 4 + type_of_ref(x.b), ky = type_of_ref(y.a) * 4 + type_of_ref(y.b);
+    return kx < ky;
+  });
+  std::vector<TileInfo> tiles(T);
+  std::vector<TileEntry> entries;
+  for (int t = 0; t < T; ++t) {
+    int lanes = std::min(kWarp, nmsph - t * kWarp);
+    uint32_t valid = lanes == 32 ? 0xffffffffu : ((1u << lanes) - 1u);
+    bool dense = true;
+    for (int s = 0; s < S; ++s)
+      if (masks[(size_t)t * S + s] != valid) dense = false;
+    TileInfo ti{};
+    ti.dense = dense ? 1 : 0;
+    ti.ent_begin = (int)entries.size();
+    for (int ty : {G_SPHERE, G_BOX, G_CAPSULE}) {
+      if (!dense)
+        for (int s = 0; s < S; ++s)
+          if (hp.static_type[s] == ty && masks[(size_t)t * S + s]) entries.push_back({(uint32_t)s, masks[(size_t)t * S + s]});
+      if (ty == G_SPHERE) ti.ent_sph_end = (int)entries.size();
+      if (ty == G_BOX) ti.ent_box_end = (int)entries.size();
+    }
+    ti.ent_end = (int)entries.size();
+    tiles[t] = ti;
+  }
+  hp.num_tile_pairs = tile_pairs;
+
+  // ---- FK output tables
+  std::vector<int> link_slot(L);
+  std::vector<float> link_fixed((size_t)L * 12, 0.f);
+  for (int l = 0; l < L; ++l) {
+    link_slot[l] = slot[l];
+    for (int i = 0; i < 9; ++i) link_fixed[(size_t)l * 12 + i] = (float)X[l].R[i];
+    for (int r = 0; r < 3; ++r) link_fixed[(size_t)l * 12 + 9 + r] = (float)X[l].t[r];
+  }
+
+  // ---- upload
+  size_t off = 0;
+  auto section = [&](size_t bytes) {
+    size_t o = off;
+    off = align256(off + std::max<size_t>(bytes, 16));
+    return o;
+  };
+  size_t o_fk = section(fk.size() * sizeof(FkJoint));
+  size_t o_mv = section(hp.moving.size() * sizeof(MovingGeom));
+  size_t o_st = section(hp.statics.size() * sizeof(float));
+  size_t o_sty = section(hp.static_type.size() * sizeof(int));
+  size_t o_ti = section(tiles.size() * sizeof(TileInfo));
+  size_t o_en = section(entries.size() * sizeof(TileEntry));
+  size_t o_ge = section(generic.size() * sizeof(GenericPair));
+  size_t o_ls = section(link_slot.size() * sizeof(int));
+  size_t o_lf = section(link_fixed.size() * sizeof(float));
+  std::vector<char> host_blob(off, 0);
+  auto put = [&](size_t o, const void* src, size_t n) {
+    if (n) std::memcpy(host_blob.data() + o, src, n);
+  };
+  put(o_fk, fk.data(), fk.size() * sizeof(FkJoint));
+  put(o_mv, hp.moving.data(), hp.moving.size() * sizeof(MovingGeom));
+  put(o_st, hp.statics.data(), hp.statics.size() * sizeof(float));
+  put(o_sty, hp.static_type.data(), hp.static_type.size() * sizeof(int));
+  put(o_ti, tiles.data(), tiles.size() * sizeof(TileInfo));
+  put(o_en, entries.data(), entries.size() * sizeof(TileEntry));
+  put(o_ge, generic.data(), generic.size() * sizeof(GenericPair));
+  put(o_ls, link_slot.data(), link_slot.size() * sizeof(int));
+  put(o_lf, link_fixed.data(), link_fixed.size() * sizeof(float));
+  CSD_CUDA_TRY(cudaMalloc(&h->blob, off));
+  CSD_CUDA_TRY(cudaMemcpy(h->blob, host_blob.data(), off, cudaMemcpyHostToDevice));
+  char* base = (char*)h->blob;
+  DevPlant& dp = h->dp;
+  dp.dim = D;
+  dp.num_fk = (int)fk.size();
+  dp.num_slots = (int)fk.size();
+  dp.num_moving = (int)hp.moving.size();
+  dp.num_msph = nmsph;
+  dp.num_mcap = (int)mov_cap.size();
+  dp.num_tiles = T;
+  dp.num_static = S;
+  dp.num_ssph = (int)st_sph.size();
+  dp.num_sbox = (int)st_box.size();
+  dp.num_scap = (int)st_cap.size();
+  dp.num_generic = (int)generic.size();
+  dp.pose_words = pose_words;
+  dp.always_colliding = always;
+  dp.num_links = L;
+  dp.fk = (const FkJoint*)(base + o_fk);
+  dp.moving = (const MovingGeom*)(base + o_mv);
+  dp.statics = (const float4*)(base + o_st);
+  dp.static_type = (const int*)(base + o_sty);
+  dp.tiles = (const TileInfo*)(base + o_ti);
+  dp.entries = (const TileEntry*)(base + o_en);
+  dp.generic = (const GenericPair*)(base + o_ge);
+  dp.link_slot = (const int*)(base + o_ls);
+  dp.link_fixed = (const float*)(base + o_lf);
+  *out = h.release();
+  return CSD_OK;
+}
+
+csd_status_t csd_plant_destroy(csd_plant_t p) {
+  if (!p) return CSD_OK;
+  int cur = 0, dev = p->device;
+  cudaGetDevice(&cur);
+  if (cur != dev) cudaSetDevice(dev);
+  delete p;
+  if (cur != dev) cudaSetDevice(cur);
+  return CSD_OK;
+}
+
+csd_status_t csd_plant_info(csd_plant_t p, csd_plant_info_t* info) {
+  CSD_CHECK(p && info, CSD_ERR_INVALID, "null argument");
+  info->dim = p->dp.dim;
+  info->num_links = p->dp.num_links;
+  info->num_fk_joints = p->dp.num_fk;
+  info->num_moving = p->dp.num_moving;
+  info->num_static = p->dp.num_static;
+  info->num_tile_pairs = p->host.num_tile_pairs;
+  info->num_generic_pairs = p->dp.num_generic;
+  info->always_colliding = p->dp.always_colliding;
+  return CSD_OK;
+}
+
+}  // extern "C"

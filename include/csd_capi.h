@@ -1,0 +1,207 @@
+/*
+ * csd_capi.h -- C ABI of csdecomp_b200, the B200 (sm_100a) implementation of
+ * CSDecomp's hot path: batched forward kinematics, primitive-pair collision
+ * checking over a MinimalPlant, batched edge checks, hit-and-run sampling in
+ * an H-polytope and EI-ZO edge inflation.
+ *
+ * Every entry point names the reference interface it replaces (paths are
+ * relative to the wernerpe/csdecomp source tree). Conventions:
+ *   - configurations are [N][dim] float32, contiguous (= Eigen's column-major
+ *     dim x N matrix of the reference);
+ *   - transforms are [N][num_links][16] float32, each 4x4 column-major;
+ *   - verdicts are uint8, 1 = collision free (the reference's convention);
+ *   - polytopes are A [F][dim] row-major float32 and b [F] float32;
+ *   - `flags` selects host (CSD_PTR_HOST) or device (CSD_PTR_DEVICE) memory
+ *     for the array arguments of a call. Device-pointer calls are ordered on
+ *     `stream` (a cudaStream_t, NULL = legacy default stream) and return
+ *     without synchronising; host-pointer calls copy through the handle's
+ *     device buffers and synchronise `stream` before returning;
+ *   - every function returns a csd_status_t; csd_last_error() gives the
+ *     message of the last failure on the calling thread. Nothing calls exit().
+ * Handles are not thread safe: use one handle per thread or lock externally.
+ */
+#ifndef CSD_CAPI_H
+#define CSD_CAPI_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t csd_status_t;
+enum {
+  CSD_OK = 0,
+  CSD_ERR_INVALID = 1,       /* bad argument (reference: std::invalid_argument / assert) */
+  CSD_ERR_CAPACITY = 2,      /* a capacity is exceeded (reference: std::runtime_error) */
+  CSD_ERR_NOT_CONTAINED = 3, /* start point outside its polytope (cuda_hit_and_run_sampling.cu:159-164) */
+  CSD_ERR_CUDA = 4,          /* CUDA runtime error (reference: CUDACHECKERROR -> exit) */
+  CSD_ERR_UNSUPPORTED = 5,   /* cylinders (collision_checker.cpp:104-107) */
+  CSD_ERR_DIMENSION = 6,     /* dimension mismatch (reference: std::runtime_error) */
+  CSD_ERR_NO_DEVICE = 7      /* no CUDA device visible */
+};
+
+enum { CSD_PTR_HOST = 0, CSD_PTR_DEVICE = 1 };
+
+/* Edge discretisation rules for csd_check_edges. */
+enum {
+  CSD_EDGE_L2_REF = 0, /* T = ceil(|q2-q1|_2 / step), t = k/T, k = 0..T-1 (end excluded):
+                          checkEdgeCollisionFree, csdecomp/src/plant/collision_checker.cpp:41-53 */
+  CSD_EDGE_LINF = 1,   /* T = ceil(|q2-q1|_inf / step), t = k/T, k = 0..T (both ends) */
+  CSD_EDGE_VG = 2      /* n = (uint)(|q2-q1|_2/step + 2) points incl. both ends:
+                          csdecomp/src/planning/cuda_visibility_graph.cu:58-72,123-172 */
+};
+
+/* Flat view of a MinimalPlant (csdecomp/src/plant/minimal_plant.h:16-39,
+ * minimal_kinematic_tree.h:18-53, collision_geometry.h:27-35), with no fixed
+ * capacities. All pointers are host memory and are only read during
+ * csd_plant_create. */
+typedef struct {
+  int32_t num_joints;
+  int32_t num_links;
+  int32_t num_configuration_variables;
+  int32_t num_geometries;
+  int32_t num_collision_pairs;
+  const int32_t* joint_type;               /* [J] 0 FIXED, 1 REVOLUTE, 2 PRISMATIC */
+  const int32_t* joint_parent_link;        /* [J] */
+  const int32_t* joint_child_link;         /* [J] */
+  const int32_t* joint_idx_to_config_idx;  /* [J], -1 for fixed joints */
+  const int32_t* joint_traversal_sequence; /* [J] */
+  const float* joint_X_PL_J;               /* [J][16] column-major */
+  const float* joint_axis;                 /* [J][3] */
+  const int32_t* geom_type;                /* [G] 0 BOX, 1 SPHERE, 2 CYLINDER, 3 CAPSULE */
+  const int32_t* geom_link_index;          /* [G] */
+  const int32_t* geom_group;               /* [G] 0 ROBOT, 1 WORLD, 2 VOXELS */
+  const float* geom_dimensions;            /* [G][3] box: full extents; sphere: (r,-1,-1);
+                                              capsule: (r, length, r), axis = local z */
+  const float* geom_X_L_B;                 /* [G][16] column-major */
+  const int32_t* collision_pairs_flat;     /* [2P] */
+} csd_plant_desc_t;
+
+typedef struct {
+  int32_t dim;             /* configuration variables */
+  int32_t num_links;
+  int32_t num_fk_joints;   /* moving joints evaluated per configuration */
+  int32_t num_moving;      /* geometries whose pose depends on q */
+  int32_t num_static;      /* geometries fixed in the world */
+  int32_t num_tile_pairs;  /* moving-sphere/static pairs swept by tiles */
+  int32_t num_generic_pairs;
+  int32_t always_colliding;/* a pair of static geometries collides */
+} csd_plant_info_t;
+
+typedef struct csd_plant_s* csd_plant_t;
+typedef struct csd_inflator_s* csd_inflator_t;
+
+const char* csd_last_error(void);
+int32_t csd_version(void);
+
+/* Uploads a plant once (device-resident, reusable across calls). Replaces the
+ * per-call CudaPtr<const MinimalPlant> upload of checkCollisionFreeCuda,
+ * csdecomp/src/plant/cuda_collision_checker.cu:458-462. Uses the current device. */
+csd_status_t csd_plant_create(const csd_plant_desc_t* desc, csd_plant_t* out);
+csd_status_t csd_plant_destroy(csd_plant_t plant);
+csd_status_t csd_plant_info(csd_plant_t plant, csd_plant_info_t* info);
+
+/* Forward kinematics: computeForwardKinematicsCuda,
+ * csdecomp/src/plant/cuda_forward_kinematics.cu:92-129 (device-pointer form:
+ * executeForwardKinematicsKernel, :79-90). transforms: [n][num_links][16]. */
+csd_status_t csd_fk(csd_plant_t plant, const float* q, int64_t n, float* transforms, int32_t flags,
+                    void* stream);
+
+/* Point check: checkCollisionFreeCuda, csdecomp/src/plant/cuda_collision_checker.cu:437-487,
+ * and with voxels (num_voxels > 0) checkCollisionFreeVoxelsCuda, :374-435
+ * (device-pointer forms: executeCollisionFreeKernel :182-209,
+ * executeCollisionFreeVoxelsKernel :256-307). voxels: [V][3] world positions of
+ * voxel spheres of radius voxel_radius, checked against robot_geometry_ids. */
+csd_status_t csd_check_points(csd_plant_t plant, const float* q, int64_t n, const float* voxels,
+                              int32_t num_voxels, float voxel_radius, const int32_t* robot_geometry_ids,
+                              int32_t num_robot_geometries, uint8_t* free_out, int32_t flags, void* stream);
+
+/* Batched edge check with early exit (new; the reference's CPU
+ * checkEdgeCollisionFree, collision_checker.cpp:41-53, checks one edge; its GPU
+ * edge checks live inside VisibilityGraph, cuda_visibility_graph.cu:175-375).
+ * starts/ends: [n][dim]. points_checked (optional, [n] int64): points
+ * evaluated before the verdict was known. */
+csd_status_t csd_check_edges(csd_plant_t plant, const float* starts, const float* ends, int64_t n,
+                             float step_size, int32_t mode, uint8_t* free_out, int64_t* points_checked,
+                             int32_t flags, void* stream);
+
+/* One pair: pairCollisionFree, csdecomp/src/plant/collision_checker.cpp:91-203
+ * (GPU contact rule of cuda_geometry_utilities.h:16-125). 4x4 matrices column-major. */
+csd_status_t csd_pair_collision_free(int32_t type_a, const float* dims_a, const float* X_L_B_a,
+                                     const float* X_W_LA, int32_t type_b, const float* dims_b,
+                                     const float* X_L_B_b, const float* X_W_LB, uint8_t* free_out);
+
+/* Hit-and-run sampling in several polytopes: UniformSampleInHPolyhedronCuda,
+ * csdecomp/src/geometry/cuda_hit_and_run_sampling.cu:137-210 (device-pointer
+ * form executeUniformSampleInHPolyhedronKernel, :121-134). Polytope p owns rows
+ * [face_offsets[p], face_offsets[p+1]) of A [F_total][dim] and b; starts:
+ * [P][dim]; samples: [P][samples_per_polytope][dim]. Host-pointer calls check
+ * every start point is contained (tolerance 1e-9, hpolyhedron.cpp:265-274).
+ * A chain whose line search fails writes NaN (the reference leaves the slot
+ * unwritten) and is counted in num_failed (optional, host int32). */
+csd_status_t csd_uniform_sample_hpolyhedra(const float* A, const float* b, const int32_t* face_offsets,
+                                           int32_t num_polytopes, int32_t dim, const float* starts,
+                                           int32_t samples_per_polytope, int32_t mixing_steps, uint64_t seed,
+                                           float* samples, int32_t* num_failed, int32_t flags, void* stream);
+
+/* EizoOptions, csdecomp/src/planning/cuda_edge_inflation_zero_order.h:18-32. */
+typedef struct {
+  float configuration_margin;
+  float tau;
+  float delta;
+  float epsilon;
+  uint32_t bisection_steps;
+  uint32_t num_particles;
+  uint32_t max_hyperplanes_per_iteration;
+  uint32_t max_iterations;
+  uint32_t mixing_steps;
+  uint64_t seed;
+  int32_t verbose;
+  int32_t track_iteration_information;
+} csd_eizo_options_t;
+
+/* EizoIterationInfo, cuda_edge_inflation_zero_order.h:37-47 (without the
+ * plotting buffer). */
+typedef struct {
+  int32_t iteration_index;
+  int32_t num_samples_drawn;
+  int32_t collisions_threshold;
+  int32_t num_collisions_unadaptive;
+  int32_t num_collisions_updated;
+  int32_t num_faces_placed;
+  float iteration_time_ms;
+} csd_eizo_iteration_info_t;
+
+/* CudaEdgeInflator constructor, csdecomp/src/planning/cuda_polytope_builder.cu:70-109:
+ * allocates all device memory once. domain: A [domain_faces][dim], b [domain_faces]
+ * (host). face_capacity: maximum faces of a region (domain included). */
+csd_status_t csd_inflator_create(csd_plant_t plant, const int32_t* robot_geometry_ids,
+                                 int32_t num_robot_geometries, const csd_eizo_options_t* options,
+                                 const float* domain_A, const float* domain_b, int32_t domain_faces,
+                                 int32_t max_voxels, int32_t face_capacity, csd_inflator_t* out);
+/* CudaEdgeInflator::inflateEdge, cuda_polytope_builder.cu:111-163, whose loop is
+ * executeEizo, cuda_edge_inflation_zero_order.cu:94-339. Inputs are host arrays;
+ * A_out/b_out (host) receive up to face_capacity rows; iteration records go to
+ * info (host, may be NULL). */
+csd_status_t csd_inflator_inflate(csd_inflator_t inflator, const float* line_start, const float* line_end,
+                                  const float* voxels, int32_t num_voxels, float voxel_radius, float* A_out,
+                                  float* b_out, int32_t* num_faces, csd_eizo_iteration_info_t* info,
+                                  int32_t info_capacity, int32_t* num_iterations, void* stream);
+csd_status_t csd_inflator_destroy(csd_inflator_t inflator);
+
+/* EizoCuda one-shot form, cuda_edge_inflation_zero_order.cu:341-446: creates an
+ * inflator, inflates, destroys it. */
+csd_status_t csd_eizo(csd_plant_t plant, const float* line_start, const float* line_end, const float* voxels,
+                      int32_t num_voxels, float voxel_radius, const float* domain_A, const float* domain_b,
+                      int32_t domain_faces, const int32_t* robot_geometry_ids, int32_t num_robot_geometries,
+                      const csd_eizo_options_t* options, int32_t face_capacity, float* A_out, float* b_out,
+                      int32_t* num_faces, csd_eizo_iteration_info_t* info, int32_t info_capacity,
+                      int32_t* num_iterations);
+
+/* numSamplesUnadaptive, csdecomp/src/planning/cuda_set_builder_utils.h:198-203. */
+uint32_t csd_num_samples_unadaptive(float epsilon, float delta, float tau);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
