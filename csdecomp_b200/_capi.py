@@ -85,7 +85,7 @@ EXPORTS = (
     "csd_last_error", "csd_version", "csd_plant_create", "csd_plant_destroy", "csd_plant_info", "csd_fk",
     "csd_check_points", "csd_check_edges", "csd_pair_collision_free", "csd_uniform_sample_hpolyhedra",
     "csd_inflator_create", "csd_inflator_inflate", "csd_inflator_destroy", "csd_eizo",
-    "csd_num_samples_unadaptive",
+    "csd_num_samples_unadaptive", "csd_fp32_fma_probe", "csd_plant_flops",
 )
 
 _lib = None
@@ -150,6 +150,12 @@ class PlantHandle:
         self.handle = h
         self.dim = dim
         self.num_links = num_links
+
+    def flops(self) -> dict:
+        fk, pl, pa = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        check(lib().csd_plant_flops(self.handle, ctypes.byref(fk), ctypes.byref(pl), ctypes.byref(pa)))
+        return {"fk": fk.value, "placement": pl.value, "pairs": pa.value,
+                "total": fk.value + pl.value + pa.value}
 
     def info(self) -> dict:
         i = PlantInfo()

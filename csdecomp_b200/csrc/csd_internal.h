@@ -55,7 +55,26 @@ struct HostPlant {  // host copies kept for host-side checks and voxel tables
   std::vector<float> statics;       // [S][16]
   std::vector<int> static_type;
   int num_tile_pairs = 0;
+  // algorithmic FP32 work of one configuration checked without early exit
+  // (FMA = 2 FLOP, add/mul/min/max/compare = 1; sqrt, div and sincos not counted)
+  double flops_fk = 0, flops_place = 0, flops_pairs = 0;
 };
+
+// FLOP of one evaluation of each pair test, from the code in csd_device.cuh.
+constexpr double kFlopSphSph = 11, kFlopSphBox = 32, kFlopSphCap = 24, kFlopCapCap = 58, kFlopCapBox = 240,
+                 kFlopBoxBox = 800;
+constexpr double kFlopFkRevolute = 99, kFlopFkPrismatic = 69, kFlopFkRootRevolute = 36, kFlopFkRootPrismatic = 6;
+constexpr double kFlopPlaceSphere = 18, kFlopPlaceCapsule = 33, kFlopPlaceBox = 78;
+inline double pair_flops(int ta, int tb) {
+  if (ta > tb) { int t = ta; ta = tb; tb = t; }
+  // types: 0 box, 1 sphere, 3 capsule
+  if (ta == 1 && tb == 1) return kFlopSphSph;
+  if (ta == 0 && tb == 1) return kFlopSphBox;
+  if (ta == 1 && tb == 3) return kFlopSphCap;
+  if (ta == 3 && tb == 3) return kFlopCapCap;
+  if (ta == 0 && tb == 3) return kFlopCapBox;
+  return kFlopBoxBox;
+}
 
 }  // namespace csd
 

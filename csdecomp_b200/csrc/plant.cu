@@ -422,6 +422,20 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
     tiles[t] = ti;
   }
   hp.num_tile_pairs = tile_pairs;
+  for (const FkJoint& f : fk)
+    hp.flops_fk += f.type == J_REVOLUTE ? (f.parent < 0 ? kFlopFkRootRevolute : kFlopFkRevolute)
+                                        : (f.parent < 0 ? kFlopFkRootPrismatic : kFlopFkPrismatic);
+  for (const MovingGeom& g : hp.moving)
+    hp.flops_place += g.type == G_SPHERE ? kFlopPlaceSphere : g.type == G_CAPSULE ? kFlopPlaceCapsule : kFlopPlaceBox;
+  for (int t = 0; t < T; ++t) {
+    int lanes = std::min(kWarp, nmsph - t * kWarp);
+    for (int sidx = 0; sidx < S; ++sidx) {
+      uint32_t w = masks[(size_t)t * S + sidx];
+      int cnt = tiles[t].dense ? lanes : __builtin_popcount(w);
+      hp.flops_pairs += cnt * pair_flops(G_SPHERE, hp.static_type[sidx]);
+    }
+  }
+  for (const GenericPair& gp : generic) hp.flops_pairs += pair_flops(type_of_ref(gp.a), type_of_ref(gp.b));
 
   // ---- FK output tables
   std::vector<int> link_slot(L);
@@ -500,6 +514,14 @@ csd_status_t csd_plant_destroy(csd_plant_t p) {
   if (cur != dev) cudaSetDevice(dev);
   delete p;
   if (cur != dev) cudaSetDevice(cur);
+  return CSD_OK;
+}
+
+csd_status_t csd_plant_flops(csd_plant_t p, double* fk, double* place, double* pairs) {
+  CSD_CHECK(p && fk && place && pairs, CSD_ERR_INVALID, "null argument");
+  *fk = p->host.flops_fk;
+  *place = p->host.flops_place;
+  *pairs = p->host.flops_pairs;
   return CSD_OK;
 }
 

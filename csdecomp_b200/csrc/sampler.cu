@@ -73,10 +73,11 @@ __global__ void __launch_bounds__(128) hit_and_run_kernel(const float* __restric
       if (k < dim) x[k] = __fmaf_rn(theta, dir[k], x[k]);
   }
   if (!ok && num_failed) atomicAdd(num_failed, 1);
+  // a chain whose line search fails writes NaN, or (fail_keep) its start point
   float* dst = out + i * dim;
 #pragma unroll
   for (int k = 0; k < MAXD; ++k)
-    if (k < dim) dst[k] = (ok || fail_keep) ? x[k] : __int_as_float(0x7fc00000);
+    if (k < dim) dst[k] = ok ? x[k] : fail_keep ? starts[(int64_t)poly * dim + k] : __int_as_float(0x7fc00000);
 }
 
 csd_status_t launch_hit_and_run(const float* A, const float* b, const int32_t* face_off, int num_poly, int dim,

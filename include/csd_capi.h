@@ -201,6 +201,14 @@ csd_status_t csd_eizo(csd_plant_t plant, const float* line_start, const float* l
 /* numSamplesUnadaptive, csdecomp/src/planning/cuda_set_builder_utils.h:198-203. */
 uint32_t csd_num_samples_unadaptive(float epsilon, float delta, float tau);
 
+/* Diagnostics (no counterpart in the reference): FP32 FMA throughput of the
+ * current device, the denominator of the collision kernels' roofline. */
+csd_status_t csd_fp32_fma_probe(int64_t iters, double* flops, double* seconds);
+/* Algorithmic FP32 work of checking one configuration of this plant without
+ * early exit: forward kinematics, geometry placement and all pair tests
+ * (FMA = 2 FLOP; sqrt, division and sincos not counted). */
+csd_status_t csd_plant_flops(csd_plant_t plant, double* fk_flops, double* placement_flops, double* pair_flops);
+
 #ifdef __cplusplus
 }
 #endif

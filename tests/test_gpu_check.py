@@ -1,0 +1,198 @@
+"""GPU parity of FK, point checks, edge checks and pair tests against the
+oracle (through the C ABI)."""
+import numpy as np
+import pytest
+
+import csdecomp_b200 as csd
+from csdecomp_b200 import scenes
+from csdecomp_b200.plant import CollisionGeometry, ShapePrimitive
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+BAND = 1e-5  # metres: verdicts may differ only within this signed-distance band
+
+
+def test_golden_verdicts(plants, golden):
+    for case in golden["verdicts"]:
+        p = plants[case["plant"]].plant
+        assert csd.CheckCollisionFreeCuda(np.array(case["free"], np.float32).T, p).all(), case["src"]
+        assert not csd.CheckCollisionFreeCuda(np.array(case["col"], np.float32).T, p).any(), case["src"]
+        assert csd.CheckCollisionFree(np.array(case["free"][0], np.float32), p)
+
+
+def test_golden_voxel_verdicts(plants, golden):
+    case = golden["voxel_verdicts"]
+    gp = plants[case["plant"]]
+    nx, ny, nz = case["grid"]
+    sx, sy, sz = case["spacing"]
+    off = np.array([-(nx - 1) * sx / 2, -(ny - 1) * sy / 2, 0], np.float32)
+    vox = np.array([np.array([ix * sx, iy * sy, iz * sz], np.float32) + off
+                    for ix in range(nx) for iy in range(ny) for iz in range(nz)], np.float32).T
+    f = csd.CheckCollisionFreeVoxelsCuda(np.array(case["free"], np.float32).T, csd.Voxels(vox), case["radius"],
+                                         gp.plant, gp.robot_geometry_ids)
+    c = csd.CheckCollisionFreeVoxelsCuda(np.array(case["col"], np.float32).T, csd.Voxels(vox), case["radius"],
+                                         gp.plant, gp.robot_geometry_ids)
+    assert f.all() and not c.any()
+
+
+@pytest.mark.parametrize("idx", range(4))
+def test_fk_golden(plants, golden, idx):
+    g = golden["fk"][idx]
+    gp = plants[g["plant"]]
+    tf = csd.ComputeForwardKinematicsCuda(np.array(g["q"], np.float32).reshape(-1, 1), gp.plant)[0]
+    np.testing.assert_allclose(tf[gp.link(g["link"])], np.array(g["X"]), atol=2e-6)
+    stacked = csd.computeLinkFrameToWorldTransformsMinimal(np.array(g["q"], np.float32), gp.plant.kin_tree)
+    np.testing.assert_allclose(stacked[4 * gp.link(g["link"]):4 * gp.link(g["link"]) + 4], np.array(g["X"]), atol=2e-6)
+
+
+@pytest.mark.parametrize("name", ["kinova_on_table", "2_branch_5dof", "movable_block", "synthetic14"])
+def test_fk_vs_fp64(plants, name):
+    if name == "synthetic14":
+        sc = scenes.arm_scene(7, num_spheres=40, arms=2)
+        p, q = sc.plant, sc.random_configs(3000, 1)
+    else:
+        gp = plants[name]
+        rng = np.random.default_rng(0)
+        p = gp.plant
+        lo, hi = np.maximum(gp.lower, -np.pi), np.minimum(gp.upper, np.pi)
+        q = (lo + (hi - lo) * rng.random((3000, gp.dim))).astype(np.float32)
+    tf = csd.ComputeForwardKinematicsCuda(q.T, p)
+    ref = O.fk(p, q, fp64=True).reshape(q.shape[0], -1, 4, 4).transpose(0, 1, 3, 2)
+    scale = max(1.0, np.abs(ref[..., :3, 3]).max())
+    err = np.abs(tf - ref).max()
+    # FP32 relative error bound of the FK transforms against the FP64 oracle
+    assert err <= 1e-5 * scale, err
+
+
+def band_parity(plant, q, voxels=None, vr=0.0, rids=()):
+    if voxels is None:
+        gpu = csd.CheckCollisionFreeCuda(q.T, plant)
+    else:
+        gpu = csd.CheckCollisionFreeVoxelsCuda(q.T, csd.Voxels(np.asarray(voxels).T), vr, plant, rids)
+    ref = O.check_points(plant, q, O.RULE_GPU, voxels, vr, rids)
+    v64, sd = O.signed_distance(plant, q, voxels, vr, rids)
+    outside = np.abs(sd) > BAND
+    assert (gpu[outside] == ref[outside]).all(), np.nonzero(gpu[outside] != ref[outside])
+    assert (gpu[outside] == v64[outside]).all()
+    return gpu, int((~outside).sum())
+
+
+@pytest.mark.parametrize("n", [1, 31, 33, 5000])
+def test_point_check_sizes(n):
+    sc = scenes.point_check_scene()
+    band_parity(sc.plant, sc.random_configs(n, 5))
+
+
+def test_point_check_parity_large():
+    sc = scenes.point_check_scene()
+    gpu, band = band_parity(sc.plant, sc.random_configs(40000, 11))
+    assert 0.1 < gpu.mean() < 0.5
+    assert band < 40
+
+
+def test_point_check_capsules_boxes_spheres():
+    sc = scenes.edge_check_scene(keepout=0.8)
+    band_parity(sc.plant, sc.random_configs(6000, 3))
+
+
+def test_point_check_two_arms():
+    sc = scenes.arm_scene(21, num_spheres=60, num_capsules=4, num_world_boxes=30, num_world_spheres=30, arms=2,
+                          keepout=0.6)
+    band_parity(sc.plant, sc.random_configs(4000, 4))
+
+
+def test_point_check_kinova(plants):
+    gp = plants["kinova_on_table"]
+    rng = np.random.default_rng(8)
+    q = (gp.lower + (gp.upper - gp.lower) * rng.random((8000, gp.dim))).astype(np.float32)
+    band_parity(gp.plant, q)
+
+
+def test_voxels_random(plants):
+    gp = plants["movable_block"]
+    rng = np.random.default_rng(2)
+    q = (gp.lower + (gp.upper - gp.lower) * rng.random((3000, gp.dim))).astype(np.float32)
+    vox = rng.uniform(-1, 1, (500, 3)).astype(np.float32)
+    band_parity(gp.plant, q, vox, 0.02, gp.robot_geometry_ids)
+
+
+def test_empty_batch():
+    sc = scenes.point_check_scene()
+    assert csd.CheckCollisionFreeCuda(np.zeros((7, 0), np.float32), sc.plant).shape == (0,)
+
+
+@pytest.mark.parametrize("mode", [csd.CSD_EDGE_L2_REF, csd.CSD_EDGE_LINF, csd.CSD_EDGE_VG])
+def test_edges_vs_oracle(mode):
+    sc = scenes.edge_check_scene(keepout=0.8)
+    rng = np.random.default_rng(mode)
+    # short edges so that free edges exist
+    s = sc.random_configs(1500, 40 + mode)
+    e = (s + rng.normal(0, 0.15, s.shape)).astype(np.float32)
+    gpu, pts = csd.CheckEdgesCollisionFreeCuda(s.T, e.T, sc.plant, 0.01, mode, return_points_checked=True)
+    ref, _ = O.check_edges(sc.plant, s, e, 0.01, mode)
+    diff = np.nonzero(gpu != ref)[0]
+    # a differing edge must contain a point within the contact band
+    for i in diff:
+        pts_i = O.edge_points(s[i], e[i], 0.01, mode)
+        _, sd = O.signed_distance(sc.plant, pts_i)
+        assert np.abs(sd).min() <= BAND, i
+    assert len(diff) <= 3
+    assert 0.05 < gpu.mean() < 0.95
+    n_all = np.array([O.edge_num_points(s[i], e[i], 0.01, mode) for i in range(len(s))])
+    assert (pts <= n_all).all() and (pts[gpu == 1] == n_all[gpu == 1]).all()
+
+
+def test_edge_visibility_graph_golden(plants, golden):
+    case = golden["visibility_graph"]
+    gp = plants[case["plant"]]
+    nodes = np.array(case["nodes"], np.float32)
+    n = len(nodes)
+    s, e = zip(*[(nodes[i], nodes[j]) for i in range(n - 1) for j in range(i + 1, n)])
+    v = csd.CheckEdgesCollisionFreeCuda(np.array(s).T, np.array(e).T, gp.plant, case["step"], csd.CSD_EDGE_VG)
+    assert list(v) == case["adjacency_upper"]
+
+
+def test_zero_length_edge_reference_rule():
+    sc = scenes.point_check_scene()
+    q = sc.random_configs(64, 9)
+    col = q[csd.CheckCollisionFreeCuda(q.T, sc.plant) == 0][:1]
+    # the reference's rule checks no point on a zero-length edge (collision_checker.cpp:44-52)
+    assert csd.CheckEdgesCollisionFreeCuda(col.T, col.T, sc.plant, 0.01, csd.CSD_EDGE_L2_REF)[0] == 1
+    assert csd.CheckEdgesCollisionFreeCuda(col.T, col.T, sc.plant, 0.01, csd.CSD_EDGE_LINF)[0] == 0
+
+
+def test_pair_collision_free_vs_oracle():
+    rng = np.random.default_rng(1)
+    types = [ShapePrimitive.SPHERE, ShapePrimitive.BOX, ShapePrimitive.CAPSULE]
+    agree = 0
+    for k in range(60):
+        ga = CollisionGeometry(type=types[k % 3], dimensions=np.array([0.3, 0.4, 0.2], np.float32))
+        gb = CollisionGeometry(type=types[(k // 3) % 3], dimensions=np.array([0.25, 0.3, 0.35], np.float32))
+        if ga.type == ShapePrimitive.SPHERE:
+            ga.dimensions[1:] = -1
+        if gb.type == ShapePrimitive.SPHERE:
+            gb.dimensions[1:] = -1
+        Xa = np.eye(4, dtype=np.float32)
+        Xb = np.eye(4, dtype=np.float32)
+        Xb[:3, :3] = scenes.random_rotation(rng)
+        Xb[:3, 3] = rng.uniform(-0.8, 0.8, 3)
+        g = csd.PairCollisionFree(ga, Xa, gb, Xb)
+        o = O.pair_collision_free(ga, Xa, gb, Xb, O.RULE_GPU)
+        agree += int(g == bool(o))
+    assert agree >= 59
+
+
+def test_errors():
+    sc = scenes.point_check_scene()
+    with pytest.raises(RuntimeError):
+        csd.CheckCollisionFreeCuda(np.zeros((5, 3), np.float32), sc.plant)
+    with pytest.raises(ValueError):
+        csd.CheckCollisionFreeVoxelsCuda(np.zeros((7, 3), np.float32), csd.Voxels(np.zeros((3, 2))), 0.1, sc.plant,
+                                         [10 ** 6])
+    bad = scenes.point_check_scene()
+    bad.plant.scene_collision_geometries[0].type = ShapePrimitive.CYLINDER
+    bad.plant._arrays = None
+    with pytest.raises(csd.CsdError) as ei:
+        csd.CheckCollisionFreeCuda(np.zeros((7, 1), np.float32), bad.plant)
+    assert ei.value.code == 5
