@@ -519,3 +519,222 @@ csd_status_t csd_eizo(csd_plant_t plant, const float* ls, const float* le, const
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------- allocation-free EI-ZO
+// csd_eizo_noalloc: the one-shot inflation for callers that must not allocate
+// device memory during the call. Its scratch (samples, verdict bytes,
+// collision points, projections, distances, the region being grown, segment,
+// voxel tables, counters) is carved from one file-scope device array; the
+// plant handle is created beforehand. Host code cannot pass the array's name
+// to a kernel (in host code it is a stand-in, not a device address), so the
+// first call on each device looks the address up with cudaGetSymbolAddress.
+#include <mutex>
+
+namespace csd {
+
+constexpr size_t kNoAllocScratchBytes = size_t(2) << 20;  // 2 MiB per device, held until process exit
+constexpr int kNoAllocMaxTiles = 64;
+constexpr int kNoAllocMaxRobotIds = 1024;
+
+static __device__ __align__(256) unsigned char g_eizo_scratch[kNoAllocScratchBytes];
+
+static std::mutex g_scratch_mu;
+static void* g_scratch_addr[64] = {nullptr};
+
+// Device address of g_eizo_scratch on the current device (looked up once per device).
+static csd_status_t scratch_address(int dev, unsigned char** out) {
+  CSD_CHECK(dev >= 0 && dev < 64, CSD_ERR_INVALID, "device index out of range");
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    CSD_CUDA_TRY(cudaGetSymbolAddress(&p, g_eizo_scratch));
+    g_scratch_addr[dev] = p;
+  }
+  *out = static_cast<unsigned char*>(g_scratch_addr[dev]);
+  return CSD_OK;
+}
+
+}  // namespace csd
+
+extern "C" csd_status_t csd_eizo_noalloc(csd_plant_t plant, const float* ls, const float* le, const float* voxels,
+                                         int32_t nv, float vr, const float* dA, const float* db, int32_t F0,
+                                         const int32_t* ids, int32_t nr, const csd_eizo_options_t* o,
+                                         int32_t capacity, float* A_out, float* b_out, int32_t* num_faces,
+                                         csd_eizo_iteration_info_t* info, int32_t info_cap, int32_t* num_iters,
+                                         void* stream) {
+  using namespace csd;
+  CSD_CHECK(plant && o && ls && le && A_out && b_out && num_faces, CSD_ERR_INVALID, "null argument");
+  CSD_CHECK(F0 >= 0 && (F0 == 0 || (dA && db)) && nr >= 0 && (nr == 0 || ids) && nv >= 0 && (nv == 0 || voxels),
+            CSD_ERR_INVALID, "bad domain, robot geometry or voxel arguments");
+  const int d = plant->dp.dim;
+  CSD_CHECK(d >= 1 && d <= kMaxDim, CSD_ERR_DIMENSION, "plant dimension must be in [1, 16]");
+  CSD_CHECK(capacity >= F0 && capacity > 0 && F0 <= 0.9 * capacity, CSD_ERR_CAPACITY,
+            "The domain polyhedron is already reserving almost all of the allocated faces.");
+  CSD_CHECK(o->num_particles >= 1 && o->max_iterations >= 1, CSD_ERR_INVALID,
+            "num_particles and max_iterations must be positive");
+  CSD_CHECK(o->tau > 0.f && o->tau < 1.f && o->epsilon > 0.f && o->delta > 0.f, CSD_ERR_INVALID,
+            "bad epsilon/delta/tau");
+  double delta_min = 6 * o->delta / (M_PI * M_PI * (double)o->max_iterations * (double)o->max_iterations);
+  const uint32_t mmax = csd_num_samples_unadaptive(o->epsilon, (float)delta_min, o->tau);
+  CSD_CHECK(o->num_particles <= mmax, CSD_ERR_CAPACITY,
+            "Current required particle count exceeds buffer size of the unadaptive test.");
+  CSD_CHECK(plant->dp.num_tiles <= kNoAllocMaxTiles && nr <= kNoAllocMaxRobotIds, CSD_ERR_CAPACITY,
+            "csd_eizo_noalloc supports at most 2048 moving spheres and 1024 robot geometry ids");
+  // point-in-domain check of the segment (as CudaEdgeInflator::inflateEdge asserts)
+  for (int s = 0; s < 2; ++s) {
+    const float* x = s ? le : ls;
+    for (int f = 0; f < F0; ++f) {
+      float ax = 0.f;
+      for (int k = 0; k < d; ++k) ax += dA[(size_t)f * d + k] * x[k];
+      CSD_CHECK(ax <= db[f] + 1e-9f, CSD_ERR_NOT_CONTAINED, "line segment endpoints must lie in the domain");
+    }
+  }
+  // ---- carve the scratch
+  const size_t max_configs = std::max<uint32_t>(mmax, o->num_particles), np = o->num_particles;
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t vtab_words = (size_t)plant->dp.num_tiles + (size_t)nr;
+  const size_t sz_A = al((size_t)capacity * d * 4), sz_b = al((size_t)capacity * 4), sz_nf = 256,
+               sz_samples = al(max_configs * d * 4), sz_flags = al(max_configs), sz_cols = al(np * d * 4),
+               sz_dist = al(np * 4), sz_seg = al(2 * (size_t)d * 4), sz_vox = al((size_t)nv * 12),
+               sz_vtab = al(vtab_words * 4), sz_cnt = 256;
+  const size_t need = sz_A + sz_b + sz_nf + sz_samples + sz_flags + 2 * sz_cols + sz_dist + sz_seg + sz_vox +
+                      sz_vtab + sz_cnt;
+  if (need > kNoAllocScratchBytes) {
+    set_error("csd_eizo_noalloc needs " + std::to_string(need) + " bytes of scratch for these options, more than its " +
+              std::to_string(kNoAllocScratchBytes) +
+              "-byte array (fewer particles, faces, voxels or unadaptive samples fit)");
+    return CSD_ERR_CAPACITY;
+  }
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != plant->device) cudaSetDevice(plant->device);
+  struct Restore {
+    int cur, dev;
+    ~Restore() {
+      if (cur != dev) cudaSetDevice(cur);
+    }
+  } restore{cur, plant->device};
+  unsigned char* base = nullptr;
+  csd_status_t s = scratch_address(plant->device, &base);
+  if (s) return s;
+  unsigned char* at = base;
+  auto take = [&](size_t n) {
+    unsigned char* p = at;
+    at += n;
+    return p;
+  };
+  float* A = (float*)take(sz_A);
+  float* b = (float*)take(sz_b);
+  int* nf = (int*)take(sz_nf);
+  float* samples = (float*)take(sz_samples);
+  uint8_t* flags = (uint8_t*)take(sz_flags);
+  float* cols = (float*)take(sz_cols);
+  float* proj = (float*)take(sz_cols);
+  float* dist = (float*)take(sz_dist);
+  float* seg = (float*)take(sz_seg);
+  float* vox = (float*)take(sz_vox);
+  uint32_t* vtab = (uint32_t*)take(sz_vtab);
+  EizoCounters* cnt = (EizoCounters*)take(sz_cnt);
+  cudaStream_t st = (cudaStream_t)stream;
+  // voxel tables from the robot geometry ids (fixed-size host arrays, no allocation)
+  uint32_t vt_host[kNoAllocMaxTiles + kNoAllocMaxRobotIds];
+  int num_other = 0;
+  const int T = plant->dp.num_tiles;
+  for (int t = 0; t < T; ++t) vt_host[t] = 0u;
+  for (int k = 0; k < nr; ++k) {
+    int g = ids[k];
+    CSD_CHECK(g >= 0 && g < (int)plant->host.moving_of_geom.size(), CSD_ERR_INVALID, "Invalid robot geometry ID");
+    int m = plant->host.moving_of_geom[g];
+    if (m >= 0 && m < plant->dp.num_msph)
+      vt_host[m / kWarp] |= 1u << (m % kWarp);
+    else
+      vt_host[T + num_other++] = m >= 0 ? (uint32_t)m : (0x80000000u | (uint32_t)plant->host.static_of_geom[g]);
+  }
+  // calls share the array: clear the counters, then reset region, segment and voxels
+  CSD_CUDA_TRY(cudaMemsetAsync(cnt, 0, sz_cnt, st));
+  if (F0) {
+    CSD_CUDA_TRY(cudaMemcpyAsync(A, dA, (size_t)F0 * d * 4, cudaMemcpyHostToDevice, st));
+    CSD_CUDA_TRY(cudaMemcpyAsync(b, db, (size_t)F0 * 4, cudaMemcpyHostToDevice, st));
+  }
+  int nf_host = F0;
+  CSD_CUDA_TRY(cudaMemcpyAsync(nf, &nf_host, sizeof(int), cudaMemcpyHostToDevice, st));
+  CSD_CUDA_TRY(cudaMemcpyAsync(seg, ls, d * 4, cudaMemcpyHostToDevice, st));
+  CSD_CUDA_TRY(cudaMemcpyAsync(seg + d, le, d * 4, cudaMemcpyHostToDevice, st));
+  if (nv) CSD_CUDA_TRY(cudaMemcpyAsync(vox, voxels, (size_t)nv * 12, cudaMemcpyHostToDevice, st));
+  if (vtab_words) CSD_CUDA_TRY(cudaMemcpyAsync(vtab, vt_host, (T + num_other) * 4, cudaMemcpyHostToDevice, st));
+  CSD_CUDA_TRY(cudaStreamSynchronize(st));  // host staging arrays go out of scope below
+  VoxelTables vt;
+  if (nv > 0 && nr > 0) {
+    vt.vox = vox;
+    vt.nv = nv;
+    vt.vr = vr;
+    vt.tile_mask = vtab;
+    vt.other = vtab + T;
+    vt.num_other = num_other;
+  }
+  VoxArgs va{vt.vox, vt.nv, vt.vr, vt.tile_mask, vt.other, vt.num_other};
+  EizoCounters hc{};
+  int nit = 0, last_with_faces = -1;
+  for (uint32_t it = 0; it < o->max_iterations; ++it) {
+    auto t0 = std::chrono::high_resolution_clock::now();
+    float delta_k = (float)(6 * o->delta / (M_PI * M_PI * (it + 1) * (it + 1)));
+    uint32_t M = csd_num_samples_unadaptive(o->epsilon, delta_k, o->tau);
+    uint32_t N = std::max(M, o->num_particles);
+    if ((s = launch_hit_and_run(A, b, nullptr, 1, d, seg, (int)N, (int)o->mixing_steps, o->seed, 0u, 1, samples,
+                                nullptr, nf, st)))
+      return s;
+    if ((s = launch_check_points(plant, samples, N, vt, flags, st))) return s;
+    compact_kernel<<<1, 1024, 0, st>>>(flags, samples, (int)N, (int)M, (int)o->num_particles, d, cols, cnt);
+    CSD_CUDA_TRY(cudaGetLastError());
+    CSD_CUDA_TRY(cudaMemcpyAsync(&hc, cnt, sizeof(EizoCounters), cudaMemcpyDeviceToHost, st));
+    CSD_CUDA_TRY(cudaStreamSynchronize(st));
+    if (last_with_faces >= 0) {
+      if (info && last_with_faces < info_cap) info[last_with_faces].num_faces_placed = (int32_t)hc.placed;
+      if (hc.status == 2) {
+        set_error("Max face count exceeded.");
+        return CSD_ERR_CAPACITY;
+      }
+      last_with_faces = -1;
+    }
+    const float thr = (1 - o->tau) * o->epsilon * M;
+    csd_eizo_iteration_info_t rec{};
+    rec.iteration_index = (int32_t)it;
+    rec.num_samples_drawn = (int32_t)N;
+    rec.collisions_threshold = (int32_t)thr;
+    rec.num_collisions_unadaptive = (int32_t)hc.first_m;
+    if ((float)hc.first_m <= thr) {
+      rec.iteration_time_ms =
+          std::chrono::duration<float, std::milli>(std::chrono::high_resolution_clock::now() - t0).count();
+      if (info && nit < info_cap) info[nit] = rec;
+      ++nit;
+      break;
+    }
+    const uint32_t K = std::min(hc.total, o->num_particles);
+    if ((s = launch_bisect(plant, (int)K, d, (int)o->bisection_steps, seg, seg + d, va, cols, proj, dist, st))) return s;
+    faces_kernel<<<1, 1024, 0, st>>>((int)K, d, (int)o->max_hyperplanes_per_iteration, capacity,
+                                     o->configuration_margin, seg, seg + d, cols, proj, dist, A, b, nf, cnt);
+    CSD_CUDA_TRY(cudaGetLastError());
+    rec.num_collisions_updated = (int32_t)K;
+    rec.iteration_time_ms =
+        std::chrono::duration<float, std::milli>(std::chrono::high_resolution_clock::now() - t0).count();
+    if (info && nit < info_cap) info[nit] = rec;
+    last_with_faces = nit;
+    ++nit;
+  }
+  CSD_CUDA_TRY(cudaMemcpyAsync(&hc, cnt, sizeof(EizoCounters), cudaMemcpyDeviceToHost, st));
+  CSD_CUDA_TRY(cudaMemcpyAsync(&nf_host, nf, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CSD_CUDA_TRY(cudaStreamSynchronize(st));
+  if (last_with_faces >= 0) {
+    if (info && last_with_faces < info_cap) info[last_with_faces].num_faces_placed = (int32_t)hc.placed;
+    if (hc.status == 2) {
+      set_error("Max face count exceeded.");
+      return CSD_ERR_CAPACITY;
+    }
+  }
+  CSD_CUDA_TRY(cudaMemcpyAsync(A_out, A, (size_t)nf_host * d * 4, cudaMemcpyDeviceToHost, st));
+  CSD_CUDA_TRY(cudaMemcpyAsync(b_out, b, (size_t)nf_host * 4, cudaMemcpyDeviceToHost, st));
+  CSD_CUDA_TRY(cudaStreamSynchronize(st));
+  *num_faces = nf_host;
+  if (num_iters) *num_iters = nit;
+  return CSD_OK;
+}

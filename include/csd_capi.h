@@ -198,6 +198,29 @@ csd_status_t csd_eizo(csd_plant_t plant, const float* line_start, const float* l
                       int32_t* num_faces, csd_eizo_iteration_info_t* info, int32_t info_capacity,
                       int32_t* num_iterations);
 
+/* Allocation-free EI-ZO (no counterpart in the reference). Same inputs,
+ * outputs and results as csd_eizo, for callers that must not allocate device
+ * memory while they run (a real-time loop that owns a fixed memory budget, a
+ * host that forbids allocation after start-up, code that has set aside all
+ * device memory for itself): no cudaMalloc/cudaFree or other allocating call is
+ * made. Its scratch is one 2 MiB array in the library's static device memory,
+ * present on every device that loads the library until the process exits;
+ * options whose scratch (samples of the unadaptive test, particles, region
+ * faces, voxels, at most 2048 moving spheres and 1024 robot geometry ids)
+ * exceeds it are rejected with CSD_ERR_CAPACITY. The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress); make that first
+ * call before any stream capture. All calls share the one array, so calls
+ * that overlap on the GPU (several streams or threads at once) race: issue
+ * them one at a time. Arrays are host memory; stream orders the work and is
+ * synchronised before return. The plant is created beforehand with
+ * csd_plant_create. */
+csd_status_t csd_eizo_noalloc(csd_plant_t plant, const float* line_start, const float* line_end,
+                              const float* voxels, int32_t num_voxels, float voxel_radius, const float* domain_A,
+                              const float* domain_b, int32_t domain_faces, const int32_t* robot_geometry_ids,
+                              int32_t num_robot_geometries, const csd_eizo_options_t* options, int32_t face_capacity,
+                              float* A_out, float* b_out, int32_t* num_faces, csd_eizo_iteration_info_t* info,
+                              int32_t info_capacity, int32_t* num_iterations, void* stream);
+
 /* numSamplesUnadaptive, csdecomp/src/planning/cuda_set_builder_utils.h:198-203. */
 uint32_t csd_num_samples_unadaptive(float epsilon, float delta, float tau);
 
