@@ -1,5 +1,20 @@
-// check_core.cuh -- warp-level collision checking shared by the check and
-// EI-ZO kernels (see check.cu for the design).
+// check_core.cuh -- warp-level collision checking shared by the check, edge and
+// EI-ZO kernels.
+//
+// One warp checks one configuration:
+//   1. FK, lane-parallel: lane j evaluates sin/cos of joint j, then for each
+//      moving joint lanes 0..11 compute one entry of its 3x4 world transform
+//      (R column-major 0..8, t 9..11) from the parent's entries in shared
+//      memory and the joint's local entries exchanged by warp shuffles.
+//   2. Placement, lane = moving geometry: world poses to shared memory.
+//   3. Sweep: a lane holds one moving sphere of a 32-sphere tile and all lanes
+//      stream the same static geometry (a shared-memory broadcast): static
+//      spheres, axis-aligned boxes, rotated boxes, capsules, then the tile's
+//      moving-sphere partners (self pairs, lane masks). Remaining pairs run in
+//      type-uniform segments, one pair per lane. A warp vote every few
+//      geometries stops the sweep at the first colliding pair.
+// The static tables are staged into shared memory once per block by a bulk
+// (TMA) copy; every wait on it is bounded and reports through p.status.
 #pragma once
 #include <algorithm>
 
@@ -8,7 +23,9 @@
 namespace csd {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kRow = 33;  // shared-memory row stride (floats) of the slot table
+constexpr long long kSpinLimit = 1ll << 26;   // mbarrier polls before a wait gives up
+constexpr int kStaticSmemLimit = 96 * 1024;   // larger static tables are read from global memory
+constexpr int kWarpsPerBlock = 8;
 
 struct VoxArgs {
   const float* vox;
@@ -19,55 +36,110 @@ struct VoxArgs {
   int num_other;
 };
 
-// Per-warp shared memory (floats): slot table [slots][12][kRow], the batch's
-// configurations [kMaxDim][kRow], moving world poses [pose_words].
-static __device__ __forceinline__ int per_warp_floats(const DevPlant& p) {
-  return p.num_slots * 12 * kRow + kMaxDim * kRow + ((p.pose_words + 3) & ~3);
-}
-static __device__ __forceinline__ float* warp_qbuf(const DevPlant& p, float* tf) { return tf + p.num_slots * 12 * kRow; }
-static __device__ __forceinline__ float* warp_pose(const DevPlant& p, float* tf) {
-  return tf + p.num_slots * 12 * kRow + kMaxDim * kRow;
+// Per-warp shared memory (floats): slot transforms [slots][12], the warp's
+// configuration [kMaxDim], moving world poses [pose_words].
+static __host__ __device__ __forceinline__ int warp_floats(const DevPlant& p) {
+  return p.num_slots * 12 + kMaxDim + ((p.pose_words + 3) & ~3);
 }
 
-static __device__ __forceinline__ void load_fk_joint(const FkJoint* src, FkJoint& J) {
-  const float4* s4 = reinterpret_cast<const float4*>(src);
-  float4* d4 = reinterpret_cast<float4*>(&J);
-#pragma unroll
-  for (int i = 0; i < 10; ++i) d4[i] = __ldg(s4 + i);
+// ------------------------------------------------------------ bulk staging
+static __device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
 }
 
-// FK of the configuration in column `lane` of the warp's configuration
-// buffer (qbuf[k * kRow + lane]) by one lane into the slot table.
-static __device__ __forceinline__ void fk_lane(const DevPlant& p, const float* qbuf, float* tf, int lane) {
-  for (int j = 0; j < p.num_fk; ++j) {
-    FkJoint J;
-    load_fk_joint(p.fk + j, J);
-    float Rl[9], tl[3], R[9], t[3];
-    joint_local(J, qbuf[J.qidx * kRow + lane], Rl, tl);
-    if (J.parent < 0) {
-#pragma unroll
-      for (int i = 0; i < 9; ++i) R[i] = Rl[i];
-#pragma unroll
-      for (int i = 0; i < 3; ++i) t[i] = tl[i];
-    } else {
-      float Rp[9], tp[3];
-      const float* src = tf + J.parent * 12 * kRow + lane;
-#pragma unroll
-      for (int i = 0; i < 9; ++i) Rp[i] = src[i * kRow];
-#pragma unroll
-      for (int i = 0; i < 3; ++i) tp[i] = src[(9 + i) * kRow];
-      compose(Rp, tp, Rl, tl, R, t);
+// Copies the static tables (p.static_bytes, a multiple of 16) into dst with
+// one cp.async.bulk per 64 KiB chunk completing on an mbarrier. Returns false
+// (and sets p.status) if the wait does not complete within kSpinLimit polls.
+static __device__ bool stage_statics(const DevPlant& p, float4* dst, uint64_t* bar) {
+  const unsigned bytes = (unsigned)p.static_bytes;
+  if (bytes == 0) return true;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+    const char* src = reinterpret_cast<const char*>(p.statics);
+    char* d = reinterpret_cast<char*>(dst);
+    for (unsigned off = 0; off < bytes; off += 65536u) {
+      unsigned n = min(65536u, bytes - off);
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+              smem_addr(d + off)),
+          "l"(src + off), "r"(n), "r"(smem_addr(bar))
+          : "memory");
     }
-    float* dst = tf + J.child * 12 * kRow + lane;
-#pragma unroll
-    for (int i = 0; i < 9; ++i) dst[i * kRow] = R[i];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) dst[(9 + i) * kRow] = t[i];
+  }
+  __syncthreads();
+  unsigned done = 0;
+  for (long long i = 0; i < kSpinLimit && !done; ++i) {
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(smem_addr(bar))
+        : "memory");
+  }
+  if (!done) {
+    atomicExch(p.status, 1);
+    // wait (bounded) once more for the copy still in flight before the block leaves
+    for (long long i = 0; i < kSpinLimit && !done; ++i)
+      asm volatile(
+          "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+          : "=r"(done)
+          : "r"(smem_addr(bar))
+          : "memory");
+    return false;
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------- FK
+// FK of the configuration in qs (shared, dim floats) into X[slot][12].
+static __device__ __forceinline__ void fk_warp(const DevPlant& p, const float* qs, float* X, int lane) {
+  float sj = 0.f, cj = 1.f, qj = 0.f;
+  if (lane < p.num_fk) {
+    qj = qs[__ldg(&p.fk[lane].qidx)];
+    sincosf(qj, &sj, &cj);
+  }
+  const int r = lane < 9 ? lane % 3 : lane - 9;
+  const int base = lane < 9 ? (lane / 3) * 3 : 9;
+  for (int j = 0; j < p.num_fk; ++j) {
+    const FkJoint* J = p.fk + j;
+    const int type = __ldg(&J->type), parent = __ldg(&J->parent), child = __ldg(&J->child);
+    const float s = __shfl_sync(kFull, sj, j), c = __shfl_sync(kFull, cj, j), qv = __shfl_sync(kFull, qj, j);
+    float loc = 0.f;
+    if (lane < 9) {
+      float P = __ldg(&J->P[lane]);
+      loc = type == J_REVOLUTE ? fmaf(c, P, fmaf(s, __ldg(&J->S[lane]), __ldg(&J->T[lane]))) : P;
+    } else if (lane < 12) {
+      float t = __ldg(&J->t[lane - 9]);
+      loc = type == J_PRISMATIC ? fmaf(__ldg(&J->v[lane - 9]), qv, t) : t;
+    }
+    float out = loc;
+    if (parent >= 0) {
+      const float a0 = __shfl_sync(kFull, loc, base);
+      const float a1 = __shfl_sync(kFull, loc, base + 1);
+      const float a2 = __shfl_sync(kFull, loc, base + 2);
+      if (lane < 12) {
+        const float* Xp = X + parent * 12;
+        float acc = lane < 9 ? Xp[r] * a0 : fmaf(Xp[r], a0, Xp[9 + r]);
+        acc = fmaf(Xp[3 + r], a1, acc);
+        out = fmaf(Xp[6 + r], a2, acc);
+      }
+    }
+    __syncwarp();
+    if (lane < 12) X[child * 12 + lane] = out;
+    __syncwarp();
   }
 }
 
-// Moving-geometry world poses of configuration c of the batch.
-static __device__ __forceinline__ void place_all(const DevPlant& p, const float* tf, float* pose, int c, int lane) {
+// ---------------------------------------------------------------- placement
+static __device__ __forceinline__ int pose_offset(const DevPlant& p, int m) {
+  if (m < p.num_msph) return 4 * m;
+  if (m < p.num_msph + p.num_mcap) return 4 * p.num_msph + 8 * (m - p.num_msph);
+  return 4 * p.num_msph + 8 * p.num_mcap + 16 * (m - p.num_msph - p.num_mcap);
+}
+
+static __device__ __forceinline__ void place_all(const DevPlant& p, const float* X, float* pose, int lane) {
   for (int m = lane; m < p.num_moving; m += kWarp) {
     const float4* s4 = reinterpret_cast<const float4*>(p.moving + m);
     MovingGeom g;
@@ -82,23 +154,23 @@ static __device__ __forceinline__ void place_all(const DevPlant& p, const float*
       d4[6] = __ldg(s4 + 6);
     }
     float R[9], t[3];
-    const float* src = tf + g.slot * 12 * kRow + c;
+    const float* src = X + g.slot * 12;
 #pragma unroll
-    for (int i = 0; i < 9; ++i) R[i] = src[i * kRow];
+    for (int i = 0; i < 9; ++i) R[i] = src[i];
 #pragma unroll
-    for (int i = 0; i < 3; ++i) t[i] = src[(9 + i) * kRow];
+    for (int i = 0; i < 3; ++i) t[i] = src[9 + i];
     float out[16];
     place_moving(g, R, t, out);
     float* dst = pose + g.pose_off;
     int nw = g.type == G_SPHERE ? 4 : g.type == G_CAPSULE ? 8 : 16;
-    for (int i = 0; i < nw; i += 4) *reinterpret_cast<float4*>(dst + i) = make_float4(out[i], out[i + 1], out[i + 2], out[i + 3]);
+    for (int i = 0; i < nw; i += 4)
+      *reinterpret_cast<float4*>(dst + i) = make_float4(out[i], out[i + 1], out[i + 2], out[i + 3]);
   }
 }
 
-static __device__ __forceinline__ void load_static(const DevPlant& p, int s, int nw, float* out) {
-  const float4* s4 = p.statics + 4 * s;
-  for (int i = 0; i < nw / 4; ++i) {
-    float4 v = __ldg(s4 + i);
+static __device__ __forceinline__ void load4f(const float4* src, int nq, float* out) {
+  for (int i = 0; i < nq; ++i) {
+    float4 v = src[i];
     out[4 * i] = v.x;
     out[4 * i + 1] = v.y;
     out[4 * i + 2] = v.z;
@@ -106,130 +178,142 @@ static __device__ __forceinline__ void load_static(const DevPlant& p, int s, int
   }
 }
 
-// Geometry reference (bit 31 = static) -> type and world pose.
-static __device__ __forceinline__ int load_ref(const DevPlant& p, const float* pose, uint32_t ref, float* out) {
-  if (ref & 0x80000000u) {
-    int s = (int)(ref & 0x7fffffffu);
-    int ty = __ldg(p.static_type + s);
-    load_static(p, s, ty == G_SPHERE ? 4 : ty == G_CAPSULE ? 8 : 16, out);
-    return ty;
-  }
-  int4 h = __ldg(reinterpret_cast<const int4*>(p.moving + ref));
-  int ty = h.x;
-  int nw = ty == G_SPHERE ? 4 : ty == G_CAPSULE ? 8 : 16;
-  const float* src = pose + h.z;
-  for (int i = 0; i < nw; ++i) out[i] = src[i];
-  return ty;
-}
-
-// Sphere tile t against all static geometries (dense tiles). Returns the
-// warp-uniform "some pair collides".
-static __device__ bool sweep_dense(const DevPlant& p, const float* pose, int t, int lane) {
-  const int m = t * kWarp + lane;
-  float c[4];
+static __device__ __forceinline__ void own_sphere(const DevPlant& p, const float* pose, int m, float* c) {
   if (m < p.num_msph) {
     float4 v = *reinterpret_cast<const float4*>(pose + 4 * m);
     c[0] = v.x; c[1] = v.y; c[2] = v.z; c[3] = v.w;
-  } else {
+  } else {  // no sphere: far away, tests report free
     c[0] = c[1] = c[2] = 1e30f;
     c[3] = 0.f;
   }
-  bool hit = false;
-  int s = 0;
-  const int s_sph = p.num_ssph, s_box = s_sph + p.num_sbox, s_end = s_box + p.num_scap;
-  for (; s < s_sph; ++s) {
-    float S[4];
-    load_static(p, s, 4, S);
-    hit |= sph_sph_hit(c, S);
-    if ((s & 7) == 7 && __any_sync(kFull, hit)) return true;
-  }
-  if (__any_sync(kFull, hit)) return true;
-  for (; s + 1 < s_box; s += 2) {
-    float B0[16], B1[16];
-    load_static(p, s, 16, B0);
-    load_static(p, s + 1, 16, B1);
-    hit |= sph_box_hit(c, c[3], B0) | sph_box_hit(c, c[3], B1);
-    if ((s & 6) == 6 && __any_sync(kFull, hit)) return true;
-  }
-  for (; s < s_box; ++s) {
-    float B[16];
-    load_static(p, s, 16, B);
-    hit |= sph_box_hit(c, c[3], B);
-  }
-  if (__any_sync(kFull, hit)) return true;
-  for (; s < s_end; ++s) {
-    float C[8];
-    load_static(p, s, 8, C);
-    hit |= sph_cap_hit(c, C);
-    if ((s & 3) == 3 && __any_sync(kFull, hit)) return true;
-  }
-  return __any_sync(kFull, hit);
 }
 
-// Sphere tile t against the static geometries listed in its entries.
-static __device__ bool sweep_masked(const DevPlant& p, const float* pose, int t, int lane) {
+// ------------------------------------------------------------------- sweeps
+// Tile t (moving spheres 32t .. 32t+31) against its static geometries and
+// moving-sphere partners. Returns the warp-uniform "some pair collides".
+static __device__ bool sweep_tile(const DevPlant& p, const float4* stat, const float4* aabb, const float* pose, int t,
+                                  int lane) {
   const TileInfo ti = p.tiles[t];
-  const int m = t * kWarp + lane;
   float c[4];
-  if (m < p.num_msph) {
-    float4 v = *reinterpret_cast<const float4*>(pose + 4 * m);
-    c[0] = v.x; c[1] = v.y; c[2] = v.z; c[3] = v.w;
-  } else {
-    c[0] = c[1] = c[2] = 1e30f;
-    c[3] = 0.f;
-  }
+  own_sphere(p, pose, t * kWarp + lane, c);
+  const float r2 = c[3] * c[3];
   bool hit = false;
-  int e = ti.ent_begin;
-  for (; e < ti.ent_sph_end; ++e) {
+  const int s0 = 0, s1 = p.num_ssph, s2 = s1 + p.num_sabox, s3 = s2 + p.num_srbox, s4 = s3 + p.num_scap;
+  // static spheres
+  if (ti.dense[SC_SPH]) {
+    for (int s = s0; s < s1; ++s) {
+      float4 S = stat[4 * s];
+      float d0 = c[0] - S.x, d1 = c[1] - S.y, d2 = c[2] - S.z;
+      float dd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+      float rr = c[3] + S.w;
+      hit |= !(dd >= rr * rr);
+      if ((s & 7) == 7 && __any_sync(kFull, hit)) return true;
+    }
+  } else {
+    for (int e = ti.ent[SC_SPH]; e < ti.ent[SC_SPH + 1]; ++e) {
+      TileEntry en = p.entries[e];
+      float4 S = stat[4 * en.s];
+      float d0 = c[0] - S.x, d1 = c[1] - S.y, d2 = c[2] - S.z;
+      float dd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+      float rr = c[3] + S.w;
+      hit |= ((en.mask >> lane) & 1u) && !(dd >= rr * rr);
+      if ((e & 7) == 7 && __any_sync(kFull, hit)) return true;
+    }
+  }
+  if (__any_sync(kFull, hit)) return true;
+  // axis-aligned static boxes
+  if (ti.dense[SC_ABOX]) {
+    for (int i = 0; i < p.num_sabox; ++i) {
+      hit |= sph_abox_hit(c, c[3], aabb[2 * i], aabb[2 * i + 1]);
+      if ((i & 7) == 7 && __any_sync(kFull, hit)) return true;
+    }
+  } else {
+    for (int e = ti.ent[SC_ABOX]; e < ti.ent[SC_ABOX + 1]; ++e) {
+      TileEntry en = p.entries[e];
+      const int i = en.s - s1;
+      hit |= ((en.mask >> lane) & 1u) && sph_abox_hit(c, c[3], aabb[2 * i], aabb[2 * i + 1]);
+      if ((e & 7) == 7 && __any_sync(kFull, hit)) return true;
+    }
+  }
+  if (__any_sync(kFull, hit)) return true;
+  // rotated static boxes
+  for (int k = 0, e = ti.ent[SC_RBOX]; ti.dense[SC_RBOX] ? k < s3 - s2 : e < ti.ent[SC_RBOX + 1]; ++k, ++e) {
+    int s = s2 + k;
+    uint32_t mask = kFull;
+    if (!ti.dense[SC_RBOX]) {
+      TileEntry en = p.entries[e];
+      s = en.s;
+      mask = en.mask;
+    }
+    float B[16];
+    load4f(stat + 4 * s, 4, B);
+    hit |= ((mask >> lane) & 1u) && sph_box_hit(c, c[3], B);
+    if ((k & 3) == 3 && __any_sync(kFull, hit)) return true;
+  }
+  // static capsules
+  for (int k = 0, e = ti.ent[SC_CAP]; ti.dense[SC_CAP] ? k < s4 - s3 : e < ti.ent[SC_CAP + 1]; ++k, ++e) {
+    int s = s3 + k;
+    uint32_t mask = kFull;
+    if (!ti.dense[SC_CAP]) {
+      TileEntry en = p.entries[e];
+      s = en.s;
+      mask = en.mask;
+    }
+    float C[8];
+    load4f(stat + 4 * s, 2, C);
+    hit |= ((mask >> lane) & 1u) && sph_cap_hit(c, C);
+    if ((k & 3) == 3 && __any_sync(kFull, hit)) return true;
+  }
+  if (__any_sync(kFull, hit)) return true;
+  // moving-sphere partners
+  for (int e = ti.self_begin; e < ti.self_end; ++e) {
     TileEntry en = p.entries[e];
-    float S[4];
-    load_static(p, en.s, 4, S);
-    hit |= ((en.mask >> lane) & 1u) && sph_sph_hit(c, S);
+    float4 Q = *reinterpret_cast<const float4*>(pose + 4 * en.s);
+    float d0 = c[0] - Q.x, d1 = c[1] - Q.y, d2 = c[2] - Q.z;
+    float dd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+    float rr = c[3] + Q.w;
+    hit |= ((en.mask >> lane) & 1u) && !(dd >= rr * rr);
     if ((e & 7) == 7 && __any_sync(kFull, hit)) return true;
   }
-  for (; e < ti.ent_box_end; ++e) {
-    TileEntry en = p.entries[e];
-    float B[16];
-    load_static(p, en.s, 16, B);
-    hit |= ((en.mask >> lane) & 1u) && sph_box_hit(c, c[3], B);
-    if ((e & 3) == 3 && __any_sync(kFull, hit)) return true;
-  }
-  for (; e < ti.ent_end; ++e) {
-    TileEntry en = p.entries[e];
-    float C[8];
-    load_static(p, en.s, 8, C);
-    hit |= ((en.mask >> lane) & 1u) && sph_cap_hit(c, C);
-    if ((e & 3) == 3 && __any_sync(kFull, hit)) return true;
-  }
+  (void)r2;
   return __any_sync(kFull, hit);
 }
 
-static __device__ bool sweep_generic(const DevPlant& p, const float* pose, int lane) {
-  for (int base = 0; base < p.num_generic; base += kWarp) {
-    int k = base + lane;
-    bool hit = false;
-    if (k < p.num_generic) {
-      GenericPair gp = p.generic[k];
-      float A[16], B[16];
-      int ta = load_ref(p, pose, gp.a, A);
-      int tb = load_ref(p, pose, gp.b, B);
-      hit = pair_hit(ta, A, tb, B);
+// Remaining pairs: type-uniform segments, one pair per lane.
+static __device__ bool sweep_generic(const DevPlant& p, const float4* stat, const float* pose, int lane) {
+  for (int sgi = 0; sgi < p.num_segs; ++sgi) {
+    const GenSeg sg = p.segs[sgi];
+    const int na = sg.ta == G_SPHERE ? 4 : sg.ta == G_CAPSULE ? 8 : 16;
+    const int nb = sg.tb == G_SPHERE ? 4 : sg.tb == G_CAPSULE ? 8 : 16;
+    for (int base = sg.begin; base < sg.end; base += kWarp) {
+      const int k = base + lane;
+      bool hit = false;
+      if (k < sg.end) {
+        const GenericPair gp = p.generic[k];
+        float A[16], B[16];
+        const float* pa = pose + pose_offset(p, (int)gp.a);
+        for (int i = 0; i < na; ++i) A[i] = pa[i];
+        if (sg.b_static) {
+          load4f(stat + 4 * (gp.b & 0x7fffffffu), nb / 4, B);
+        } else {
+          const float* pb = pose + pose_offset(p, (int)gp.b);
+          for (int i = 0; i < nb; ++i) B[i] = pb[i];
+        }
+        hit = pair_hit(sg.ta, A, sg.tb, B);
+      }
+      if (__any_sync(kFull, hit)) return true;
     }
-    if (__any_sync(kFull, hit)) return true;
   }
   return false;
 }
 
-static __device__ bool sweep_voxels(const DevPlant& p, const float* pose, const VoxArgs& va, int lane) {
+static __device__ bool sweep_voxels(const DevPlant& p, const float4* stat, const float* pose, const VoxArgs& va,
+                                    int lane) {
   for (int t = 0; t < p.num_tiles; ++t) {
-    uint32_t mask = va.tile_mask[t];
+    const uint32_t mask = va.tile_mask[t];
     if (!mask) continue;
-    const int m = t * kWarp + lane;
-    float c[4] = {1e30f, 1e30f, 1e30f, 0.f};
-    if (m < p.num_msph) {
-      float4 v = *reinterpret_cast<const float4*>(pose + 4 * m);
-      c[0] = v.x; c[1] = v.y; c[2] = v.z; c[3] = v.w;
-    }
+    float c[4];
+    own_sphere(p, pose, t * kWarp + lane, c);
     const bool mine = (mask >> lane) & 1u;
     bool hit = false;
     for (int v = 0; v < va.nv; ++v) {
@@ -240,10 +324,21 @@ static __device__ bool sweep_voxels(const DevPlant& p, const float* pose, const 
     if (__any_sync(kFull, hit)) return true;
   }
   for (int o = 0; o < va.num_other; ++o) {
+    const uint32_t ref = va.other[o];
     float G[16];
-    int tg = load_ref(p, pose, va.other[o], G);
+    int tg;
+    if (ref & 0x80000000u) {
+      const int s = (int)(ref & 0x7fffffffu);
+      tg = __ldg(p.static_type + s);
+      load4f(stat + 4 * s, tg == G_SPHERE ? 1 : tg == G_CAPSULE ? 2 : 4, G);
+    } else {
+      tg = __ldg(&p.moving[ref].type);
+      const int nw = tg == G_SPHERE ? 4 : tg == G_CAPSULE ? 8 : 16;
+      const float* src = pose + pose_offset(p, (int)ref);
+      for (int i = 0; i < nw; ++i) G[i] = src[i];
+    }
     for (int base = 0; base < va.nv; base += kWarp) {
-      int v = base + lane;
+      const int v = base + lane;
       bool hit = false;
       if (v < va.nv) {
         float S[4] = {va.vox[3 * v], va.vox[3 * v + 1], va.vox[3 * v + 2], va.vr};
@@ -255,26 +350,61 @@ static __device__ bool sweep_voxels(const DevPlant& p, const float* pose, const 
   return false;
 }
 
-// Full check of configuration c of the batch (warp-uniform result: true = colliding).
-static __device__ bool check_config(const DevPlant& p, const float* tf, float* pose, int c, int lane, const VoxArgs& va) {
+// Full check of the configuration whose slot transforms are in X
+// (warp-uniform result: true = colliding).
+static __device__ bool check_config(const DevPlant& p, const float4* stat, const float4* aabb, const float* X,
+                                    float* pose, int lane, const VoxArgs& va) {
   __syncwarp();
-  place_all(p, tf, pose, c, lane);
+  place_all(p, X, pose, lane);
   __syncwarp();
   if (p.always_colliding) return true;
-  for (int t = 0; t < p.num_tiles; ++t) {
-    bool h = p.tiles[t].dense ? sweep_dense(p, pose, t, lane) : sweep_masked(p, pose, t, lane);
-    if (h) return true;
-  }
-  if (sweep_generic(p, pose, lane)) return true;
-  if (va.nv > 0 && sweep_voxels(p, pose, va, lane)) return true;
+  for (int t = 0; t < p.num_tiles; ++t)
+    if (sweep_tile(p, stat, aabb, pose, t, lane)) return true;
+  if (sweep_generic(p, stat, pose, lane)) return true;
+  if (va.nv > 0 && sweep_voxels(p, stat, pose, va, lane)) return true;
   return false;
 }
 
+// Shared-memory setup common to the warp-per-configuration kernels. SM: the
+// static tables are staged into shared memory.
+template <bool SM>
+struct WarpCtx {
+  const float4* stat;
+  const float4* aabb;
+  float* X;
+  float* qs;
+  float* pose;
+  bool ok;
+};
+
+template <bool SM>
+static __device__ __forceinline__ WarpCtx<SM> warp_setup(const DevPlant& p, float4* smem4, uint64_t* bar) {
+  WarpCtx<SM> w;
+  const int warp = threadIdx.x >> 5;
+  float* wbase;
+  if (SM) {
+    w.ok = stage_statics(p, smem4, bar);
+    w.stat = smem4;
+    w.aabb = smem4 + 4 * p.num_static;
+    wbase = reinterpret_cast<float*>(smem4) + p.static_bytes / 4;
+  } else {
+    w.ok = true;
+    w.stat = p.statics;
+    w.aabb = p.aabb;
+    wbase = reinterpret_cast<float*>(smem4);
+  }
+  w.X = wbase + warp * warp_floats(p);
+  w.qs = w.X + p.num_slots * 12;
+  w.pose = w.qs + kMaxDim;
+  return w;
+}
+
 // ---- host helpers shared by the launchers
+static inline bool statics_in_smem(const csd_plant_s* p) { return p->dp.static_bytes <= kStaticSmemLimit; }
+
 static inline size_t smem_bytes(const csd_plant_s* p, int wpb) {
-  size_t per = (size_t)p->dp.num_slots * 12 * kRow + (size_t)kMaxDim * kRow +
-               (((size_t)p->dp.pose_words + 3) & ~size_t(3));
-  return per * sizeof(float) * wpb;
+  size_t per = (size_t)warp_floats(p->dp) * sizeof(float) * wpb;
+  return per + (statics_in_smem(p) ? (size_t)p->dp.static_bytes : 0);
 }
 
 template <typename K>

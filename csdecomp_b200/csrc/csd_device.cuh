@@ -56,18 +56,26 @@ struct MovingGeom {
 };
 static_assert(sizeof(MovingGeom) == 112, "MovingGeom is 7 float4");
 
-struct GenericPair {  // a/b: bit 31 set = static geometry, low bits = index
+// Static geometry classes, in table order.
+enum : int { SC_SPH = 0, SC_ABOX = 1, SC_RBOX = 2, SC_CAP = 3 };
+
+struct GenericPair {  // a: moving index; b: bit 31 set = static geometry, low bits = index
   uint32_t a, b;
 };
 
-struct TileInfo {     // moving spheres [32*t, 32*t+32) against static geometries
-  int dense;          // 1: every valid lane pairs with every static geometry
-  int ent_begin;      // otherwise: entries [ent_begin, ent_end) grouped by static type
-  int ent_sph_end, ent_box_end, ent_end;
-  int pad[3];
+struct GenSeg {       // generic pairs [begin, end) share (type a, type b, b static)
+  int begin, end, ta, tb;
+  int b_static, pad0, pad1, pad2;
 };
 
-struct TileEntry {    // one static geometry and the lanes of the tile that pair with it
+struct TileInfo {     // moving spheres [32*t, 32*t+32) against static geometries
+  int dense[4];       // per static class: every valid lane pairs with every static of the class
+  int ent[5];         // otherwise entries [ent[c], ent[c+1]) of class c
+  int self_begin, self_end;  // moving-sphere partners of the tile's lanes (self pairs)
+  int pad;
+};
+
+struct TileEntry {    // one static geometry (or moving partner) and the lanes of the tile that pair with it
   uint32_t s;
   uint32_t mask;
 };
@@ -81,22 +89,26 @@ struct DevPlant {
   int num_msph;          // moving spheres (first in the moving list)
   int num_mcap;          // moving capsules (next)
   int num_tiles;         // ceil(num_msph / 32)
-  int num_static;        // static geometries (spheres, then boxes, then capsules)
-  int num_ssph, num_sbox, num_scap;
+  int num_static;        // static geometries: spheres, aligned boxes, rotated boxes, capsules
+  int num_ssph, num_sabox, num_srbox, num_scap;
   int num_generic;       // generic pairs
+  int num_segs;          // generic segments
   int pose_words;        // words of moving world poses per configuration
   int always_colliding;  // a static-static pair collides
   int num_links;         // all links of the reference tree (FK output)
-  int pad;
+  int static_bytes;      // bytes of statics + aabb staged in shared memory (multiple of 16)
   const FkJoint* fk;
   const MovingGeom* moving;
-  const float4* statics;       // [num_static][4] float4 (WG format)
+  const float4* statics;       // [num_static][4] float4 (WG format); followed by aabb
+  const float4* aabb;          // [num_sabox][2]: [p 0 | h 0] of axis-aligned static boxes
   const int* static_type;      // [num_static]
   const TileInfo* tiles;
   const TileEntry* entries;
   const GenericPair* generic;
-  const int* link_slot;        // [num_links] slot of each reference link (-1 world)
+  const GenSeg* segs;
+  const int* link_slot;        // [num_links] slot of each reference link (-1 world, -2 unreachable)
   const float* link_fixed;     // [num_links][12] slot->link (R col-major 9, t 3); world links: world pose
+  int* status;                 // device error word: nonzero after a bounded wait gave up
 };
 
 // ------------------------------------------------------------------ FK
@@ -180,6 +192,16 @@ __device__ __forceinline__ bool sph_box_hit(const float* c, float r, const float
     e2 = fmaf(e, e, e2);
   }
   return !(e2 >= r * r);
+}
+
+// sphere (c, r) vs an axis-aligned box [p 0 | h 0]: the WG test with unit axes,
+// which computes exactly c_i - p_i for the box coordinates.
+__device__ __forceinline__ bool sph_abox_hit(const float* c, float r, const float4& P, const float4& H) {
+  float e0 = fmaxf(fabsf(c[0] - P.x) - H.x, 0.f);
+  float e1 = fmaxf(fabsf(c[1] - P.y) - H.y, 0.f);
+  float e2 = fmaxf(fabsf(c[2] - P.z) - H.z, 0.f);
+  float s = fmaf(e2, e2, fmaf(e1, e1, e0 * e0));
+  return !(s >= r * r);
 }
 
 __device__ __forceinline__ float clampf(float x, float lo, float hi) { return fmaxf(lo, fminf(x, hi)); }

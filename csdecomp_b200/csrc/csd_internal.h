@@ -61,7 +61,7 @@ struct HostPlant {  // host copies kept for host-side checks and voxel tables
 };
 
 // FLOP of one evaluation of each pair test, from the code in csd_device.cuh.
-constexpr double kFlopSphSph = 11, kFlopSphBox = 32, kFlopSphCap = 24, kFlopCapCap = 58, kFlopCapBox = 240,
+constexpr double kFlopSphSph = 11, kFlopSphBox = 32, kFlopSphABox = 16, kFlopSphCap = 24, kFlopCapCap = 58, kFlopCapBox = 240,
                  kFlopBoxBox = 800;
 constexpr double kFlopFkRevolute = 99, kFlopFkPrismatic = 69, kFlopFkRootRevolute = 36, kFlopFkRootPrismatic = 6;
 constexpr double kFlopPlaceSphere = 18, kFlopPlaceCapsule = 33, kFlopPlaceBox = 78;

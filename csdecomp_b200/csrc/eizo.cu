@@ -84,75 +84,67 @@ __global__ void compact_kernel(const uint8_t* __restrict__ flags, const float* _
 }
 
 
-__global__ void __launch_bounds__(128) bisect_kernel(DevPlant p, int K, int dim, int steps,
-                                                     const float* __restrict__ ls, const float* __restrict__ le,
-                                                     VoxArgs va, float* __restrict__ cols, float* __restrict__ proj,
-                                                     float* __restrict__ dist) {
+// One warp per particle: lane k holds coordinate k of the collision point,
+// its projection and the bisection bounds; each step is a fused FK + check of
+// the midpoint. Dot products are accumulated in coordinate order with
+// fused multiply-adds (the order the CPU restatement uses).
+template <bool SM>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) bisect_kernel(DevPlant p, int K, int dim, int steps,
+                                                                    const float* __restrict__ ls,
+                                                                    const float* __restrict__ le, VoxArgs va,
+                                                                    float* __restrict__ cols,
+                                                                    float* __restrict__ proj,
+                                                                    float* __restrict__ dist) {
   extern __shared__ float4 smem4[];
-  float* smem = reinterpret_cast<float*>(smem4);
-  const int wpb = blockDim.x >> 5, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* tf = smem + warp * per_warp_floats(p);
-  float* qbuf = warp_qbuf(p, tf);
-  float* pose = warp_pose(p, tf);
-  const int nbatch = (K + 31) / 32;
-  for (int b = blockIdx.x * wpb + warp; b < nbatch; b += gridDim.x * wpb) {
-    const int i = b * 32 + lane;
-    const int cnt = min(32, K - b * 32);
-    const bool valid = lane < cnt;
-    float c[kMaxDim], pr[kMaxDim], lo[kMaxDim], hi[kMaxDim];
-    if (valid) {
-      float seg2 = 0.f, a = 0.f;
-      for (int k = 0; k < dim; ++k) {
-        float dk = __fsub_rn(le[k], ls[k]);
-        c[k] = cols[(size_t)i * dim + k];
-        seg2 = __fmaf_rn(dk, dk, seg2);
-        a = __fmaf_rn(__fsub_rn(c[k], ls[k]), dk, a);
-      }
-      float t = fminf(fmaxf(__fdiv_rn(a, seg2), 0.0f), 1.0f);
-      float omt = __fsub_rn(1.0f, t);
-      for (int k = 0; k < dim; ++k) {
-        pr[k] = __fmaf_rn(t, le[k], __fmul_rn(omt, ls[k]));
-        lo[k] = pr[k];
-        hi[k] = c[k];
-      }
+  __shared__ uint64_t bar;
+  const WarpCtx<SM> w = warp_setup<SM>(p, smem4, &bar);
+  if (!w.ok) return;
+  const int lane = threadIdx.x & 31;
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < K; i += nw) {
+    const float* ci = cols + (size_t)i * dim;
+    // projection onto the segment (every lane evaluates the same serial sums)
+    float seg2 = 0.f, a = 0.f;
+    for (int k = 0; k < dim; ++k) {
+      float dk = __fsub_rn(le[k], ls[k]);
+      seg2 = __fmaf_rn(dk, dk, seg2);
+      a = __fmaf_rn(__fsub_rn(ci[k], ls[k]), dk, a);
+    }
+    const float t = fminf(fmaxf(__fdiv_rn(a, seg2), 0.0f), 1.0f);
+    const float omt = __fsub_rn(1.0f, t);
+    float c = 0.f, pr = 0.f, lo = 0.f, hi = 0.f;
+    if (lane < dim) {
+      c = ci[lane];
+      pr = __fmaf_rn(t, le[lane], __fmul_rn(omt, ls[lane]));
+      lo = pr;
+      hi = c;
     }
     for (int s = 0; s < steps; ++s) {
-      float mid[kMaxDim];
-      if (valid) {
-        for (int k = 0; k < dim; ++k) {
-          mid[k] = __fmul_rn(0.5f, __fadd_rn(lo[k], hi[k]));
-          qbuf[k * kRow + lane] = mid[k];
-        }
-        fk_lane(p, qbuf, tf, lane);
-      }
+      const float mid = __fmul_rn(0.5f, __fadd_rn(lo, hi));
       __syncwarp();
-      bool mine = false;
-      for (int cc = 0; cc < cnt; ++cc) {
-        bool h = check_config(p, tf, pose, cc, lane, va);
-        if (lane == cc) mine = h;
-      }
-      if (valid) {
-        for (int k = 0; k < dim; ++k) {
-          if (mine) {
-            hi[k] = mid[k];
-            c[k] = mid[k];
-          } else {
-            lo[k] = mid[k];
-          }
-        }
-      }
+      if (lane < dim) w.qs[lane] = mid;
       __syncwarp();
-    }
-    if (valid) {
-      float s2 = 0.f;
-      for (int k = 0; k < dim; ++k) {
-        float x = __fsub_rn(c[k], pr[k]);
-        s2 = __fmaf_rn(x, x, s2);
-        cols[(size_t)i * dim + k] = c[k];
-        proj[(size_t)i * dim + k] = pr[k];
+      fk_warp(p, w.qs, w.X, lane);
+      const bool hit = check_config(p, w.stat, w.aabb, w.X, w.pose, lane, va);
+      if (hit) {
+        hi = mid;
+        c = mid;
+      } else {
+        lo = mid;
       }
-      dist[i] = __fsqrt_rn(s2);
     }
+    // distance to the projection, coordinates in order
+    __syncwarp();
+    if (lane < dim) w.qs[lane] = __fsub_rn(c, pr);
+    __syncwarp();
+    float s2 = 0.f;
+    for (int k = 0; k < dim; ++k) s2 = __fmaf_rn(w.qs[k], w.qs[k], s2);
+    if (lane < dim) {
+      cols[(size_t)i * dim + lane] = c;
+      proj[(size_t)i * dim + lane] = pr;
+    }
+    if (lane == 0) dist[i] = __fsqrt_rn(s2);
+    __syncwarp();
   }
 }
 
@@ -300,12 +292,17 @@ static bool point_in_set(const std::vector<float>& A, const std::vector<float>& 
 static csd_status_t launch_bisect(const csd_plant_s* p, int K, int dim, int steps, const float* ls, const float* le,
                                   const VoxArgs& va, float* cols, float* proj, float* dist, cudaStream_t st) {
   if (K <= 0) return CSD_OK;
-  const int wpb = 4;
-  size_t smem = smem_bytes(p, wpb);
+  const bool sm = statics_in_smem(p);
+  const size_t smem = (size_t)warp_floats(p->dp) * sizeof(float) * kWarpsPerBlock + (sm ? p->dp.static_bytes : 0);
   int grid = 0;
-  csd_status_t s = grid_for(bisect_kernel, smem, (K + 31) / 32, &grid, wpb);
-  if (s) return s;
-  bisect_kernel<<<grid, 32 * wpb, smem, st>>>(p->dp, K, dim, steps, ls, le, va, cols, proj, dist);
+  csd_status_t s;
+  if (sm) {
+    if ((s = grid_for(bisect_kernel<true>, smem, K, &grid, kWarpsPerBlock))) return s;
+    bisect_kernel<true><<<grid, 32 * kWarpsPerBlock, smem, st>>>(p->dp, K, dim, steps, ls, le, va, cols, proj, dist);
+  } else {
+    if ((s = grid_for(bisect_kernel<false>, smem, K, &grid, kWarpsPerBlock))) return s;
+    bisect_kernel<false><<<grid, 32 * kWarpsPerBlock, smem, st>>>(p->dp, K, dim, steps, ls, le, va, cols, proj, dist);
+  }
   CSD_CUDA_TRY(cudaGetLastError());
   return CSD_OK;
 }

@@ -331,8 +331,18 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   std::vector<int> mov_order(mov_sph);
   mov_order.insert(mov_order.end(), mov_cap.begin(), mov_cap.end());
   mov_order.insert(mov_order.end(), mov_box.begin(), mov_box.end());
+  // world boxes whose axes are exactly the world axes get the aligned fast path
+  std::vector<int> st_abox, st_rbox;
+  for (int g : st_box) {
+    bool aligned = true;
+    for (int c = 0; c < 3; ++c)
+      for (int r = 0; r < 3; ++r)
+        if ((float)gX[g].R[c * 3 + r] != (c == r ? 1.f : 0.f)) aligned = false;
+    (aligned ? st_abox : st_rbox).push_back(g);
+  }
   std::vector<int> st_order(st_sph);
-  st_order.insert(st_order.end(), st_box.begin(), st_box.end());
+  st_order.insert(st_order.end(), st_abox.begin(), st_abox.end());
+  st_order.insert(st_order.end(), st_rbox.begin(), st_rbox.end());
   st_order.insert(st_order.end(), st_cap.begin(), st_cap.end());
   int pose_words = 0;
   for (size_t m = 0; m < mov_order.size(); ++m) {
@@ -366,9 +376,16 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   const int S = (int)st_order.size();
   const int nmsph = (int)mov_sph.size();
   const int T = (nmsph + kWarp - 1) / kWarp;
-  std::vector<uint32_t> masks((size_t)T * S, 0u);
+  const int cls_begin[5] = {0, (int)st_sph.size(), (int)(st_sph.size() + st_abox.size()),
+                            (int)(st_sph.size() + st_abox.size() + st_rbox.size()), S};
+  std::vector<uint32_t> masks((size_t)T * S, 0u);               // tile x static
+  std::vector<uint32_t> self_masks((size_t)T * nmsph, 0u);      // tile x moving-sphere partner
   std::vector<GenericPair> generic;
   int always = 0, tile_pairs = 0;
+  auto ref = [&](int g) -> uint32_t {
+    int m = hp.moving_of_geom[g];
+    return m >= 0 ? (uint32_t)m : (0x80000000u | (uint32_t)hp.static_of_geom[g]);
+  };
   for (int k = 0; k < P; ++k) {
     int a = d->collision_pairs_flat[2 * k], b = d->collision_pairs_flat[2 * k + 1];
     CSD_CHECK(a >= 0 && a < G && b >= 0 && b < G, CSD_ERR_INVALID, "collision pair index out of range");
@@ -381,44 +398,63 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
     }
     if ((ma >= 0 && mb < 0 && ma < nmsph) || (mb >= 0 && ma < 0 && mb < nmsph)) {
       int m = ma >= 0 ? ma : mb;
-      int s = ma >= 0 ? hp.static_of_geom[b] : hp.static_of_geom[a];
-      uint32_t& w = masks[(size_t)(m / kWarp) * S + s];
+      int st = ma >= 0 ? hp.static_of_geom[b] : hp.static_of_geom[a];
+      uint32_t& w = masks[(size_t)(m / kWarp) * S + st];
       if (!(w & (1u << (m % kWarp)))) ++tile_pairs;
       w |= 1u << (m % kWarp);
       continue;
     }
-    auto ref = [&](int g) -> uint32_t {
-      int m = hp.moving_of_geom[g];
-      return m >= 0 ? (uint32_t)m : (0x80000000u | (uint32_t)hp.static_of_geom[g]);
-    };
+    if (ma >= 0 && mb >= 0 && ma < nmsph && mb < nmsph && ma != mb) {
+      int lo = std::min(ma, mb), hi = std::max(ma, mb);
+      self_masks[(size_t)(lo / kWarp) * nmsph + hi] |= 1u << (lo % kWarp);
+      continue;
+    }
+    // generic: the moving geometry first
+    if (ma < 0 || (mb >= 0 && mb < ma)) std::swap(a, b);
     generic.push_back({ref(a), ref(b)});
   }
   auto type_of_ref = [&](uint32_t r) {
     return (r & 0x80000000u) ? hp.static_type[r & 0x7fffffffu] : hp.moving[r].type;
   };
-  std::stable_sort(generic.begin(), generic.end(), [&](const GenericPair& x, const GenericPair& y) {
-    int kx = type_of_ref(x.a) * 4 + type_of_ref(x.b), ky = type_of_ref(y.a) * 4 + type_of_ref(y.b);
-    return kx < ky;
-  });
+  auto seg_key = [&](const GenericPair& x) {
+    return ((x.b >> 31) * 16 + type_of_ref(x.a) * 4 + type_of_ref(x.b));
+  };
+  std::stable_sort(generic.begin(), generic.end(),
+                   [&](const GenericPair& x, const GenericPair& y) { return seg_key(x) < seg_key(y); });
+  std::vector<GenSeg> segs;
+  for (size_t i = 0; i < generic.size();) {
+    size_t j = i;
+    while (j < generic.size() && seg_key(generic[j]) == seg_key(generic[i])) ++j;
+    GenSeg sg{};
+    sg.begin = (int)i;
+    sg.end = (int)j;
+    sg.ta = type_of_ref(generic[i].a);
+    sg.tb = type_of_ref(generic[i].b);
+    sg.b_static = (int)(generic[i].b >> 31);
+    segs.push_back(sg);
+    i = j;
+  }
   std::vector<TileInfo> tiles(T);
   std::vector<TileEntry> entries;
   for (int t = 0; t < T; ++t) {
     int lanes = std::min(kWarp, nmsph - t * kWarp);
     uint32_t valid = lanes == 32 ? 0xffffffffu : ((1u << lanes) - 1u);
-    bool dense = true;
-    for (int s = 0; s < S; ++s)
-      if (masks[(size_t)t * S + s] != valid) dense = false;
     TileInfo ti{};
-    ti.dense = dense ? 1 : 0;
-    ti.ent_begin = (int)entries.size();
-    for (int ty : {G_SPHERE, G_BOX, G_CAPSULE}) {
+    for (int c = 0; c < 4; ++c) {
+      bool dense = true;
+      for (int st = cls_begin[c]; st < cls_begin[c + 1]; ++st)
+        if (masks[(size_t)t * S + st] != valid) dense = false;
+      ti.dense[c] = dense ? 1 : 0;
+      ti.ent[c] = (int)entries.size();
       if (!dense)
-        for (int s = 0; s < S; ++s)
-          if (hp.static_type[s] == ty && masks[(size_t)t * S + s]) entries.push_back({(uint32_t)s, masks[(size_t)t * S + s]});
-      if (ty == G_SPHERE) ti.ent_sph_end = (int)entries.size();
-      if (ty == G_BOX) ti.ent_box_end = (int)entries.size();
+        for (int st = cls_begin[c]; st < cls_begin[c + 1]; ++st)
+          if (masks[(size_t)t * S + st]) entries.push_back({(uint32_t)st, masks[(size_t)t * S + st]});
     }
-    ti.ent_end = (int)entries.size();
+    ti.ent[4] = (int)entries.size();
+    ti.self_begin = (int)entries.size();
+    for (int m2 = 0; m2 < nmsph; ++m2)
+      if (self_masks[(size_t)t * nmsph + m2]) entries.push_back({(uint32_t)m2, self_masks[(size_t)t * nmsph + m2]});
+    ti.self_end = (int)entries.size();
     tiles[t] = ti;
   }
   hp.num_tile_pairs = tile_pairs;
@@ -429,13 +465,25 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
     hp.flops_place += g.type == G_SPHERE ? kFlopPlaceSphere : g.type == G_CAPSULE ? kFlopPlaceCapsule : kFlopPlaceBox;
   for (int t = 0; t < T; ++t) {
     int lanes = std::min(kWarp, nmsph - t * kWarp);
-    for (int sidx = 0; sidx < S; ++sidx) {
-      uint32_t w = masks[(size_t)t * S + sidx];
-      int cnt = tiles[t].dense ? lanes : __builtin_popcount(w);
-      hp.flops_pairs += cnt * pair_flops(G_SPHERE, hp.static_type[sidx]);
-    }
+    for (int c = 0; c < 4; ++c)
+      for (int st = cls_begin[c]; st < cls_begin[c + 1]; ++st) {
+        uint32_t w = masks[(size_t)t * S + st];
+        int cnt = tiles[t].dense[c] ? lanes : __builtin_popcount(w);
+        hp.flops_pairs += cnt * (c == SC_ABOX ? kFlopSphABox : pair_flops(G_SPHERE, hp.static_type[st]));
+      }
+    for (int e = tiles[t].self_begin; e < tiles[t].self_end; ++e)
+      hp.flops_pairs += __builtin_popcount(entries[e].mask) * kFlopSphSph;
   }
   for (const GenericPair& gp : generic) hp.flops_pairs += pair_flops(type_of_ref(gp.a), type_of_ref(gp.b));
+  // axis-aligned box table [p 0 | h 0]
+  std::vector<float> aabb(st_abox.size() * 8, 0.f);
+  for (size_t i = 0; i < st_abox.size(); ++i) {
+    const float* W = hp.statics.data() + 16 * (cls_begin[SC_ABOX] + i);
+    for (int a = 0; a < 3; ++a) {
+      aabb[8 * i + a] = -W[4 * a + 3];
+      aabb[8 * i + 4 + a] = W[12 + a];
+    }
+  }
 
   // ---- FK output tables
   std::vector<int> link_slot(L);
@@ -455,11 +503,14 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   };
   size_t o_fk = section(fk.size() * sizeof(FkJoint));
   size_t o_mv = section(hp.moving.size() * sizeof(MovingGeom));
-  size_t o_st = section(hp.statics.size() * sizeof(float));
+  const size_t static_bytes = hp.statics.size() * sizeof(float) + aabb.size() * sizeof(float);
+  size_t o_st = section(static_bytes);
   size_t o_sty = section(hp.static_type.size() * sizeof(int));
   size_t o_ti = section(tiles.size() * sizeof(TileInfo));
   size_t o_en = section(entries.size() * sizeof(TileEntry));
   size_t o_ge = section(generic.size() * sizeof(GenericPair));
+  size_t o_sg = section(segs.size() * sizeof(GenSeg));
+  size_t o_status = section(16);
   size_t o_ls = section(link_slot.size() * sizeof(int));
   size_t o_lf = section(link_fixed.size() * sizeof(float));
   std::vector<char> host_blob(off, 0);
@@ -469,10 +520,12 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   put(o_fk, fk.data(), fk.size() * sizeof(FkJoint));
   put(o_mv, hp.moving.data(), hp.moving.size() * sizeof(MovingGeom));
   put(o_st, hp.statics.data(), hp.statics.size() * sizeof(float));
+  put(o_st + hp.statics.size() * sizeof(float), aabb.data(), aabb.size() * sizeof(float));
   put(o_sty, hp.static_type.data(), hp.static_type.size() * sizeof(int));
   put(o_ti, tiles.data(), tiles.size() * sizeof(TileInfo));
   put(o_en, entries.data(), entries.size() * sizeof(TileEntry));
   put(o_ge, generic.data(), generic.size() * sizeof(GenericPair));
+  put(o_sg, segs.data(), segs.size() * sizeof(GenSeg));
   put(o_ls, link_slot.data(), link_slot.size() * sizeof(int));
   put(o_lf, link_fixed.data(), link_fixed.size() * sizeof(float));
   CSD_CUDA_TRY(cudaMalloc(&h->blob, off));
@@ -488,19 +541,25 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   dp.num_tiles = T;
   dp.num_static = S;
   dp.num_ssph = (int)st_sph.size();
-  dp.num_sbox = (int)st_box.size();
+  dp.num_sabox = (int)st_abox.size();
+  dp.num_srbox = (int)st_rbox.size();
   dp.num_scap = (int)st_cap.size();
   dp.num_generic = (int)generic.size();
+  dp.num_segs = (int)segs.size();
+  dp.static_bytes = (int)static_bytes;
   dp.pose_words = pose_words;
   dp.always_colliding = always;
   dp.num_links = L;
   dp.fk = (const FkJoint*)(base + o_fk);
   dp.moving = (const MovingGeom*)(base + o_mv);
   dp.statics = (const float4*)(base + o_st);
+  dp.aabb = (const float4*)(base + o_st + hp.statics.size() * sizeof(float));
   dp.static_type = (const int*)(base + o_sty);
   dp.tiles = (const TileInfo*)(base + o_ti);
   dp.entries = (const TileEntry*)(base + o_en);
   dp.generic = (const GenericPair*)(base + o_ge);
+  dp.segs = (const GenSeg*)(base + o_sg);
+  dp.status = (int*)(base + o_status);
   dp.link_slot = (const int*)(base + o_ls);
   dp.link_fixed = (const float*)(base + o_lf);
   *out = h.release();
