@@ -18,7 +18,7 @@
 namespace csd {
 
 template <bool SM>
-__global__ void __launch_bounds__(32 * kWarpsPerBlock) check_points_kernel(DevPlant p, const float* __restrict__ q,
+__global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) check_points_kernel(DevPlant p, const float* __restrict__ q,
                                                                           int64_t n, VoxArgs va,
                                                                           uint8_t* __restrict__ out) {
   extern __shared__ float4 smem4[];
@@ -59,6 +59,23 @@ __device__ __forceinline__ void lerp_point(const float* q1, const float* q2, int
   for (int k = 0; k < d; ++k) out[k] = __fadd_rn(__fmul_rn(t, q2[k]), __fmul_rn(omt, q1[k]));
 }
 
+// Coordinate of point k of an edge from its endpoint coordinates (a1, a2),
+// under a discretisation rule (see csd_capi.h).
+__device__ __forceinline__ float edge_coord(float a1, float a2, int64_t np, int mode, int64_t k) {
+  float t;
+  if (mode == CSD_EDGE_L2_REF) {
+    t = __double2float_rn(__ddiv_rn((double)k, (double)np));
+  } else if (mode == CSD_EDGE_LINF) {
+    if (np - 1 == 0) return a1;
+    t = __double2float_rn(__ddiv_rn((double)k, (double)(np - 1)));
+  } else {
+    if (k == 0) return a1;
+    if (k == 1) return a2;
+    t = __fmul_rn(__double2float_rn(__ddiv_rn(1.0, (double)(np - 1))), (float)(k - 1));
+  }
+  return __fadd_rn(__fmul_rn(t, a2), __fmul_rn(__fsub_rn(1.0f, t), a1));
+}
+
 // Point k of an edge under a discretisation rule (see csd_capi.h).
 __device__ __forceinline__ void edge_point(const float* q1, const float* q2, int d, int64_t np, int mode, int64_t k,
                                            float* out) {
@@ -89,7 +106,7 @@ __device__ __forceinline__ void edge_point(const float* q1, const float* q2, int
 // coarse to fine: with G = ceil(n/32), the visit order is g, G+g, 2G+g, ...
 // for g = 0, 1, ..., so the first 32 visits sample the whole edge evenly.
 template <bool SM>
-__global__ void __launch_bounds__(32 * kWarpsPerBlock) check_edges_kernel(DevPlant p, const float* __restrict__ starts,
+__global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) check_edges_kernel(DevPlant p, const float* __restrict__ starts,
                                                                          const float* __restrict__ ends, int64_t n,
                                                                          float step, int mode,
                                                                          uint8_t* __restrict__ out,
@@ -107,21 +124,23 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) check_edges_kernel(DevPla
     if (lane == 0) e = atomicAdd(counter, 1ull);
     e = __shfl_sync(kFull, e, 0);
     if (e >= (unsigned long long)n) break;
-    float q1[kMaxDim], q2[kMaxDim];
-    for (int k = 0; k < d; ++k) {
-      q1[k] = starts[e * d + k];
-      q2[k] = ends[e * d + k];
+    __syncwarp();
+    if (lane < d) {
+      w.q1[lane] = starts[e * d + lane];
+      w.q2[lane] = ends[e * d + lane];
     }
-    const int64_t np = edge_points(q1, q2, d, step, mode);
+    __syncwarp();
+    const int64_t np = edge_points(w.q1, w.q2, d, step, mode);
     const int64_t G = (np + 31) / 32;
     bool collided = false;
     int64_t checked = 0;
+    const float a1 = lane < d ? w.q1[lane] : 0.f, a2 = lane < d ? w.q2[lane] : 0.f;
     for (int64_t v = 0; v < 32 * G && !collided; ++v) {
       const int64_t k = (v % 32) * G + v / 32;
       if (k >= np) continue;
-      float qk[kMaxDim];
-      edge_point(q1, q2, d, np, mode, k, qk);
-      if (lane < d) w.qs[lane] = qk[lane];
+      const float x = edge_coord(a1, a2, np, mode, k);
+      __syncwarp();
+      if (lane < d) w.qs[lane] = x;
       __syncwarp();
       fk_warp(p, w.qs, w.X, lane);
       ++checked;

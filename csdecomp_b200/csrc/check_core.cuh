@@ -37,9 +37,10 @@ struct VoxArgs {
 };
 
 // Per-warp shared memory (floats): slot transforms [slots][12], the warp's
-// configuration [kMaxDim], moving world poses [pose_words].
+// configuration [kMaxDim], two spare configurations (edge endpoints)
+// [2][kMaxDim], moving world poses [pose_words].
 static __host__ __device__ __forceinline__ int warp_floats(const DevPlant& p) {
-  return p.num_slots * 12 + kMaxDim + ((p.pose_words + 3) & ~3);
+  return p.num_slots * 12 + 3 * kMaxDim + ((p.pose_words + 3) & ~3);
 }
 
 // ------------------------------------------------------------ bulk staging
@@ -201,13 +202,24 @@ static __device__ bool sweep_tile(const DevPlant& p, const float4* stat, const f
   const int s0 = 0, s1 = p.num_ssph, s2 = s1 + p.num_sabox, s3 = s2 + p.num_srbox, s4 = s3 + p.num_scap;
   // static spheres
   if (ti.dense[SC_SPH]) {
-    for (int s = s0; s < s1; ++s) {
-      float4 S = stat[4 * s];
-      float d0 = c[0] - S.x, d1 = c[1] - S.y, d2 = c[2] - S.z;
-      float dd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
-      float rr = c[3] + S.w;
+    int s = s0;
+    for (; s + 8 <= s1; s += 8) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const float4 S = stat[4 * (s + u)];
+        const float d0 = c[0] - S.x, d1 = c[1] - S.y, d2 = c[2] - S.z;
+        const float dd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+        const float rr = c[3] + S.w;
+        hit |= !(dd >= rr * rr);
+      }
+      if (__any_sync(kFull, hit)) return true;
+    }
+    for (; s < s1; ++s) {
+      const float4 S = stat[4 * s];
+      const float d0 = c[0] - S.x, d1 = c[1] - S.y, d2 = c[2] - S.z;
+      const float dd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+      const float rr = c[3] + S.w;
       hit |= !(dd >= rr * rr);
-      if ((s & 7) == 7 && __any_sync(kFull, hit)) return true;
     }
   } else {
     for (int e = ti.ent[SC_SPH]; e < ti.ent[SC_SPH + 1]; ++e) {
@@ -223,10 +235,13 @@ static __device__ bool sweep_tile(const DevPlant& p, const float4* stat, const f
   if (__any_sync(kFull, hit)) return true;
   // axis-aligned static boxes
   if (ti.dense[SC_ABOX]) {
-    for (int i = 0; i < p.num_sabox; ++i) {
-      hit |= sph_abox_hit(c, c[3], aabb[2 * i], aabb[2 * i + 1]);
-      if ((i & 7) == 7 && __any_sync(kFull, hit)) return true;
+    int i = 0;
+    for (; i + 8 <= p.num_sabox; i += 8) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) hit |= sph_abox_hit(c, c[3], aabb[2 * (i + u)], aabb[2 * (i + u) + 1]);
+      if (__any_sync(kFull, hit)) return true;
     }
+    for (; i < p.num_sabox; ++i) hit |= sph_abox_hit(c, c[3], aabb[2 * i], aabb[2 * i + 1]);
   } else {
     for (int e = ti.ent[SC_ABOX]; e < ti.ent[SC_ABOX + 1]; ++e) {
       TileEntry en = p.entries[e];
@@ -279,30 +294,69 @@ static __device__ bool sweep_tile(const DevPlant& p, const float4* stat, const f
   return __any_sync(kFull, hit);
 }
 
-// Remaining pairs: type-uniform segments, one pair per lane.
+template <int T>
+struct Words {
+  static constexpr int n = T == G_SPHERE ? 4 : T == G_CAPSULE ? 8 : 16;
+};
+
+// One type-uniform segment of generic pairs, one pair per lane.
+template <int TA, int TB, bool BSTATIC>
+static __device__ bool generic_segment(const DevPlant& p, const float4* stat, const float* pose, const GenSeg& sg,
+                                       int lane) {
+  for (int base = sg.begin; base < sg.end; base += kWarp) {
+    const int k = base + lane;
+    bool hit = false;
+    if (k < sg.end) {
+      const GenericPair gp = p.generic[k];
+      float A[Words<TA>::n], B[Words<TB>::n];
+      const float4* pa = reinterpret_cast<const float4*>(pose + pose_offset(p, (int)gp.a));
+#pragma unroll
+      for (int i = 0; i < Words<TA>::n / 4; ++i) {
+        float4 v = pa[i];
+        A[4 * i] = v.x; A[4 * i + 1] = v.y; A[4 * i + 2] = v.z; A[4 * i + 3] = v.w;
+      }
+      const float4* pb = BSTATIC ? stat + 4 * (gp.b & 0x7fffffffu)
+                                 : reinterpret_cast<const float4*>(pose + pose_offset(p, (int)gp.b));
+#pragma unroll
+      for (int i = 0; i < Words<TB>::n / 4; ++i) {
+        float4 v = pb[i];
+        B[4 * i] = v.x; B[4 * i + 1] = v.y; B[4 * i + 2] = v.z; B[4 * i + 3] = v.w;
+      }
+      hit = pair_hit(TA, A, TB, B);
+    }
+    if (__any_sync(kFull, hit)) return true;
+  }
+  return false;
+}
+
+// Remaining pairs (the moving geometry first; moving-moving pairs ordered
+// sphere < capsule < box), dispatched once per segment.
 static __device__ bool sweep_generic(const DevPlant& p, const float4* stat, const float* pose, int lane) {
   for (int sgi = 0; sgi < p.num_segs; ++sgi) {
     const GenSeg sg = p.segs[sgi];
-    const int na = sg.ta == G_SPHERE ? 4 : sg.ta == G_CAPSULE ? 8 : 16;
-    const int nb = sg.tb == G_SPHERE ? 4 : sg.tb == G_CAPSULE ? 8 : 16;
-    for (int base = sg.begin; base < sg.end; base += kWarp) {
-      const int k = base + lane;
-      bool hit = false;
-      if (k < sg.end) {
-        const GenericPair gp = p.generic[k];
-        float A[16], B[16];
-        const float* pa = pose + pose_offset(p, (int)gp.a);
-        for (int i = 0; i < na; ++i) A[i] = pa[i];
-        if (sg.b_static) {
-          load4f(stat + 4 * (gp.b & 0x7fffffffu), nb / 4, B);
-        } else {
-          const float* pb = pose + pose_offset(p, (int)gp.b);
-          for (int i = 0; i < nb; ++i) B[i] = pb[i];
-        }
-        hit = pair_hit(sg.ta, A, sg.tb, B);
-      }
-      if (__any_sync(kFull, hit)) return true;
+    const int key = sg.b_static * 16 + sg.ta * 4 + sg.tb;
+    bool h = false;
+    switch (key) {
+      // moving-moving
+      case G_SPHERE * 4 + G_CAPSULE: h = generic_segment<G_SPHERE, G_CAPSULE, false>(p, stat, pose, sg, lane); break;
+      case G_SPHERE * 4 + G_BOX: h = generic_segment<G_SPHERE, G_BOX, false>(p, stat, pose, sg, lane); break;
+      case G_CAPSULE * 4 + G_CAPSULE: h = generic_segment<G_CAPSULE, G_CAPSULE, false>(p, stat, pose, sg, lane); break;
+      case G_CAPSULE * 4 + G_BOX: h = generic_segment<G_CAPSULE, G_BOX, false>(p, stat, pose, sg, lane); break;
+      case G_BOX * 4 + G_BOX: h = generic_segment<G_BOX, G_BOX, false>(p, stat, pose, sg, lane); break;
+      case G_BOX * 4 + G_SPHERE: h = generic_segment<G_BOX, G_SPHERE, false>(p, stat, pose, sg, lane); break;
+      case G_BOX * 4 + G_CAPSULE: h = generic_segment<G_BOX, G_CAPSULE, false>(p, stat, pose, sg, lane); break;
+      case G_CAPSULE * 4 + G_SPHERE: h = generic_segment<G_CAPSULE, G_SPHERE, false>(p, stat, pose, sg, lane); break;
+      case G_SPHERE * 4 + G_SPHERE: h = generic_segment<G_SPHERE, G_SPHERE, false>(p, stat, pose, sg, lane); break;
+      // moving-static
+      case 16 + G_CAPSULE * 4 + G_SPHERE: h = generic_segment<G_CAPSULE, G_SPHERE, true>(p, stat, pose, sg, lane); break;
+      case 16 + G_CAPSULE * 4 + G_BOX: h = generic_segment<G_CAPSULE, G_BOX, true>(p, stat, pose, sg, lane); break;
+      case 16 + G_CAPSULE * 4 + G_CAPSULE: h = generic_segment<G_CAPSULE, G_CAPSULE, true>(p, stat, pose, sg, lane); break;
+      case 16 + G_BOX * 4 + G_SPHERE: h = generic_segment<G_BOX, G_SPHERE, true>(p, stat, pose, sg, lane); break;
+      case 16 + G_BOX * 4 + G_BOX: h = generic_segment<G_BOX, G_BOX, true>(p, stat, pose, sg, lane); break;
+      case 16 + G_BOX * 4 + G_CAPSULE: h = generic_segment<G_BOX, G_CAPSULE, true>(p, stat, pose, sg, lane); break;
+      default: h = generic_segment<G_SPHERE, G_SPHERE, true>(p, stat, pose, sg, lane); break;
     }
+    if (h) return true;
   }
   return false;
 }
@@ -373,6 +427,8 @@ struct WarpCtx {
   const float4* aabb;
   float* X;
   float* qs;
+  float* q1;
+  float* q2;
   float* pose;
   bool ok;
 };
@@ -395,7 +451,9 @@ static __device__ __forceinline__ WarpCtx<SM> warp_setup(const DevPlant& p, floa
   }
   w.X = wbase + warp * warp_floats(p);
   w.qs = w.X + p.num_slots * 12;
-  w.pose = w.qs + kMaxDim;
+  w.q1 = w.qs + kMaxDim;
+  w.q2 = w.q1 + kMaxDim;
+  w.pose = w.q2 + kMaxDim;
   return w;
 }
 

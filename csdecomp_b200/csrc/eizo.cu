@@ -89,7 +89,7 @@ __global__ void compact_kernel(const uint8_t* __restrict__ flags, const float* _
 // the midpoint. Dot products are accumulated in coordinate order with
 // fused multiply-adds (the order the CPU restatement uses).
 template <bool SM>
-__global__ void __launch_bounds__(32 * kWarpsPerBlock) bisect_kernel(DevPlant p, int K, int dim, int steps,
+__global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) bisect_kernel(DevPlant p, int K, int dim, int steps,
                                                                     const float* __restrict__ ls,
                                                                     const float* __restrict__ le, VoxArgs va,
                                                                     float* __restrict__ cols,
