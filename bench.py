@@ -243,7 +243,9 @@ def main():
     total_edges = (args.warmup + args.steps) * world
     edges = seed_edges(scene, total_edges, lambda q: csd.CheckCollisionFreeCuda(q.T, scene.plant),
                        lambda a, b: csd.CheckEdgeCollisionFree(a, b, scene.plant))
-    mine = edges[rank::world]
+    from csdecomp_b200.shard import reduce_timing, shard
+    per_rank = args.warmup + args.steps
+    mine = edges[rank * per_rank:(rank + 1) * per_rank]
     dom = csd.HPolyhedron()
     dom.MakeBox(scene.lower(), scene.upper())
     opt = csd.EizoOptions(**EIZO_KW)
@@ -277,12 +279,7 @@ def main():
             d2h += P.A().shape[0] * (scene.dim + 1) * 4 + 16 * (len(it) + 1) + 4
     torch.cuda.synchronize()
     if dist:
-        t = torch.tensor([dev_s, wall_s, float(configs)], dtype=torch.float64, device=dev)
-        tmax = t.clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tsum = t.clone()
-        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-        dev_s, wall_s, configs_all = float(tmax[0]), float(tmax[1]), float(tsum[2])
+        dev_s, wall_s, configs_all = reduce_timing(dist, dev, dev_s, wall_s, float(configs))
         dist.barrier()
     else:
         configs_all = float(configs)

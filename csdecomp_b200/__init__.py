@@ -7,7 +7,7 @@ the C ABI of include/csd_capi.h.
 """
 from .plant import (CollisionGeometry, CollisionGroup, Joint, JointType, KinematicTree, Link, MinimalKinematicTree,
                     MinimalPlant, SceneInspector, ShapePrimitive, URDFParser)
-from .api import (MAX_DIM, MAX_NUM_FACES, MAX_NUM_VOXELS, CheckCollisionFree, CheckCollisionFreeCuda,
+from .api import (MAX_DIM, BatchedEdgeInflator, MAX_NUM_FACES, MAX_NUM_VOXELS, CheckCollisionFree, CheckCollisionFreeCuda,
                   CheckCollisionFreeVoxels, CheckCollisionFreeVoxelsCuda, CheckEdgeCollisionFree,
                   CheckEdgesCollisionFreeCuda, ComputeForwardKinematicsCuda, CudaEdgeInflator, EizoCuda, EizoInfo,
                   EizoIterationInfo, EizoOptions, HPolyhedron, MinimalHPolyhedron, PairCollisionFree, Voxels,

@@ -438,3 +438,66 @@ def EizoCuda(line_start, line_end, voxels, voxel_radius: float, domain: HPolyhed
         eizo_info.iteration_info = [EizoIterationInfo(*[getattr(iters[i], n) for n, _ in C.EizoIterC._fields_])
                                     for i in range(nit.value)]
     return MinimalHPolyhedron(A_out[:nf.value].copy(), b_out[:nf.value].copy())
+
+
+class BatchedEdgeInflator:
+    """Many EI-ZO inflations advancing together on the GPU (csd_batch_*): each
+    slot has its own plant, segment and domain and yields exactly the region
+    CudaEdgeInflator.inflateEdge would for the same inputs (no voxels)."""
+
+    def __init__(self, plants: Sequence[MinimalPlant], options: EizoOptions, max_slots: int,
+                 face_capacity: int = MAX_NUM_FACES):
+        self._plants = list(plants)
+        self._handles = [plant_handle(p) for p in self._plants]
+        self._options = options
+        self._capacity = int(face_capacity)
+        self._max_slots = int(max_slots)
+        arr = (ctypes.c_void_p * len(self._handles))(*[h.handle.value for h in self._handles])
+        self._opt_c = options._c()
+        h = ctypes.c_void_p()
+        C.check(C.lib().csd_batch_create(arr, len(self._handles), self._max_slots, ctypes.byref(self._opt_c),
+                                         self._capacity, ctypes.byref(h)))
+        self._handle = h
+        self.last_iterations = None
+
+    def inflate(self, slot_plant: Sequence[int], line_starts: Sequence[np.ndarray], line_ends: Sequence[np.ndarray],
+                domains: Sequence[HPolyhedron]) -> List[HPolyhedron]:
+        n = len(slot_plant)
+        if not (len(line_starts) == len(line_ends) == len(domains) == n):
+            raise ValueError("one segment and one domain per slot")
+        dims = [self._handles[int(i)].dim for i in slot_plant]
+        sp = np.ascontiguousarray(np.asarray(slot_plant, np.int32))
+        starts = np.ascontiguousarray(np.concatenate([np.asarray(x, np.float32).reshape(-1) for x in line_starts]))
+        ends = np.ascontiguousarray(np.concatenate([np.asarray(x, np.float32).reshape(-1) for x in line_ends]))
+        for d, x in zip(dims, line_starts):
+            if np.asarray(x).size != d:
+                raise RuntimeError("segment dimension does not match the slot's plant")
+        A = np.ascontiguousarray(np.concatenate([np.asarray(dm.A(), np.float32).reshape(-1) for dm in domains]))
+        b = np.ascontiguousarray(np.concatenate([np.asarray(dm.b(), np.float32).reshape(-1) for dm in domains]))
+        off = np.zeros(n + 1, np.int32)
+        off[1:] = np.cumsum([dm.A().shape[0] for dm in domains])
+        A_out = np.zeros(sum(self._capacity * d for d in dims), np.float32)
+        b_out = np.zeros(n * self._capacity, np.float32)
+        nf = np.zeros(n, np.int32)
+        nit = np.zeros(n, np.int32)
+        ms = ctypes.c_float(0)
+        C.check(C.lib().csd_batch_inflate(self._handle, n, C.ptr(sp), C.ptr(starts), C.ptr(ends), C.ptr(A), C.ptr(b),
+                                          C.ptr(off), C.ptr(A_out), C.ptr(b_out), C.ptr(nf), C.ptr(nit),
+                                          ctypes.byref(ms)))
+        self.last_iterations = nit
+        self.last_device_ms = ms.value
+        out, aoff = [], 0
+        for i, d in enumerate(dims):
+            Ai = A_out[aoff:aoff + nf[i] * d].reshape(nf[i], d).copy()
+            out.append(HPolyhedron(Ai, b_out[i * self._capacity:i * self._capacity + nf[i]].copy()))
+            aoff += self._capacity * d
+        return out
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h and C._lib is not None:
+            try:
+                C._lib.csd_batch_destroy(h)
+            except Exception:  # pragma: no cover
+                pass
+        self._handle = None

@@ -1,0 +1,555 @@
+// batch.cu -- many EI-ZO inflations advancing together (no counterpart in the
+// reference, which inflates one edge per executeEizo call,
+// csdecomp/src/planning/cuda_edge_inflation_zero_order.cu:94-339).
+//
+// Every active slot (one inflation: its own plant, segment and domain) runs
+// the same iteration k at the same time. The unadaptive sample count M_k
+// depends only on k and the shared options, so every slot draws the same N_k.
+// One iteration is five persistent kernels over (slot, chunk) work items:
+//   sample -> check -> compact (+ the admissibility decision, on the device)
+//   -> bisect -> faces
+// plus a counter bump; the sequence is captured once as a CUDA graph and
+// replayed, and the host reads one active-slot count per iteration. Each slot
+// runs exactly the arithmetic of the single-inflation path (csd_inflator_*),
+// so it produces the same region bit for bit.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "eizo_core.cuh"
+#include "sampler_core.cuh"
+
+namespace csd {
+
+struct SlotState {
+  int plant;          // index into the batch's plant array
+  int dim;
+  int domain_faces;
+  int nf;             // faces of the region so far
+  int done;           // finished: admissible, iteration limit, or error
+  int iters;          // iterations executed
+  int K;              // collisions kept for this iteration's bisection
+  int status;         // 2: face capacity exceeded
+  long long a_off;    // floats: region A [capacity][dim]
+  long long b_off;    // floats: region b [capacity]
+  long long seg_off;  // floats: line start [dim], line end [dim]
+  long long smp_off;  // floats: samples [n_max][dim]
+  long long col_off;  // floats: collision points / projections [num_particles][dim] each
+  long long dist_off; // floats: distances [num_particles]
+  long long flag_off; // bytes: verdicts [n_max]
+  EizoCounters cnt;
+};
+
+struct BatchIter {    // device-side iteration state
+  int k;              // current iteration
+  int active;         // slots still running, counted by the faces kernel
+  int last_active;    // the count of the iteration that just finished
+  int pad;
+};
+
+struct BatchArgs {
+  SlotState* slots;
+  const DevPlant* plants;
+  int num_slots;
+  int n_max;          // max over k of N_k (buffer stride)
+  int max_iters;
+  int num_particles;
+  int mixing;
+  int bisection;
+  int max_faces;
+  int capacity;
+  float margin;
+  uint32_t k0, k1;    // Philox key (seed)
+  const int* n_tab;   // N_k
+  const int* m_tab;   // M_k
+  const float* thr_tab;  // (1 - tau) * eps * M_k
+  float* fpool;
+  uint8_t* bpool;
+  BatchIter* it;
+};
+
+// ------------------------------------------------------------------ kernels
+__global__ void __launch_bounds__(128) batch_sample_kernel(BatchArgs a) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int slot = (int)(i / a.n_max), chain = (int)(i % a.n_max);
+  if (slot >= a.num_slots) return;
+  const SlotState& S = a.slots[slot];
+  const int N = a.n_tab[a.it->k];
+  if (S.done || chain >= N) return;
+  const int dim = S.dim;
+  const float* A = a.fpool + S.a_off;
+  const float* b = a.fpool + S.b_off;
+  const float* ls = a.fpool + S.seg_off;
+  float* dst = a.fpool + S.smp_off + (int64_t)chain * dim;
+  bool ok;
+  if (dim <= 8) {
+    float x[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = k < dim ? ls[k] : 0.f;
+    ok = run_chain<8>(A, b, S.nf, dim, a.mixing, a.k0, a.k1, (uint32_t)chain, 0u, x);
+    for (int k = 0; k < dim; ++k) dst[k] = ok ? x[k] : ls[k];
+  } else {
+    float x[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) x[k] = k < dim ? ls[k] : 0.f;
+    ok = run_chain<16>(A, b, S.nf, dim, a.mixing, a.k0, a.k1, (uint32_t)chain, 0u, x);
+    for (int k = 0; k < dim; ++k) dst[k] = ok ? x[k] : ls[k];
+  }
+}
+
+// Loads plant `pi` into the block's shared DevPlant and stages its statics.
+template <bool SM>
+static __device__ bool block_plant(const BatchArgs& a, int pi, DevPlant* sp, int* cur, float4* smem4, uint64_t* bar) {
+  if (*cur == pi) return true;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *sp = a.plants[pi];
+    *cur = pi;
+  }
+  __syncthreads();
+  if (SM) return stage_statics(*sp, smem4, bar);
+  return true;
+}
+
+template <bool SM>
+static __device__ __forceinline__ WarpCtx<SM> batch_ctx(const DevPlant& p, float4* smem4, int static_floats) {
+  WarpCtx<SM> w;
+  const int warp = threadIdx.x >> 5;
+  w.ok = true;
+  w.stat = SM ? smem4 : p.statics;
+  w.aabb = SM ? smem4 + 4 * p.num_static : p.aabb;
+  float* wbase = reinterpret_cast<float*>(smem4) + (SM ? static_floats : 0);
+  w.X = wbase + warp * warp_floats(p);
+  w.qs = w.X + p.num_slots * 12;
+  w.q1 = w.qs + kMaxDim;
+  w.q2 = w.q1 + kMaxDim;
+  w.pose = w.q2 + kMaxDim;
+  return w;
+}
+
+// Work item = (slot, chunk of configurations); a block takes a contiguous
+// run of items so consecutive items usually share a plant.
+template <bool SM>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_check_kernel(BatchArgs a, int cfg_per_item,
+                                                                            int static_floats) {
+  extern __shared__ float4 smem4[];
+  __shared__ uint64_t bar;
+  __shared__ DevPlant sp;
+  __shared__ int cur;
+  if (threadIdx.x == 0) cur = -1;
+  __syncthreads();
+  const int N = a.n_tab[a.it->k];
+  const int items_per_slot = (a.n_max + cfg_per_item - 1) / cfg_per_item;
+  const int64_t items = (int64_t)a.num_slots * items_per_slot;
+  const int64_t per_block = (items + gridDim.x - 1) / gridDim.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const VoxArgs none{nullptr, 0, 0.f, nullptr, nullptr, 0};
+  for (int64_t it = blockIdx.x * per_block; it < std::min<int64_t>(items, (blockIdx.x + 1) * per_block); ++it) {
+    const int slot = (int)(it / items_per_slot), chunk = (int)(it % items_per_slot);
+    const SlotState& S = a.slots[slot];
+    const int first = chunk * cfg_per_item;
+    if (S.done || first >= N) continue;  // uniform across the block
+    if (!block_plant<SM>(a, S.plant, &sp, &cur, smem4, &bar)) return;
+    const WarpCtx<SM> w = batch_ctx<SM>(sp, smem4, static_floats);
+    const float* smp = a.fpool + S.smp_off;
+    uint8_t* flags = a.bpool + S.flag_off;
+    const int last = std::min(N, first + cfg_per_item);
+    for (int i = first + warp; i < last; i += nw) {
+      if (lane < sp.dim) w.qs[lane] = smp[(int64_t)i * sp.dim + lane];
+      __syncwarp();
+      fk_warp(sp, w.qs, w.X, lane);
+      const bool hit = check_config(sp, w.stat, w.aabb, w.X, w.pose, lane, none);
+      if (lane == 0) flags[i] = hit ? 0 : 1;
+    }
+  }
+}
+
+// Block per slot: ordered compaction, first-M count, admissibility decision.
+__global__ void __launch_bounds__(1024) batch_compact_kernel(BatchArgs a) {
+  SlotState& S = a.slots[blockIdx.x];
+  if (S.done) return;
+  const int k = a.it->k;
+  const int N = a.n_tab[k], M = a.m_tab[k];
+  if (S.status == 2) {  // the previous faces kernel ran out of capacity
+    if (threadIdx.x == 0) S.done = 1;
+    return;
+  }
+  compact_block(a.bpool + S.flag_off, a.fpool + S.smp_off, N, M, a.num_particles, S.dim, a.fpool + S.col_off,
+                &S.cnt);
+  if (threadIdx.x == 0) {
+    if ((float)S.cnt.first_m <= a.thr_tab[k]) {
+      S.done = 1;
+      S.iters = k + 1;
+      S.K = 0;
+    } else {
+      S.K = (int)std::min<uint32_t>(S.cnt.total, (uint32_t)a.num_particles);
+    }
+  }
+}
+
+template <bool SM>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_bisect_kernel(BatchArgs a, int part_per_item,
+                                                                             int static_floats) {
+  extern __shared__ float4 smem4[];
+  __shared__ uint64_t bar;
+  __shared__ DevPlant sp;
+  __shared__ int cur;
+  if (threadIdx.x == 0) cur = -1;
+  __syncthreads();
+  const int items_per_slot = (a.num_particles + part_per_item - 1) / part_per_item;
+  const int64_t items = (int64_t)a.num_slots * items_per_slot;
+  const int64_t per_block = (items + gridDim.x - 1) / gridDim.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const VoxArgs none{nullptr, 0, 0.f, nullptr, nullptr, 0};
+  for (int64_t it = blockIdx.x * per_block; it < std::min<int64_t>(items, (blockIdx.x + 1) * per_block); ++it) {
+    const int slot = (int)(it / items_per_slot), chunk = (int)(it % items_per_slot);
+    const SlotState& S = a.slots[slot];
+    const int first = chunk * part_per_item;
+    if (S.done || first >= S.K) continue;
+    if (!block_plant<SM>(a, S.plant, &sp, &cur, smem4, &bar)) return;
+    const WarpCtx<SM> w = batch_ctx<SM>(sp, smem4, static_floats);
+    const float* ls = a.fpool + S.seg_off;
+    const int last = std::min(S.K, first + part_per_item);
+    for (int i = first + warp; i < last; i += nw)
+      bisect_particle<SM>(sp, w, i, S.dim, a.bisection, ls, ls + S.dim, none, a.fpool + S.col_off,
+                          a.fpool + S.col_off + (int64_t)a.num_particles * S.dim, a.fpool + S.dist_off, lane);
+  }
+}
+
+// Block per slot: greedy faces, iteration bookkeeping, active-slot count.
+__global__ void __launch_bounds__(1024) batch_faces_kernel(BatchArgs a) {
+  SlotState& S = a.slots[blockIdx.x];
+  const int k = a.it->k;
+  if (!S.done) {
+    const float* ls = a.fpool + S.seg_off;
+    faces_block(S.K, S.dim, a.max_faces, a.capacity, a.margin, ls, ls + S.dim, a.fpool + S.col_off,
+                a.fpool + S.col_off + (int64_t)a.num_particles * S.dim, a.fpool + S.dist_off, a.fpool + S.a_off,
+                a.fpool + S.b_off, &S.nf, &S.cnt);
+    if (threadIdx.x == 0) {
+      S.iters = k + 1;
+      S.status = S.cnt.status;
+      if (k + 1 >= a.max_iters) S.done = 1;
+    }
+  }
+  if (threadIdx.x == 0 && !S.done) atomicAdd(&a.it->active, 1);
+}
+
+__global__ void batch_step_kernel(BatchIter* it) {
+  it->last_active = it->active;
+  it->active = 0;
+  it->k += 1;
+}
+
+}  // namespace csd
+
+// --------------------------------------------------------------------- handle
+struct csd_batch_s {
+  int device = 0;
+  std::vector<csd_plant_t> plants;
+  csd_eizo_options_t opt{};
+  int max_slots = 0, capacity = 0, n_max = 0, max_dim = 0;
+  bool sm = true;
+  int static_floats = 0;
+  size_t check_smem = 0;
+  int check_grid = 0, bisect_grid = 0;
+  int cfg_per_item = 64, part_per_item = 8;
+  std::vector<int> n_tab, m_tab;
+  std::vector<float> thr_tab;
+  csd::DevBuf plants_dev, slots_dev, tabs, fpool, bpool, iter;
+  std::vector<csd::SlotState> host_slots;
+  cudaGraphExec_t graph = nullptr;
+  int graph_slots = -1;
+  cudaStream_t graph_stream = nullptr;
+  csd::BatchIter* host_iter = nullptr;
+  ~csd_batch_s() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (graph_stream) cudaStreamDestroy(graph_stream);
+    if (host_iter) cudaFreeHost(host_iter);
+  }
+};
+
+using namespace csd;
+
+namespace {
+
+csd_status_t build_graph(csd_batch_s* h, int num_slots, const BatchArgs& a) {
+  if (h->graph && h->graph_slots == num_slots) return CSD_OK;
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  cudaStream_t s = h->graph_stream;
+  cudaGraph_t g = nullptr;
+  CSD_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  const int64_t chains = (int64_t)num_slots * h->n_max;
+  batch_sample_kernel<<<(unsigned)((chains + 127) / 128), 128, 0, s>>>(a);
+  if (h->sm)
+    batch_check_kernel<true><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->cfg_per_item,
+                                                                                      h->static_floats);
+  else
+    batch_check_kernel<false><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->cfg_per_item, 0);
+  batch_compact_kernel<<<num_slots, 1024, 0, s>>>(a);
+  if (h->sm)
+    batch_bisect_kernel<true><<<h->bisect_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->part_per_item,
+                                                                                        h->static_floats);
+  else
+    batch_bisect_kernel<false><<<h->bisect_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->part_per_item, 0);
+  batch_faces_kernel<<<num_slots, 1024, 0, s>>>(a);
+  batch_step_kernel<<<1, 1, 0, s>>>(a.it);
+  cudaError_t e = cudaStreamEndCapture(s, &g);
+  if (e != cudaSuccess) {
+    set_error(std::string("graph capture failed: ") + cudaGetErrorString(e));
+    return CSD_ERR_CUDA;
+  }
+  e = cudaGraphInstantiate(&h->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    set_error(std::string("graph instantiation failed: ") + cudaGetErrorString(e));
+    return CSD_ERR_CUDA;
+  }
+  h->graph_slots = num_slots;
+  return CSD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+csd_status_t csd_batch_create(const csd_plant_t* plants, int32_t num_plants, int32_t max_slots,
+                              const csd_eizo_options_t* o, int32_t face_capacity, csd_batch_t* out) {
+  CSD_CHECK(plants && num_plants > 0 && max_slots > 0 && o && out && face_capacity > 0, CSD_ERR_INVALID,
+            "bad batch arguments");
+  *out = nullptr;
+  CSD_CHECK(o->num_particles >= 1 && o->max_iterations >= 1, CSD_ERR_INVALID,
+            "num_particles and max_iterations must be positive");
+  CSD_CHECK(o->tau > 0.f && o->tau < 1.f && o->epsilon > 0.f && o->delta > 0.f, CSD_ERR_INVALID,
+            "bad epsilon/delta/tau");
+  std::unique_ptr<csd_batch_s> h(new csd_batch_s());
+  h->device = plants[0]->device;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != h->device) cudaSetDevice(h->device);
+  struct Restore {
+    int cur, dev;
+    ~Restore() {
+      if (cur != dev) cudaSetDevice(cur);
+    }
+  } restore{cur, h->device};
+  h->opt = *o;
+  h->max_slots = max_slots;
+  h->capacity = face_capacity;
+  int max_static = 0, max_wf = 0;
+  std::vector<DevPlant> dps;
+  for (int i = 0; i < num_plants; ++i) {
+    CSD_CHECK(plants[i] && plants[i]->device == h->device, CSD_ERR_INVALID, "plants must live on one device");
+    h->plants.push_back(plants[i]);
+    dps.push_back(plants[i]->dp);
+    CSD_CHECK(plants[i]->dp.dim >= 1 && plants[i]->dp.dim <= kMaxDim, CSD_ERR_DIMENSION, "plant dimension must be in [1, 16]");
+    h->max_dim = std::max(h->max_dim, plants[i]->dp.dim);
+    max_static = std::max(max_static, plants[i]->dp.static_bytes);
+    max_wf = std::max(max_wf, warp_floats(plants[i]->dp));
+  }
+  // iteration tables (cuda_edge_inflation_zero_order.cu:113-119)
+  for (uint32_t k = 0; k < o->max_iterations; ++k) {
+    float delta_k = (float)(6 * o->delta / (M_PI * M_PI * (k + 1) * (k + 1)));
+    uint32_t M = csd_num_samples_unadaptive(o->epsilon, delta_k, o->tau);
+    h->m_tab.push_back((int)M);
+    h->n_tab.push_back((int)std::max(M, o->num_particles));
+    h->thr_tab.push_back((1 - o->tau) * o->epsilon * M);
+  }
+  h->n_max = *std::max_element(h->n_tab.begin(), h->n_tab.end());
+  h->sm = max_static <= kStaticSmemLimit;
+  h->static_floats = h->sm ? max_static / 4 : 0;
+  h->check_smem = (size_t)max_wf * sizeof(float) * kWarpsPerBlock + (h->sm ? (size_t)max_static : 0);
+  csd_status_t s;
+  int g1 = 0, g2 = 0;
+  if (h->sm) {
+    if ((s = grid_for(batch_check_kernel<true>, h->check_smem, 1ll << 40, &g1, kWarpsPerBlock))) return s;
+    if ((s = grid_for(batch_bisect_kernel<true>, h->check_smem, 1ll << 40, &g2, kWarpsPerBlock))) return s;
+  } else {
+    if ((s = grid_for(batch_check_kernel<false>, h->check_smem, 1ll << 40, &g1, kWarpsPerBlock))) return s;
+    if ((s = grid_for(batch_bisect_kernel<false>, h->check_smem, 1ll << 40, &g2, kWarpsPerBlock))) return s;
+  }
+  h->check_grid = g1;
+  h->bisect_grid = g2;
+  // buffers
+  const size_t D = (size_t)h->max_dim, np = o->num_particles, cap = (size_t)face_capacity;
+  const size_t per_slot_f = cap * D + cap + 2 * D + (size_t)h->n_max * D + 2 * np * D + np;
+  if ((s = h->plants_dev.reserve(dps.size() * sizeof(DevPlant))) || (s = h->slots_dev.reserve(max_slots * sizeof(SlotState))) ||
+      (s = h->tabs.reserve(h->n_tab.size() * 12 + 64)) || (s = h->fpool.reserve(per_slot_f * max_slots * 4 + 256)) ||
+      (s = h->bpool.reserve((size_t)h->n_max * max_slots + 256)) || (s = h->iter.reserve(sizeof(BatchIter))))
+    return s;
+  CSD_CUDA_TRY(cudaMemcpy(h->plants_dev.ptr, dps.data(), dps.size() * sizeof(DevPlant), cudaMemcpyHostToDevice));
+  int* t = h->tabs.as<int>();
+  const size_t K = h->n_tab.size();
+  CSD_CUDA_TRY(cudaMemcpy(t, h->n_tab.data(), K * 4, cudaMemcpyHostToDevice));
+  CSD_CUDA_TRY(cudaMemcpy(t + K, h->m_tab.data(), K * 4, cudaMemcpyHostToDevice));
+  CSD_CUDA_TRY(cudaMemcpy(t + 2 * K, h->thr_tab.data(), K * 4, cudaMemcpyHostToDevice));
+  CSD_CUDA_TRY(cudaStreamCreateWithFlags(&h->graph_stream, cudaStreamNonBlocking));
+  CSD_CUDA_TRY(cudaMallocHost((void**)&h->host_iter, sizeof(BatchIter)));
+  *out = h.release();
+  return CSD_OK;
+}
+
+csd_status_t csd_batch_destroy(csd_batch_t h) {
+  if (!h) return CSD_OK;
+  int cur = 0, dev = h->device;
+  cudaGetDevice(&cur);
+  if (cur != dev) cudaSetDevice(dev);
+  delete h;
+  if (cur != dev) cudaSetDevice(cur);
+  return CSD_OK;
+}
+
+csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_plant, const float* starts,
+                               const float* ends, const float* domain_A, const float* domain_b,
+                               const int32_t* domain_face_offsets, float* A_out, float* b_out, int32_t* num_faces,
+                               int32_t* num_iterations, float* device_ms) {
+  CSD_CHECK(h && n >= 0 && n <= h->max_slots, CSD_ERR_INVALID, "bad slot count");
+  if (n == 0) return CSD_OK;
+  CSD_CHECK(slot_plant && starts && ends && domain_A && domain_b && domain_face_offsets && A_out && b_out && num_faces,
+            CSD_ERR_INVALID, "null argument");
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != h->device) cudaSetDevice(h->device);
+  struct Restore {
+    int cur, dev;
+    ~Restore() {
+      if (cur != dev) cudaSetDevice(cur);
+    }
+  } restore{cur, h->device};
+  const size_t D = (size_t)h->max_dim, np = h->opt.num_particles, cap = (size_t)h->capacity;
+  const size_t per_slot_f = cap * D + cap + 2 * D + (size_t)h->n_max * D + 2 * np * D + np;
+  std::vector<SlotState> slots(n);
+  size_t qoff = 0, arow = 0;
+  cudaStream_t st = h->graph_stream;
+  for (int i = 0; i < n; ++i) {
+    const int pi = slot_plant[i];
+    CSD_CHECK(pi >= 0 && pi < (int)h->plants.size(), CSD_ERR_INVALID, "slot plant index out of range");
+    const int d = h->plants[pi]->dp.dim;
+    const int f0 = domain_face_offsets[i], f1 = domain_face_offsets[i + 1];
+    CSD_CHECK(f0 >= 0 && f1 >= f0, CSD_ERR_INVALID, "bad domain face offsets");
+    CSD_CHECK(f1 - f0 <= 0.9 * h->capacity, CSD_ERR_CAPACITY, "domain uses almost all of the face capacity");
+    // the segment must lie in the domain (CudaEdgeInflator::inflateEdge asserts it)
+    for (int sidx = 0; sidx < 2; ++sidx) {
+      const float* x = (sidx ? ends : starts) + qoff;
+      for (int f = 0; f < f1 - f0; ++f) {
+        float ax = 0.f;
+        for (int k = 0; k < d; ++k) ax += domain_A[arow + (size_t)f * d + k] * x[k];
+        if (!(ax <= domain_b[f0 + f] + 1e-9f)) {
+          set_error("slot " + std::to_string(i) + ": line segment endpoints must lie in the domain");
+          return CSD_ERR_NOT_CONTAINED;
+        }
+      }
+    }
+    arow += (size_t)(f1 - f0) * d;
+    SlotState& S = slots[i];
+    S = SlotState{};
+    S.plant = pi;
+    S.dim = d;
+    S.domain_faces = f1 - f0;
+    S.nf = f1 - f0;
+    const long long base = (long long)(per_slot_f * i);
+    S.a_off = base;
+    S.b_off = S.a_off + (long long)(cap * D);
+    S.seg_off = S.b_off + (long long)cap;
+    S.smp_off = S.seg_off + (long long)(2 * D);
+    S.col_off = S.smp_off + (long long)((size_t)h->n_max * D);
+    S.dist_off = S.col_off + (long long)(2 * np * D);
+    S.flag_off = (long long)h->n_max * i;
+    qoff += d;
+  }
+  // domain rows of slot i are rows [f0, f1) of domain_A with that slot's dim
+  {
+    size_t arow = 0;  // float offset into domain_A
+    for (int i = 0; i < n; ++i) {
+      const int d = slots[i].dim;
+      const int F = slots[i].nf;
+      const int f0 = domain_face_offsets[i];
+      (void)f0;
+      CSD_CUDA_TRY(cudaMemcpyAsync(h->fpool.as<float>() + slots[i].a_off, domain_A + arow, (size_t)F * d * 4,
+                                   cudaMemcpyHostToDevice, st));
+      CSD_CUDA_TRY(cudaMemcpyAsync(h->fpool.as<float>() + slots[i].b_off, domain_b + domain_face_offsets[i],
+                                   (size_t)F * 4, cudaMemcpyHostToDevice, st));
+      arow += (size_t)F * d;
+    }
+    size_t q = 0;
+    for (int i = 0; i < n; ++i) {
+      const int d = slots[i].dim;
+      CSD_CUDA_TRY(cudaMemcpyAsync(h->fpool.as<float>() + slots[i].seg_off, starts + q, d * 4,
+                                   cudaMemcpyHostToDevice, st));
+      CSD_CUDA_TRY(cudaMemcpyAsync(h->fpool.as<float>() + slots[i].seg_off + d, ends + q, d * 4,
+                                   cudaMemcpyHostToDevice, st));
+      q += d;
+    }
+  }
+  CSD_CUDA_TRY(cudaMemcpyAsync(h->slots_dev.ptr, slots.data(), n * sizeof(SlotState), cudaMemcpyHostToDevice, st));
+  BatchIter zero{};
+  *h->host_iter = zero;
+  CSD_CUDA_TRY(cudaMemcpyAsync(h->iter.ptr, h->host_iter, sizeof(BatchIter), cudaMemcpyHostToDevice, st));
+  BatchArgs a{};
+  a.slots = h->slots_dev.as<SlotState>();
+  a.plants = h->plants_dev.as<DevPlant>();
+  a.num_slots = n;
+  a.n_max = h->n_max;
+  a.max_iters = (int)h->opt.max_iterations;
+  a.num_particles = (int)h->opt.num_particles;
+  a.mixing = (int)h->opt.mixing_steps;
+  a.bisection = (int)h->opt.bisection_steps;
+  a.max_faces = (int)h->opt.max_hyperplanes_per_iteration;
+  a.capacity = h->capacity;
+  a.margin = h->opt.configuration_margin;
+  a.k0 = (uint32_t)h->opt.seed;
+  a.k1 = (uint32_t)(h->opt.seed >> 32);
+  const size_t K = h->n_tab.size();
+  a.n_tab = h->tabs.as<int>();
+  a.m_tab = h->tabs.as<int>() + K;
+  a.thr_tab = reinterpret_cast<const float*>(h->tabs.as<int>() + 2 * K);
+  a.fpool = h->fpool.as<float>();
+  a.bpool = h->bpool.as<uint8_t>();
+  a.it = h->iter.as<BatchIter>();
+  csd_status_t s = build_graph(h, n, a);
+  if (s) return s;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (device_ms) {
+    CSD_CUDA_TRY(cudaEventCreate(&ev0));
+    CSD_CUDA_TRY(cudaEventCreate(&ev1));
+    CSD_CUDA_TRY(cudaEventRecord(ev0, st));
+  }
+  for (uint32_t k = 0; k < h->opt.max_iterations; ++k) {
+    CSD_CUDA_TRY(cudaGraphLaunch(h->graph, st));
+    CSD_CUDA_TRY(cudaMemcpyAsync(h->host_iter, h->iter.ptr, sizeof(BatchIter), cudaMemcpyDeviceToHost, st));
+    CSD_CUDA_TRY(cudaStreamSynchronize(st));
+    if (h->host_iter->last_active == 0) break;
+  }
+  if (device_ms) {
+    CSD_CUDA_TRY(cudaEventRecord(ev1, st));
+    CSD_CUDA_TRY(cudaEventSynchronize(ev1));
+    cudaEventElapsedTime(device_ms, ev0, ev1);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+  }
+  CSD_CUDA_TRY(cudaMemcpyAsync(slots.data(), h->slots_dev.ptr, n * sizeof(SlotState), cudaMemcpyDeviceToHost, st));
+  CSD_CUDA_TRY(cudaStreamSynchronize(st));
+  size_t aoff = 0;
+  for (int i = 0; i < n; ++i) {
+    const SlotState& S = slots[i];
+    if (S.status == 2) {
+      set_error("Max face count exceeded in slot " + std::to_string(i));
+      return CSD_ERR_CAPACITY;
+    }
+    num_faces[i] = S.nf;
+    if (num_iterations) num_iterations[i] = S.iters;
+    CSD_CUDA_TRY(cudaMemcpyAsync(A_out + aoff, h->fpool.as<float>() + S.a_off, (size_t)S.nf * S.dim * 4,
+                                 cudaMemcpyDeviceToHost, st));
+    CSD_CUDA_TRY(cudaMemcpyAsync(b_out + (size_t)i * h->capacity, h->fpool.as<float>() + S.b_off, (size_t)S.nf * 4,
+                                 cudaMemcpyDeviceToHost, st));
+    aoff += (size_t)h->capacity * S.dim;
+  }
+  CSD_CUDA_TRY(cudaStreamSynchronize(st));
+  return CSD_OK;
+}
+
+}  // extern "C"

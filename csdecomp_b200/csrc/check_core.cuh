@@ -49,8 +49,10 @@ static __device__ __forceinline__ unsigned smem_addr(const void* p) {
 }
 
 // Copies the static tables (p.static_bytes, a multiple of 16) into dst with
-// one cp.async.bulk per 64 KiB chunk completing on an mbarrier. Returns false
-// (and sets p.status) if the wait does not complete within kSpinLimit polls.
+// one cp.async.bulk per 64 KiB chunk completing on an mbarrier, then
+// invalidates the barrier so a later call can stage another plant. Returns
+// false (and sets p.status) if the wait does not complete within kSpinLimit
+// polls. Every thread of the block must call it.
 static __device__ bool stage_statics(const DevPlant& p, float4* dst, uint64_t* bar) {
   const unsigned bytes = (unsigned)p.static_bytes;
   if (bytes == 0) return true;
@@ -90,6 +92,8 @@ static __device__ bool stage_statics(const DevPlant& p, float4* dst, uint64_t* b
           : "memory");
     return false;
   }
+  __syncthreads();  // every thread has seen the phase complete: the barrier can be reused
+  if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
   return true;
 }
 

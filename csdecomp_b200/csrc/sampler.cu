@@ -13,6 +13,7 @@
 
 #include "csd_internal.h"
 #include "csd_rng.cuh"
+#include "sampler_core.cuh"
 
 namespace csd {
 
@@ -30,48 +31,11 @@ __global__ void __launch_bounds__(128) hit_and_run_kernel(const float* __restric
   const int s = (int)(i % S);
   const int f0 = face_off ? face_off[poly] : 0;
   const int F = face_off ? face_off[poly + 1] - f0 : *num_faces_dev;
-  const float* Ap = A + (int64_t)f0 * dim;
-  const float* bp = b + f0;
-  float x[MAXD], dir[MAXD];
+  float x[MAXD];
 #pragma unroll
-  for (int k = 0; k < MAXD; ++k) {
-    x[k] = k < dim ? starts[(int64_t)poly * dim + k] : 0.f;
-    dir[k] = 0.f;
-  }
-  bool ok = true;
-  for (int step = 0; step < mixing; ++step) {
-    float ut;
-    step_draws<MAXD>(k0, k1, (uint32_t)s, stream_base + (uint32_t)poly, (uint32_t)step, dim, dir, &ut);
-    float tmax = FLT_MAX, tmin = -FLT_MAX;
-    for (int f = 0; f < F; ++f) {
-      const float* a = Ap + (int64_t)f * dim;
-      float ax = __fmul_rn(a[0], x[0]);
-      float ad = __fmul_rn(a[0], dir[0]);
-#pragma unroll
-      for (int k = 1; k < MAXD; ++k) {
-        if (k < dim) {
-          float ak = a[k];
-          ax = __fmaf_rn(ak, x[k], ax);
-          ad = __fmaf_rn(ak, dir[k], ad);
-        }
-      }
-      float lb = __fsub_rn(bp[f], ax);
-      if (ad < 0.0f)
-        tmin = fmaxf(tmin, __fdiv_rn(lb, ad));
-      else if (ad > 0.0f)
-        tmax = fminf(tmax, __fdiv_rn(lb, ad));
-    }
-    if (isinf(tmax) || isinf(tmin) || tmax < tmin) {
-      ok = false;
-      break;
-    }
-    double th = __dadd_rn(__dmul_rn((double)ut, __dsub_rn(__dmul_rn(0.999999, (double)tmax), (double)tmin)),
-                          (double)tmin);
-    float theta = __double2float_rn(th);
-#pragma unroll
-    for (int k = 0; k < MAXD; ++k)
-      if (k < dim) x[k] = __fmaf_rn(theta, dir[k], x[k]);
-  }
+  for (int k = 0; k < MAXD; ++k) x[k] = k < dim ? starts[(int64_t)poly * dim + k] : 0.f;
+  const bool ok = run_chain<MAXD>(A + (int64_t)f0 * dim, b + f0, F, dim, mixing, k0, k1, (uint32_t)s,
+                                  stream_base + (uint32_t)poly, x);
   if (!ok && num_failed) atomicAdd(num_failed, 1);
   // a chain whose line search fails writes NaN, or (fail_keep) its start point
   float* dst = out + i * dim;

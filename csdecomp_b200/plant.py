@@ -368,32 +368,32 @@ def _path_all_fixed(tree: KinematicTree, a: int, b: int, depth: List[int]) -> bo
 def compute_collision_pairs(tree: KinematicTree, geoms: List[CollisionGeometry]) -> List[Tuple[int, int]]:
     """Pair filter of urdf_parser.cpp:546-613: every (A<B) pair with at least one
     robot geometry, excluding same-link, parent/child ("successive") links and
-    links connected by fixed joints only."""
+    links connected by fixed joints only. Vectorised over geometry pairs; the
+    fixed-path test is tabulated per link pair."""
     n = len(tree.links)
     depth = [0] * n
     for j in tree.joint_traversal_sequence:
         jt = tree.joints[j]
         depth[jt.child_link] = depth[jt.parent_link] + 1
-    parent_of = []
-    for g in geoms:
-        pj = tree.links[g.link_index].parent_joint
-        parent_of.append(tree.joints[pj].parent_link if pj >= 0 else -1)
-    pairs = []
     G = len(geoms)
-    for a in range(G - 1):
-        ga = geoms[a]
-        for b in range(a + 1, G):
-            gb = geoms[b]
-            if ga.group == CollisionGroup.WORLD and gb.group == CollisionGroup.WORLD:
-                continue
-            not_successive = parent_of[a] != gb.link_index and parent_of[b] != ga.link_index
-            not_same = ga.link_index != gb.link_index
-            if not (not_successive and not_same):
-                continue
-            if _path_all_fixed(tree, ga.link_index, gb.link_index, depth):
-                continue
-            pairs.append((a, b))
-    return pairs
+    if G < 2:
+        return []
+    link = np.array([g.link_index for g in geoms], np.int64)
+    world = np.array([g.group == CollisionGroup.WORLD for g in geoms])
+    parent_of = np.array([tree.joints[tree.links[g.link_index].parent_joint].parent_link
+                          if tree.links[g.link_index].parent_joint >= 0 else -1 for g in geoms], np.int64)
+    used = sorted(set(link.tolist()))
+    fixed = np.zeros((n, n), bool)
+    for la in used:
+        for lb in used:
+            fixed[la, lb] = _path_all_fixed(tree, la, lb, depth)
+    ia, ib = np.triu_indices(G, k=1)
+    la, lb = link[ia], link[ib]
+    keep = ~(world[ia] & world[ib])
+    keep &= (parent_of[ia] != lb) & (parent_of[ib] != la)
+    keep &= la != lb
+    keep &= ~fixed[la, lb]
+    return list(zip(ia[keep].tolist(), ib[keep].tolist()))
 
 
 def build_plant(tree: KinematicTree, geoms: List[CollisionGeometry],

@@ -106,13 +106,14 @@ def _add_arm(tree: KinematicTree, geoms: List[CollisionGeometry], rng: np.random
 
 
 def _world_primitives(rng: np.random.Generator, obstacle_link: int, num_boxes: int, num_spheres: int,
-                      keepout: float) -> List[CollisionGeometry]:
+                      keepout: float, bases: Optional[List[np.ndarray]] = None) -> List[CollisionGeometry]:
     out = []
+    bases = bases or [np.zeros(3)]
 
     def centre(extent: float) -> np.ndarray:
         while True:
             c = rng.uniform(-1.0, 1.0, 3)
-            if keepout <= 0 or np.linalg.norm(c) - extent > keepout:
+            if keepout <= 0 or all(np.linalg.norm(c - b) - extent > keepout for b in bases):
                 return c
 
     for _ in range(num_boxes):
@@ -130,7 +131,7 @@ def _world_primitives(rng: np.random.Generator, obstacle_link: int, num_boxes: i
 
 def arm_scene(seed: int, num_spheres: int = 40, num_capsules: int = 0, num_world_boxes: int = 20,
               num_world_spheres: int = 0, arms: int = 1, dof_per_arm: int = 7, keepout: float = 0.0,
-              description: str = "") -> Scene:
+              description: str = "", arm_spacing: float = 0.6) -> Scene:
     """One (arms=1) or two (arms=2, on a welded base) random revolute arms in a
     field of world primitives. keepout > 0 rejects world primitives within that
     distance of the base."""
@@ -140,18 +141,20 @@ def arm_scene(seed: int, num_spheres: int = 40, num_capsules: int = 0, num_world
     geoms: List[CollisionGeometry] = []
     if arms == 1:
         _add_arm(tree, geoms, rng, 0, "", dof_per_arm, num_spheres, num_capsules)
-    else:
+    bases = [np.zeros(3)]
+    if arms != 1:
+        bases = [np.array([0.0, (a - (arms - 1) / 2.0) * arm_spacing, 0.0]) for a in range(arms)]
         base = tree.add_link(Link(name="base"))
         tree.add_joint(Joint(name="base_weld", type=JointType.FIXED, parent_link=0, child_link=base))
         for a in range(arms):
             mount = tree.add_link(Link(name=f"mount{a}"))
-            y = (a - (arms - 1) / 2.0) * 0.6
+            y = (a - (arms - 1) / 2.0) * arm_spacing
             tree.add_joint(Joint(name=f"mount{a}_weld", type=JointType.FIXED, parent_link=base, child_link=mount,
                                  X_PL_J=make_transform(np.eye(3), [0.0, y, 0.0])))
             _add_arm(tree, geoms, rng, mount, f"arm{a}_", dof_per_arm, num_spheres // arms, num_capsules // arms)
     obst = tree.add_link(Link(name="obstacles"))
     tree.add_joint(Joint(name="obstacles_weld", type=JointType.FIXED, parent_link=0, child_link=obst))
-    geoms.extend(_world_primitives(rng, obst, num_world_boxes, num_world_spheres, keepout))
+    geoms.extend(_world_primitives(rng, obst, num_world_boxes, num_world_spheres, keepout, bases))
     tree.finalize()
     plant, insp = build_plant(tree, geoms)
     return Scene(plant, insp, tree, seed, description)
@@ -173,3 +176,28 @@ def edge_check_scene(seed: int = EDGE_CHECK_SEED, keepout: float = 0.0) -> Scene
     200 world primitives (100 boxes, 100 spheres)."""
     return arm_scene(seed, num_spheres=80, num_capsules=4, num_world_boxes=100, num_world_spheres=100,
                      keepout=keepout, description="7-DOF arm, 80 spheres + 4 capsules, 100 boxes + 100 spheres")
+
+
+BATCH_SEED = 4000
+
+
+def batch_scene(i: int, seed: int, keepout: float = 0.8) -> Scene:
+    """Scene i of the batched-EI-ZO workload: even i a 7-DOF arm (80 spheres + 4
+    capsules), odd i a 14-DOF two-arm plant (bases 1.4 m apart, 2 x (40
+    spheres + 2 capsules)); U{50..400} world primitives (half boxes, half
+    spheres) placed as in edge_check_scene, clear of every arm base."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(50, 401))
+    nb = n // 2
+    s = int(rng.integers(1 << 30))
+    if i % 2 == 0:
+        return arm_scene(s, num_spheres=80, num_capsules=4, num_world_boxes=nb, num_world_spheres=n - nb,
+                         keepout=keepout, description=f"7-DOF arm, {n} world primitives")
+    return arm_scene(s, num_spheres=80, num_capsules=4, num_world_boxes=nb, num_world_spheres=n - nb, arms=2,
+                     keepout=keepout, arm_spacing=1.4, description=f"14-DOF two-arm, {n} world primitives")
+
+
+def batch_scenes(count: int = 256, seed: int = BATCH_SEED, keepout: float = 0.8) -> List[Scene]:
+    """`count` scenes for the batched-EI-ZO workload (see batch_scene)."""
+    rng = np.random.default_rng(seed)
+    return [batch_scene(i, int(rng.integers(1 << 30)), keepout) for i in range(count)]

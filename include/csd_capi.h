@@ -198,6 +198,29 @@ csd_status_t csd_eizo(csd_plant_t plant, const float* line_start, const float* l
                       int32_t* num_faces, csd_eizo_iteration_info_t* info, int32_t info_capacity,
                       int32_t* num_iterations);
 
+/* Batched EI-ZO (no counterpart in the reference, which inflates one edge per
+ * executeEizo call, cuda_edge_inflation_zero_order.cu:94-339): up to max_slots
+ * inflations, each with its own plant (one of `plants`, which must outlive the
+ * batch), segment and domain, advance together through one persistent kernel
+ * per stage, replayed as a CUDA graph. Each slot computes exactly what
+ * csd_inflator_inflate computes for the same inputs. No voxels. */
+typedef struct csd_batch_s* csd_batch_t;
+csd_status_t csd_batch_create(const csd_plant_t* plants, int32_t num_plants, int32_t max_slots,
+                              const csd_eizo_options_t* options, int32_t face_capacity, csd_batch_t* out);
+/* n slots: slot i uses plants[slot_plant[i]] (dim d_i); starts/ends hold the
+ * segments back to back (d_i floats each); the domain of slot i is rows
+ * [domain_face_offsets[i], domain_face_offsets[i+1]) of domain_b and the same
+ * rows of domain_A, stored back to back with d_i floats per row. Region i is
+ * written to A_out at float offset sum_{j<i} face_capacity * d_j (row-major,
+ * d_i floats per row) and b_out at i * face_capacity; num_faces[i] rows. All
+ * arrays are host memory; the call synchronises before returning. device_ms
+ * (optional) receives the GPU time from the first to the last iteration. */
+csd_status_t csd_batch_inflate(csd_batch_t batch, int32_t n, const int32_t* slot_plant, const float* starts,
+                               const float* ends, const float* domain_A, const float* domain_b,
+                               const int32_t* domain_face_offsets, float* A_out, float* b_out, int32_t* num_faces,
+                               int32_t* num_iterations, float* device_ms);
+csd_status_t csd_batch_destroy(csd_batch_t batch);
+
 /* Allocation-free EI-ZO (no counterpart in the reference). Same inputs,
  * outputs and results as csd_eizo, for callers that must not allocate device
  * memory while they run (a real-time loop that owns a fixed memory budget, a

@@ -1,0 +1,66 @@
+"""Batched EI-ZO: every slot equals the single-inflation region bit for bit
+(7-DOF and 14-DOF plants mixed in one batch)."""
+import numpy as np
+import pytest
+
+import csdecomp_b200 as csd
+from csdecomp_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def free_edges(sc, count, length, seed):
+    rng = np.random.default_rng(seed)
+    q = sc.random_configs(4000, seed)
+    free = q[csd.CheckCollisionFreeCuda(q.T, sc.plant) == 1]
+    out = []
+    for q0 in free:
+        d = rng.normal(size=q0.size)
+        d /= np.linalg.norm(d)
+        q1 = (q0 + length * d).astype(np.float32)
+        if np.all(np.abs(q1) < np.pi) and csd.CheckEdgeCollisionFree(q0, q1, sc.plant):
+            out.append((q0.copy(), q1))
+            if len(out) == count:
+                break
+    assert len(out) == count
+    return out
+
+
+def box(sc):
+    d = csd.HPolyhedron()
+    d.MakeBox(sc.lower(), sc.upper())
+    return d
+
+
+def test_batch_matches_single_inflations():
+    s7 = scenes.arm_scene(31, num_spheres=40, num_capsules=2, num_world_boxes=30, num_world_spheres=30, keepout=0.8)
+    s14 = scenes.arm_scene(32, num_spheres=40, num_capsules=2, num_world_boxes=20, num_world_spheres=20, arms=2,
+                           keepout=0.9, arm_spacing=1.4)
+    opt = csd.EizoOptions(num_particles=600, mixing_steps=20, max_iterations=40)
+    cap = 300
+    e7 = free_edges(s7, 3, 0.3, 1)
+    e14 = free_edges(s14, 3, 0.3, 2)
+    slots = [0, 1, 0, 1, 0, 1]
+    edges = [e7[0], e14[0], e7[1], e14[1], e7[2], e14[2]]
+    scn = [s7, s14]
+    batch = csd.BatchedEdgeInflator([s7.plant, s14.plant], opt, max_slots=8, face_capacity=cap)
+    got = batch.inflate(slots, [e[0] for e in edges], [e[1] for e in edges], [box(scn[i]) for i in slots])
+    for i, (pi, e) in enumerate(zip(slots, edges)):
+        inf = csd.CudaEdgeInflator(scn[pi].plant, scn[pi].inspector.robot_geometry_ids, opt, box(scn[pi]),
+                                   face_capacity=cap)
+        ref = inf.inflateEdge(e[0], e[1], None, 0.0, verbose=False)
+        np.testing.assert_array_equal(got[i].A(), ref.A(), err_msg=f"slot {i}")
+        np.testing.assert_array_equal(got[i].b(), ref.b(), err_msg=f"slot {i}")
+        assert batch.last_iterations[i] == len(inf.last_info.iteration_info)
+    # reuse with fewer slots
+    got2 = batch.inflate(slots[:2], [e[0] for e in edges[:2]], [e[1] for e in edges[:2]],
+                         [box(scn[i]) for i in slots[:2]])
+    np.testing.assert_array_equal(got2[1].A(), got[1].A())
+
+
+def test_batch_rejects_segment_outside_domain():
+    s7 = scenes.arm_scene(31, num_spheres=20, num_world_boxes=10, keepout=0.8)
+    batch = csd.BatchedEdgeInflator([s7.plant], csd.EizoOptions(num_particles=100, max_iterations=5), 2, 100)
+    far = np.full(7, 5.0, np.float32)
+    with pytest.raises(RuntimeError):
+        batch.inflate([0], [far], [far], [box(s7)])
