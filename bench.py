@@ -1,13 +1,14 @@
 #!/usr/bin/env python
-"""Benchmark: EI-ZO regions/s on one B200 (plain GPU form) on the synthetic
-7-DOF / 200-primitive scene, with the fused collision kernel's FP32 roofline
-and the CPU oracle's EI-ZO on the host cores beside it.
+"""Benchmark: EI-ZO regions/s and configs/s on one B200, batched form: 256
+inflations per step on 256 seeded scenes (7-DOF and 14-DOF plants mixed), the
+plain GPU form (one inflation per call) on the same inputs beside it, the
+collision kernel's FP32 roofline and the CPU oracle's EI-ZO on the host cores.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {b200,reference}]
 
-One step = one EI-ZO inflation (CudaEdgeInflator.inflateEdge) of a distinct
-seed edge. N > 1 (torchrun): every rank inflates its own seed edges (weak
-scaling, no collective on the data path); rank 0 prints one JSON line.
+One step = one BatchedEdgeInflator.inflate of 256 seed edges, one per scene.
+N > 1 (torchrun): every rank inflates its own 256 scenes (weak scaling, no
+collective on the data path); rank 0 prints one JSON line.
 """
 from __future__ import annotations
 
@@ -25,42 +26,56 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "EI-ZO regions/s and configs/s on 1 B200: surrogate+batched vs plain GPU, ε=0.01"
-WORKLOAD = ("single EI-ZO inflation, plain GPU form: 7-DOF arm (80 spheres + 4 capsules), 200 world primitives "
-            "(100 boxes + 100 spheres, centres U[-1,1]^3, 0.8 m base keep-out), seed edges U[0.1,0.5] rad, "
-            "2000 particles, mixing 50, 9 bisection steps, <=10 faces/iteration, eps=0.01, delta=0.05, tau=0.5")
+NUM_SLOTS = 256
+FACE_CAPACITY = 4000          # hpolyhedron.h:5 default region capacity
 EIZO_KW = dict(num_particles=2000, mixing_steps=50, bisection_steps=9, max_hyperplanes_per_iteration=10,
                epsilon=0.01, delta=0.05, tau=0.5, max_iterations=500, configuration_margin=0.01, seed=1337)
+WORKLOAD = ("batched EI-ZO: 256 inflations per step, one per seeded scene (even: 7-DOF arm, 80 spheres + 4 "
+            "capsules; odd: 14-DOF two-arm plant, 2 x (40 spheres + 2 capsules)); U{50..400} world primitives per "
+            "scene (half boxes, half spheres, centres U[-1,1]^3, 0.8 m keep-out around each base); seed edges "
+            "U[0.05,1.0] rad in free space; domain = joint-limit box; 2000 particles, mixing 50, 9 bisection steps, "
+            "<=10 faces/iteration, eps=0.01, delta=0.05, tau=0.5")
 SEED_EDGE_SEED = 3000
+RANK_SCENE_STRIDE = 7919
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     return ap.parse_args()
 
 
-def seed_edges(scene, count: int, check_points, check_edge):
-    """Seeded pool of free seed edges: a free q0, a direction uniform on the
-    sphere, length U[0.1, 0.5] rad, accepted iff the edge lies in the joint
-    limits and is collision free (the reference's edge rule)."""
-    rng = np.random.default_rng(SEED_EDGE_SEED)
-    lo, hi = scene.lower(), scene.upper()
-    out = []
-    while len(out) < count:
-        q = scene.random_configs(4096, int(rng.integers(1 << 30)))
-        free = q[check_points(q) == 1]
-        for q0 in free:
-            d = rng.normal(size=q0.size)
-            d /= np.linalg.norm(d)
-            q1 = (q0 + rng.uniform(0.1, 0.5) * d).astype(np.float32)
-            if np.all(q1 > lo) and np.all(q1 < hi) and check_edge(q0, q1):
-                out.append((q0.copy(), q1))
-                if len(out) == count:
-                    break
-    return out
+def box_domain(scene):
+    d = scene.dim
+    A = np.zeros((2 * d, d), np.float32)
+    for i in range(d):
+        A[2 * i, i], A[2 * i + 1, i] = -1, 1
+    b = np.concatenate([[-scene.lower()[i], scene.upper()[i]] for i in range(d)]).astype(np.float32)
+    return A, b
+
+
+def workload(rank: int, count: int, edges_per_scene: int, make_checkers):
+    """`count` scenes of the batched workload with `edges_per_scene` free seed
+    edges each. Scenes come from the rank's seeded stream in order; a scene in
+    which 8 x 4096 uniform draws yield too few free seed edges is skipped (the
+    number skipped is reported)."""
+    from csdecomp_b200 import scenes
+    seeds = scenes.batch_scene_seeds(4 * count + 64, scenes.BATCH_SEED + RANK_SCENE_STRIDE * rank)
+    out, skipped = [], 0
+    for i, s in enumerate(seeds):
+        sc = scenes.batch_scene(i, s)
+        cp, ce = make_checkers(sc)
+        e = scenes.seed_edges(sc, edges_per_scene, SEED_EDGE_SEED + 101 * i + rank, cp, ce)
+        if len(e) < edges_per_scene:
+            skipped += 1
+            continue
+        out.append((sc, e))
+        if len(out) == count:
+            return out, skipped
+    raise RuntimeError("scene stream exhausted")
 
 
 class ClockSampler:
@@ -117,64 +132,65 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_eizo_baseline(scene, edges, nthreads: int):
+def oracle_checkers(nthreads: int):
+    from oracle import oracle as O
+
+    def make(sc):
+        return (lambda q: O.check_points(sc.plant, q, O.RULE_GPU, nthreads=nthreads),
+                lambda a, b: O.check_edges(sc.plant, a, b, nthreads=nthreads)[0])
+    return make
+
+
+def cpu_eizo(items, nthreads: int, budget_s: float):
+    """The oracle's restated executeEizo on (scene, edge) items until the time
+    budget runs out; returns (regions/s, regions, seconds)."""
     from csdecomp_b200.api import EizoOptions
     from oracle import oracle as O
-    d = scene.dim
-    A0 = np.zeros((2 * d, d), np.float32)
-    for i in range(d):
-        A0[2 * i, i], A0[2 * i + 1, i] = -1, 1
-    b0 = np.concatenate([[-scene.lower()[i], scene.upper()[i]] for i in range(d)]).astype(np.float32)
     opt = EizoOptions(**EIZO_KW)
     t0 = time.perf_counter()
     n = 0
-    for q0, q1 in edges:
-        O.eizo(scene.plant, q0, q1, A0, b0, opt, scene.inspector.robot_geometry_ids, nthreads=nthreads)
+    for sc, (q0, q1) in items:
+        A0, b0 = box_domain(sc)
+        O.eizo(sc.plant, q0, q1, A0, b0, opt, sc.inspector.robot_geometry_ids, capacity=FACE_CAPACITY,
+               nthreads=nthreads)
         n += 1
-        if time.perf_counter() - t0 > 20.0:
+        if time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
     return n / dt, n, dt
 
 
 def run_reference(args, rank):
+    """CPU arm: the oracle's EI-ZO (restating the reference's executeEizo) on
+    the host cores, one inflation per step, on the first W + K scenes of the
+    same workload with their first timed seed edge. A CPU inflation takes tens
+    of seconds, so warm-up stops after 30 s and the timed steps after 120 s;
+    the line reports how many inflations ran."""
     if rank != 0:
         return
-    from csdecomp_b200 import scenes
-    from oracle import oracle as O
-    scene = scenes.edge_check_scene(keepout=0.8)
     ncores = os.cpu_count() or 1
-    edges = seed_edges(scene, args.warmup + args.steps,
-                       lambda q: O.check_points(scene.plant, q, O.RULE_GPU, nthreads=ncores),
-                       lambda a, b: bool(O.check_edges(scene.plant, a[None], b[None], nthreads=ncores)[0][0]))
-    d = scene.dim
-    A0 = np.zeros((2 * d, d), np.float32)
-    for i in range(d):
-        A0[2 * i, i], A0[2 * i + 1, i] = -1, 1
-    b0 = np.concatenate([[-scene.lower()[i], scene.upper()[i]] for i in range(d)]).astype(np.float32)
-    from csdecomp_b200.api import EizoOptions
-    opt = EizoOptions(**EIZO_KW)
-    for q0, q1 in edges[:args.warmup]:
-        O.eizo(scene.plant, q0, q1, A0, b0, opt, scene.inspector.robot_geometry_ids, nthreads=ncores)
-    t0 = time.perf_counter()
-    for q0, q1 in edges[args.warmup:]:
-        O.eizo(scene.plant, q0, q1, A0, b0, opt, scene.inspector.robot_geometry_ids, nthreads=ncores)
-    dt = time.perf_counter() - t0
-    v = args.steps / dt
-    line = {"metric": METRIC, "value": v, "unit": "regions/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+    items, skipped = workload(0, args.warmup + args.steps, args.warmup + 1, oracle_checkers(ncores))
+    items = [(sc, e[args.warmup]) for sc, e in items]
+    cpu_eizo(items[:args.warmup], ncores, 30.0)
+    rate, n, dt = cpu_eizo(items[args.warmup:], ncores, 120.0)
+    line = {"metric": METRIC, "value": rate, "unit": "regions/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": n, "warmup": args.warmup, "ms_per_step": 1e3 * dt / n,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded)", "config": {"workload": WORKLOAD, "l2": "n/a (CPU)"},
-            "cpu_baseline": {"value": v, "unit": "regions/s", "cores": ncores, "kind": "port",
-                             "sample": f"{args.steps} inflations on all host threads (the reference's CPU path "
-                                       "cannot be built here: Eigen/glpk/Bazel absent; oracle/ restates executeEizo)"},
-            "e2e": {"value": v, "unit": "regions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "form": "CPU, one inflation per step", "l2": "n/a (CPU)",
+                       "scenes_skipped": skipped},
+            "cpu_baseline": {"value": rate, "unit": "regions/s", "cores": ncores, "kind": "port",
+                             "sample": f"{n} inflations (scenes {args.warmup}..{args.warmup + n - 1} of the "
+                                       "workload, one seed edge each) on all host threads; the reference's CPU path "
+                                       "cannot be built here (Eigen, glpk and Bazel absent), so oracle/ restates "
+                                       "executeEizo"},
+            "e2e": {"value": rate, "unit": "regions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 def roofline_point_check(csd, scene, torch, dev):
-    """Fused FK + pair sweep on collision-free configurations of the scene:
-    every pair is evaluated, so the FLOP count is exact."""
+    """Fused FK + pair sweep on collision-free configurations of the 7-DOF /
+    200-primitive scene: every pair is evaluated, so the FLOP count is exact."""
     from csdecomp_b200 import _capi as C
     import ctypes
     h = csd.plant_handle(scene.plant)
@@ -193,7 +209,7 @@ def roofline_point_check(csd, scene, torch, dev):
         C.check(C.lib().csd_check_points(h.handle, C.ptr(tq.data_ptr()), ctypes.c_int64(n), None, 0,
                                          ctypes.c_float(0), None, 0, C.ptr(out.data_ptr()), C.CSD_PTR_DEVICE,
                                          ctypes.c_void_p(st.cuda_stream)))
-    for _ in range(2):
+    for _ in range(3):
         launch()
     times = []
     for _ in range(5):
@@ -213,11 +229,11 @@ def roofline_point_check(csd, scene, torch, dev):
     achieved = flops / t
     return {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
             "frac": achieved / peak, "traffic": None,
-            "kernel": "check_points_kernel (fused FK + pair sweep)",
+            "kernel": "check_points_kernel (fused FK + pair sweep; the batched check stage runs the same device code)",
             "per_config_flop": fl, "configs_per_launch": n, "launch_ms": t * 1e3,
             "peak_source": "measured FP32 FMA probe (csd_fp32_fma_probe) in this run",
-            "workload": "1,048,576 collision-free configurations of the bench scene (full sweep, no early exit); "
-                        "L2 flushed between launches"}
+            "workload": "1,048,576 collision-free configurations of the 7-DOF arm (80 spheres + 4 capsules) in "
+                        "200 world primitives (full sweep, no early exit); L2 flushed between launches"}
 
 
 def main():
@@ -228,6 +244,8 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank)
         return
+    if args.warmup < 1:
+        raise SystemExit("--warmup must be >= 1")
     import torch
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -235,76 +253,114 @@ def main():
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     import csdecomp_b200 as csd
     from csdecomp_b200 import scenes
+    from csdecomp_b200.shard import reduce_timing
 
-    scene = scenes.edge_check_scene(keepout=0.8)
-    total_edges = (args.warmup + args.steps) * world
-    edges = seed_edges(scene, total_edges, lambda q: csd.CheckCollisionFreeCuda(q.T, scene.plant),
-                       lambda a, b: csd.CheckEdgeCollisionFree(a, b, scene.plant))
-    from csdecomp_b200.shard import reduce_timing, shard
-    per_rank = args.warmup + args.steps
-    mine = edges[rank * per_rank:(rank + 1) * per_rank]
-    dom = csd.HPolyhedron()
-    dom.MakeBox(scene.lower(), scene.upper())
+    def gpu_checkers(sc):
+        return (lambda q: csd.CheckCollisionFreeCuda(q.T, sc.plant),
+                lambda a, b: csd.CheckEdgesCollisionFreeCuda(a.T, b.T, sc.plant))
+
+    steps_total = args.warmup + args.steps
+    items, skipped = workload(rank, NUM_SLOTS, steps_total, gpu_checkers)
+    scs = [sc for sc, _ in items]
+    doms = []
+    for sc in scs:
+        d = csd.HPolyhedron()
+        d.MakeBox(sc.lower(), sc.upper())
+        doms.append(d)
     opt = csd.EizoOptions(**EIZO_KW)
-    inf = csd.CudaEdgeInflator(scene.plant, scene.inspector.robot_geometry_ids, opt, dom)
-    for q0, q1 in mine[:args.warmup]:
-        inf.inflateEdge(q0, q1, None, 0.0, verbose=False)
+    batch = csd.BatchedEdgeInflator([sc.plant for sc in scs], opt, max_slots=NUM_SLOTS, face_capacity=FACE_CAPACITY)
+    slot_plant = list(range(NUM_SLOTS))
+
+    def step_inputs(s):
+        return [e[s][0] for _, e in items], [e[s][1] for _, e in items]
+
+    for s in range(args.warmup):
+        q0s, q1s = step_inputs(s)
+        batch.inflate(slot_plant, q0s, q1s, doms)
     torch.cuda.synchronize()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    st = torch.cuda.current_stream()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    dev_s, wall_s, faces, configs, launches = 0.0, 0.0, 0, 0, 0
-    d2h = 0
+    dev_s, wall_s, configs, launches = 0.0, 0.0, 0, 0
+    faces, iters, h2d, d2h = [], [], 0, 0
+    first_regions = None
     with ClockSampler(local) as clk:
-        for q0, q1 in mine[args.warmup:]:
+        for s in range(args.warmup, steps_total):
+            q0s, q1s = step_inputs(s)
             flush.fill_(1)  # L2 flush between steps (outside the timed window)
             torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             w0 = time.perf_counter()
-            e0.record(st)
-            P = inf.inflateEdge(q0, q1, None, 0.0, verbose=False)
-            e1.record(st)
-            e1.synchronize()
+            regions = batch.inflate(slot_plant, q0s, q1s, doms)
             wall_s += time.perf_counter() - w0
-            dev_s += e0.elapsed_time(e1) * 1e-3
-            it = inf.last_info.iteration_info
-            faces += P.A().shape[0]
-            configs += sum(i.num_samples_drawn + i.num_collisions_updated * opt.bisection_steps for i in it)
-            launches += sum(3 + (2 if i.num_collisions_updated else 0) for i in it)
-            d2h += P.A().shape[0] * (scene.dim + 1) * 4 + 16 * (len(it) + 1) + 4
+            dev_s += batch.last_device_ms * 1e-3
+            if first_regions is None:
+                first_regions = regions
+            configs += int(batch.last_configs_checked.sum())
+            n_graph = int(batch.last_iterations.max())
+            launches += 6 * n_graph
+            faces += [r.A().shape[0] for r in regions]
+            iters += [int(x) for x in batch.last_iterations]
+            h2d += sum(sc.dim * 8 + d.A().nbytes + d.b().nbytes for sc, d in zip(scs, doms)) + 8 * NUM_SLOTS + 4
+            d2h += sum(r.A().nbytes + r.b().nbytes for r in regions) + 16 * n_graph + 120 * NUM_SLOTS
     torch.cuda.synchronize()
+    # plain GPU form (one CudaEdgeInflator call per region) on the first timed step's inputs
+    plain_s, identical = 0.0, True
+    st = torch.cuda.current_stream()
+    q0s, q1s = step_inputs(args.warmup)
+    for i, sc in enumerate(scs):
+        inf = csd.CudaEdgeInflator(sc.plant, sc.inspector.robot_geometry_ids, opt, doms[i],
+                                   face_capacity=FACE_CAPACITY)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        P = inf.inflateEdge(q0s[i], q1s[i], None, 0.0, verbose=False)
+        e1.record(st)
+        e1.synchronize()
+        plain_s += e0.elapsed_time(e1) * 1e-3
+        identical &= bool(np.array_equal(P.A(), first_regions[i].A()) and np.array_equal(P.b(), first_regions[i].b()))
+        del inf
     if dist:
         dev_s, wall_s, configs_all = reduce_timing(dist, dev, dev_s, wall_s, float(configs))
+        plain_s, _, _ = reduce_timing(dist, dev, plain_s, 0.0, 0.0)
         dist.barrier()
     else:
         configs_all = float(configs)
-    regions = args.steps * world
+    regions_all = NUM_SLOTS * args.steps * world
     if rank == 0:
-        value = regions / dev_s
+        value = regions_all / dev_s
+        plain = NUM_SLOTS * world / plain_s
         line = {"metric": METRIC, "value": value, "unit": "regions/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 * dev_s / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-                "config": {"workload": WORKLOAD, "form": "plain GPU (one inflation per call)",
-                           "parallelism": f"{world} independent ranks",
-                           "l2": "flushed between steps (256 MB write)"},
+                "config": {"workload": WORKLOAD, "form": "batched (BatchedEdgeInflator, 256 slots, CUDA graph)",
+                           "surrogate": "not used", "parallelism": f"{world} independent ranks",
+                           "l2": "flushed between steps (256 MB write)", "scenes_skipped": skipped,
+                           "face_capacity": FACE_CAPACITY},
                 "configs_per_s": configs_all / dev_s,
-                "mean_faces": faces / args.steps,
-                "e2e": {"value": regions / wall_s, "unit": "regions/s",
-                        "h2d_bytes_per_step": 2 * scene.dim * 4, "d2h_bytes_per_step": d2h // args.steps,
-                        "path": "CudaEdgeInflator.inflateEdge with host numpy segment and host polytope out"},
+                "plain_gpu": {"value": plain, "unit": "regions/s",
+                              "sample": "the first timed step's 256 inflations, one CudaEdgeInflator.inflateEdge "
+                                        "call each", "identical_regions": identical,
+                              "batched_over_plain": value / plain},
+                "faces": {"mean": float(np.mean(faces)), "max": int(np.max(faces)), "min": int(np.min(faces))},
+                "iterations": {"mean": float(np.mean(iters)), "max": int(np.max(iters))},
+                "e2e": {"value": regions_all / wall_s, "unit": "regions/s",
+                        "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
+                        "path": "BatchedEdgeInflator.inflate with host numpy segments and polytopes in, host "
+                                "polytopes out"},
                 "gpu_launches": launches,
                 "clocks": clk.summary()}
-        line["roofline"] = roofline_point_check(csd, scene, torch, dev)
+        line["roofline"] = roofline_point_check(csd, scenes.edge_check_scene(keepout=0.8), torch, dev)
         if world == 1:
-            rate, n, dt = cpu_eizo_baseline(scene, mine[args.warmup:args.warmup + 4], os.cpu_count() or 1)
-            line["cpu_baseline"] = {"value": rate, "unit": "regions/s", "cores": os.cpu_count() or 1, "kind": "port",
-                                    "sample": f"{n} inflations of the same seed edges ({dt:.1f} s) by the oracle's "
-                                              "restated executeEizo with OpenMP"}
+            sample = [(sc, e[args.warmup]) for sc, e in items[:8]]
+            rate, n, dt = cpu_eizo(sample, os.cpu_count() or 1, 20.0)
+            line["cpu_baseline"] = {"value": rate, "unit": "regions/s", "cores": os.cpu_count() or 1,
+                                    "kind": "port",
+                                    "sample": f"{n} inflations of the first timed step's seed edges ({dt:.1f} s) by "
+                                              "the oracle's restated executeEizo with OpenMP"}
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()

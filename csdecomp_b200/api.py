@@ -486,12 +486,27 @@ class BatchedEdgeInflator:
                                           ctypes.byref(ms)))
         self.last_iterations = nit
         self.last_device_ms = ms.value
+        cfg = np.zeros(n, np.int64)
+        C.check(C.lib().csd_batch_configs_checked(self._handle, n, C.ptr(cfg)))
+        self.last_configs_checked = cfg
         out, aoff = [], 0
         for i, d in enumerate(dims):
             Ai = A_out[aoff:aoff + nf[i] * d].reshape(nf[i], d).copy()
             out.append(HPolyhedron(Ai, b_out[i * self._capacity:i * self._capacity + nf[i]].copy()))
             aoff += self._capacity * d
         return out
+
+    STAGES = ("sample", "check", "compact", "bisect", "faces", "step")
+
+    def set_profiling(self, enable: bool) -> None:
+        """Launch stage by stage with events (no graph) and accumulate each
+        stage's GPU time; toggling resets the accumulators."""
+        C.check(C.lib().csd_batch_set_profiling(self._handle, int(bool(enable))))
+
+    def stage_ms(self) -> dict:
+        ms = np.zeros(6, np.float32)
+        C.check(C.lib().csd_batch_stage_ms(self._handle, C.ptr(ms)))
+        return dict(zip(self.STAGES, ms.tolist()))
 
     def __del__(self):
         h = getattr(self, "_handle", None)

@@ -33,20 +33,24 @@ struct SlotState {
   int K;              // collisions kept for this iteration's bisection
   int status;         // 2: face capacity exceeded
   long long a_off;    // floats: region A [capacity][dim]
+  long long at_off;   // floats: region A transposed [dim][capacity]
   long long b_off;    // floats: region b [capacity]
   long long seg_off;  // floats: line start [dim], line end [dim]
   long long smp_off;  // floats: samples [n_max][dim]
   long long col_off;  // floats: collision points / projections [num_particles][dim] each
   long long dist_off; // floats: distances [num_particles]
   long long flag_off; // bytes: verdicts [n_max]
+  long long configs;  // configurations checked: samples + bisection points
   EizoCounters cnt;
 };
+
+static_assert(sizeof(SlotState) == 120, "slot record size is part of the transfer accounting");
 
 struct BatchIter {    // device-side iteration state
   int k;              // current iteration
   int active;         // slots still running, counted by the faces kernel
   int last_active;    // the count of the iteration that just finished
-  int pad;
+  int num_act;        // length of the active-slot list of iteration k
 };
 
 struct BatchArgs {
@@ -60,6 +64,8 @@ struct BatchArgs {
   int bisection;
   int max_faces;
   int capacity;
+  int cfg_max;        // largest check work item (configurations)
+  int part_max;       // largest bisection work item (particles)
   float margin;
   uint32_t k0, k1;    // Philox key (seed)
   const int* n_tab;   // N_k
@@ -68,35 +74,68 @@ struct BatchArgs {
   float* fpool;
   uint8_t* bpool;
   BatchIter* it;
+  int* act;           // active-slot list of iteration k (slot indices, ascending)
 };
 
+// Work-item size for `total` units over the grid: about four items per
+// block, a multiple of the block's warps, at most `cap`.
+static __device__ __forceinline__ int item_size(int64_t total, int cap, int nw) {
+  int64_t c = total / (4 * (int64_t)gridDim.x);
+  c = c < nw ? nw : c > cap ? cap : c;
+  return (int)(c / nw) * nw;
+}
+
 // ------------------------------------------------------------------ kernels
-__global__ void __launch_bounds__(128) batch_sample_kernel(BatchArgs a) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int slot = (int)(i / a.n_max), chain = (int)(i % a.n_max);
-  if (slot >= a.num_slots) return;
-  const SlotState& S = a.slots[slot];
+// Chains of the active slots in work items (slot, chunk of chains); a block
+// takes a contiguous run of items, stages each new slot's region (At, b) in
+// shared memory and runs its chains G lanes per chain (G from the total
+// chain count: 8 when the batch is full, up to 32 in the tail).
+__global__ void __launch_bounds__(256) batch_sample_kernel(BatchArgs a) {
+  extern __shared__ float smf[];
   const int N = a.n_tab[a.it->k];
-  if (S.done || chain >= N) return;
-  const int dim = S.dim;
-  const float* A = a.fpool + S.a_off;
-  const float* b = a.fpool + S.b_off;
-  const float* ls = a.fpool + S.seg_off;
-  float* dst = a.fpool + S.smp_off + (int64_t)chain * dim;
-  bool ok;
-  if (dim <= 8) {
-    float x[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) x[k] = k < dim ? ls[k] : 0.f;
-    ok = run_chain<8>(A, b, S.nf, dim, a.mixing, a.k0, a.k1, (uint32_t)chain, 0u, x);
-    for (int k = 0; k < dim; ++k) dst[k] = ok ? x[k] : ls[k];
-  } else {
-    float x[16];
-#pragma unroll
-    for (int k = 0; k < 16; ++k) x[k] = k < dim ? ls[k] : 0.f;
-    ok = run_chain<16>(A, b, S.nf, dim, a.mixing, a.k0, a.k1, (uint32_t)chain, 0u, x);
-    for (int k = 0; k < dim; ++k) dst[k] = ok ? x[k] : ls[k];
+  const int64_t total = (int64_t)a.it->num_act * N;
+  const int G = group_width(total, (int64_t)gridDim.x * (blockDim.x >> 5));
+  int64_t c = total / (4 * (int64_t)gridDim.x);
+  c = c < 32 ? 32 : c > 1024 ? 1024 : c;
+  const int chunk = (int)(c / 32) * 32;
+  const int ips = (N + chunk - 1) / chunk;
+  const int64_t items = (int64_t)a.it->num_act * ips;
+  const int64_t per_block = (items + gridDim.x - 1) / gridDim.x;
+  const int64_t i0 = blockIdx.x * per_block, i1 = min(items, i0 + per_block);
+  int staged = -1;
+  for (int64_t it = i0; it < i1; ++it) {
+    const int slot = a.act[it / ips], first = (int)(it % ips) * chunk, last = min(N, first + chunk);
+    const SlotState& S = a.slots[slot];
+    const int dim = S.dim, F = S.nf;
+    const float* At = a.fpool + S.at_off;
+    const float* b = a.fpool + S.b_off;
+    const float* ls = a.fpool + S.seg_off;
+    float* out = a.fpool + S.smp_off;
+    const bool fits = F <= (dim <= 8 ? kStageFaces8 : kStageFaces16);
+    if (fits && staged != slot) {
+      __syncthreads();  // the previous slot's chains are done with the buffer
+      if (dim <= 8)
+        stage_polytope<8, kStageFaces8>(At, a.capacity, b, F, dim, smf);
+      else
+        stage_polytope<16, kStageFaces16>(At, a.capacity, b, F, dim, smf);
+      __syncthreads();
+      staged = slot;
+    }
+    if (dim <= 8)
+      sample_range<8>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, G, smf, fits);
+    else
+      sample_range<16>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, G, smf, fits);
   }
+}
+
+// Block per slot: the domain rows of A into At.
+__global__ void batch_transpose_kernel(BatchArgs a) {
+  if ((int)blockIdx.x >= a.num_slots) return;
+  const SlotState& S = a.slots[blockIdx.x];
+  const float* A = a.fpool + S.a_off;
+  float* At = a.fpool + S.at_off;
+  for (int i = threadIdx.x; i < S.nf * S.dim; i += blockDim.x)
+    At[(int64_t)(i % S.dim) * a.capacity + i / S.dim] = A[i];
 }
 
 // Loads plant `pi` into the block's shared DevPlant and stages its statics.
@@ -129,11 +168,11 @@ static __device__ __forceinline__ WarpCtx<SM> batch_ctx(const DevPlant& p, float
   return w;
 }
 
-// Work item = (slot, chunk of configurations); a block takes a contiguous
-// run of items so consecutive items usually share a plant.
+// Work item = (active slot, chunk of configurations), sized so that the grid
+// gets about four items per block whether 256 slots or one are active; items
+// are dealt round robin to the blocks.
 template <bool SM>
-__global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_check_kernel(BatchArgs a, int cfg_per_item,
-                                                                            int static_floats) {
+__global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_check_kernel(BatchArgs a, int static_floats) {
   extern __shared__ float4 smem4[];
   __shared__ uint64_t bar;
   __shared__ DevPlant sp;
@@ -141,21 +180,20 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_check_kernel(Bat
   if (threadIdx.x == 0) cur = -1;
   __syncthreads();
   const int N = a.n_tab[a.it->k];
-  const int items_per_slot = (a.n_max + cfg_per_item - 1) / cfg_per_item;
-  const int64_t items = (int64_t)a.num_slots * items_per_slot;
-  const int64_t per_block = (items + gridDim.x - 1) / gridDim.x;
+  const int na = a.it->num_act;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int c = item_size((int64_t)na * N, a.cfg_max, nw);
+  const int ips = (N + c - 1) / c;
+  const int64_t items = (int64_t)na * ips;
   const VoxArgs none{nullptr, 0, 0.f, nullptr, nullptr, 0};
-  for (int64_t it = blockIdx.x * per_block; it < std::min<int64_t>(items, (blockIdx.x + 1) * per_block); ++it) {
-    const int slot = (int)(it / items_per_slot), chunk = (int)(it % items_per_slot);
+  for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
+    const int slot = a.act[it / ips], first = (int)(it % ips) * c;
     const SlotState& S = a.slots[slot];
-    const int first = chunk * cfg_per_item;
-    if (S.done || first >= N) continue;  // uniform across the block
     if (!block_plant<SM>(a, S.plant, &sp, &cur, smem4, &bar)) return;
     const WarpCtx<SM> w = batch_ctx<SM>(sp, smem4, static_floats);
     const float* smp = a.fpool + S.smp_off;
     uint8_t* flags = a.bpool + S.flag_off;
-    const int last = std::min(N, first + cfg_per_item);
+    const int last = std::min(N, first + c);
     for (int i = first + warp; i < last; i += nw) {
       if (lane < sp.dim) w.qs[lane] = smp[(int64_t)i * sp.dim + lane];
       __syncwarp();
@@ -179,39 +217,40 @@ __global__ void __launch_bounds__(1024) batch_compact_kernel(BatchArgs a) {
   compact_block(a.bpool + S.flag_off, a.fpool + S.smp_off, N, M, a.num_particles, S.dim, a.fpool + S.col_off,
                 &S.cnt);
   if (threadIdx.x == 0) {
+    S.configs += N;
     if ((float)S.cnt.first_m <= a.thr_tab[k]) {
       S.done = 1;
       S.iters = k + 1;
       S.K = 0;
     } else {
       S.K = (int)std::min<uint32_t>(S.cnt.total, (uint32_t)a.num_particles);
+      S.configs += (long long)S.K * a.bisection;
     }
   }
 }
 
 template <bool SM>
-__global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_bisect_kernel(BatchArgs a, int part_per_item,
-                                                                             int static_floats) {
+__global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_bisect_kernel(BatchArgs a, int static_floats) {
   extern __shared__ float4 smem4[];
   __shared__ uint64_t bar;
   __shared__ DevPlant sp;
   __shared__ int cur;
   if (threadIdx.x == 0) cur = -1;
   __syncthreads();
-  const int items_per_slot = (a.num_particles + part_per_item - 1) / part_per_item;
-  const int64_t items = (int64_t)a.num_slots * items_per_slot;
-  const int64_t per_block = (items + gridDim.x - 1) / gridDim.x;
+  const int na = a.it->num_act;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int c = item_size((int64_t)na * a.num_particles, a.part_max, nw);
+  const int ips = (a.num_particles + c - 1) / c;
+  const int64_t items = (int64_t)na * ips;
   const VoxArgs none{nullptr, 0, 0.f, nullptr, nullptr, 0};
-  for (int64_t it = blockIdx.x * per_block; it < std::min<int64_t>(items, (blockIdx.x + 1) * per_block); ++it) {
-    const int slot = (int)(it / items_per_slot), chunk = (int)(it % items_per_slot);
+  for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
+    const int slot = a.act[it / ips], first = (int)(it % ips) * c;
     const SlotState& S = a.slots[slot];
-    const int first = chunk * part_per_item;
-    if (S.done || first >= S.K) continue;
+    if (S.done || first >= S.K) continue;  // uniform across the block
     if (!block_plant<SM>(a, S.plant, &sp, &cur, smem4, &bar)) return;
     const WarpCtx<SM> w = batch_ctx<SM>(sp, smem4, static_floats);
     const float* ls = a.fpool + S.seg_off;
-    const int last = std::min(S.K, first + part_per_item);
+    const int last = std::min(S.K, first + c);
     for (int i = first + warp; i < last; i += nw)
       bisect_particle<SM>(sp, w, i, S.dim, a.bisection, ls, ls + S.dim, none, a.fpool + S.col_off,
                           a.fpool + S.col_off + (int64_t)a.num_particles * S.dim, a.fpool + S.dist_off, lane);
@@ -226,7 +265,7 @@ __global__ void __launch_bounds__(1024) batch_faces_kernel(BatchArgs a) {
     const float* ls = a.fpool + S.seg_off;
     faces_block(S.K, S.dim, a.max_faces, a.capacity, a.margin, ls, ls + S.dim, a.fpool + S.col_off,
                 a.fpool + S.col_off + (int64_t)a.num_particles * S.dim, a.fpool + S.dist_off, a.fpool + S.a_off,
-                a.fpool + S.b_off, &S.nf, &S.cnt);
+                a.fpool + S.b_off, &S.nf, &S.cnt, a.fpool + S.at_off);
     if (threadIdx.x == 0) {
       S.iters = k + 1;
       S.status = S.cnt.status;
@@ -236,10 +275,34 @@ __global__ void __launch_bounds__(1024) batch_faces_kernel(BatchArgs a) {
   if (threadIdx.x == 0 && !S.done) atomicAdd(&a.it->active, 1);
 }
 
-__global__ void batch_step_kernel(BatchIter* it) {
-  it->last_active = it->active;
-  it->active = 0;
-  it->k += 1;
+// One block: advances k and rebuilds the active-slot list (ascending).
+__global__ void __launch_bounds__(1024) batch_step_kernel(BatchArgs a) {
+  __shared__ int warp_n[32];
+  __shared__ int base;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  if (tid == 0) base = 0;
+  __syncthreads();
+  for (int s0 = 0; s0 < a.num_slots; s0 += blockDim.x) {
+    const int s = s0 + tid;
+    const bool act = s < a.num_slots && !a.slots[s].done;
+    const unsigned m = __ballot_sync(0xffffffffu, act);
+    if (lane == 0) warp_n[warp] = __popc(m);
+    __syncthreads();
+    int off = base;
+    for (int w = 0; w < warp; ++w) off += warp_n[w];
+    if (act) a.act[off + __popc(m & ((1u << lane) - 1u))] = s;
+    __syncthreads();
+    if (tid == 0)
+      for (int w = 0; w < nw; ++w) base += warp_n[w];
+    __syncthreads();
+  }
+  if (tid == 0) {
+    BatchIter* it = a.it;
+    it->last_active = it->active;
+    it->active = 0;
+    it->k += 1;
+    it->num_act = base;
+  }
 }
 
 }  // namespace csd
@@ -254,16 +317,22 @@ struct csd_batch_s {
   int static_floats = 0;
   size_t check_smem = 0;
   int check_grid = 0, bisect_grid = 0;
-  int cfg_per_item = 64, part_per_item = 8;
+  int cfg_max = 256, part_max = 64, sample_grid = 0;
   std::vector<int> n_tab, m_tab;
   std::vector<float> thr_tab;
-  csd::DevBuf plants_dev, slots_dev, tabs, fpool, bpool, iter;
+  csd::DevBuf plants_dev, slots_dev, tabs, fpool, bpool, iter, act;
   std::vector<csd::SlotState> host_slots;
+  std::vector<int> act_host;
   cudaGraphExec_t graph = nullptr;
   int graph_slots = -1;
   cudaStream_t graph_stream = nullptr;
   csd::BatchIter* host_iter = nullptr;
+  bool profile = false;         // launch stage by stage with events instead of the graph
+  cudaEvent_t ev[7] = {};
+  double stage_ms[6] = {};
   ~csd_batch_s() {
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
     if (graph) cudaGraphExecDestroy(graph);
     if (graph_stream) cudaStreamDestroy(graph_stream);
     if (host_iter) cudaFreeHost(host_iter);
@@ -274,6 +343,30 @@ using namespace csd;
 
 namespace {
 
+// One iteration's six launches on stream s; with ev (7 events) recorded
+// between the stages for the profiling mode.
+void launch_iteration(csd_batch_s* h, int num_slots, const BatchArgs& a, cudaStream_t s, cudaEvent_t* ev) {
+  if (ev) cudaEventRecord(ev[0], s);
+  batch_sample_kernel<<<h->sample_grid, 256, kStageBytes, s>>>(a);
+  if (ev) cudaEventRecord(ev[1], s);
+  if (h->sm)
+    batch_check_kernel<true><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->static_floats);
+  else
+    batch_check_kernel<false><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, 0);
+  if (ev) cudaEventRecord(ev[2], s);
+  batch_compact_kernel<<<num_slots, 1024, 0, s>>>(a);
+  if (ev) cudaEventRecord(ev[3], s);
+  if (h->sm)
+    batch_bisect_kernel<true><<<h->bisect_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->static_floats);
+  else
+    batch_bisect_kernel<false><<<h->bisect_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, 0);
+  if (ev) cudaEventRecord(ev[4], s);
+  batch_faces_kernel<<<num_slots, 1024, 0, s>>>(a);
+  if (ev) cudaEventRecord(ev[5], s);
+  batch_step_kernel<<<1, 1024, 0, s>>>(a);
+  if (ev) cudaEventRecord(ev[6], s);
+}
+
 csd_status_t build_graph(csd_batch_s* h, int num_slots, const BatchArgs& a) {
   if (h->graph && h->graph_slots == num_slots) return CSD_OK;
   if (h->graph) {
@@ -283,21 +376,7 @@ csd_status_t build_graph(csd_batch_s* h, int num_slots, const BatchArgs& a) {
   cudaStream_t s = h->graph_stream;
   cudaGraph_t g = nullptr;
   CSD_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-  const int64_t chains = (int64_t)num_slots * h->n_max;
-  batch_sample_kernel<<<(unsigned)((chains + 127) / 128), 128, 0, s>>>(a);
-  if (h->sm)
-    batch_check_kernel<true><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->cfg_per_item,
-                                                                                      h->static_floats);
-  else
-    batch_check_kernel<false><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->cfg_per_item, 0);
-  batch_compact_kernel<<<num_slots, 1024, 0, s>>>(a);
-  if (h->sm)
-    batch_bisect_kernel<true><<<h->bisect_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->part_per_item,
-                                                                                        h->static_floats);
-  else
-    batch_bisect_kernel<false><<<h->bisect_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->part_per_item, 0);
-  batch_faces_kernel<<<num_slots, 1024, 0, s>>>(a);
-  batch_step_kernel<<<1, 1, 0, s>>>(a.it);
+  launch_iteration(h, num_slots, a, s, nullptr);
   cudaError_t e = cudaStreamEndCapture(s, &g);
   if (e != cudaSuccess) {
     set_error(std::string("graph capture failed: ") + cudaGetErrorString(e));
@@ -374,12 +453,20 @@ csd_status_t csd_batch_create(const csd_plant_t* plants, int32_t num_plants, int
   }
   h->check_grid = g1;
   h->bisect_grid = g2;
+  CSD_CUDA_TRY(cudaFuncSetAttribute(batch_sample_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kStageBytes));
+  {
+    int per_sm = 0;
+    CSD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_sample_kernel, 256, kStageBytes));
+    h->sample_grid = device_sm_count() * std::max(1, per_sm);
+  }
   // buffers
   const size_t D = (size_t)h->max_dim, np = o->num_particles, cap = (size_t)face_capacity;
-  const size_t per_slot_f = cap * D + cap + 2 * D + (size_t)h->n_max * D + 2 * np * D + np;
+  const size_t per_slot_f = 2 * cap * D + cap + 2 * D + (size_t)h->n_max * D + 2 * np * D + np;
   if ((s = h->plants_dev.reserve(dps.size() * sizeof(DevPlant))) || (s = h->slots_dev.reserve(max_slots * sizeof(SlotState))) ||
       (s = h->tabs.reserve(h->n_tab.size() * 12 + 64)) || (s = h->fpool.reserve(per_slot_f * max_slots * 4 + 256)) ||
-      (s = h->bpool.reserve((size_t)h->n_max * max_slots + 256)) || (s = h->iter.reserve(sizeof(BatchIter))))
+      (s = h->bpool.reserve((size_t)h->n_max * max_slots + 256)) || (s = h->iter.reserve(sizeof(BatchIter))) ||
+      (s = h->act.reserve((size_t)max_slots * 4)))
     return s;
   CSD_CUDA_TRY(cudaMemcpy(h->plants_dev.ptr, dps.data(), dps.size() * sizeof(DevPlant), cudaMemcpyHostToDevice));
   int* t = h->tabs.as<int>();
@@ -421,7 +508,7 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
     }
   } restore{cur, h->device};
   const size_t D = (size_t)h->max_dim, np = h->opt.num_particles, cap = (size_t)h->capacity;
-  const size_t per_slot_f = cap * D + cap + 2 * D + (size_t)h->n_max * D + 2 * np * D + np;
+  const size_t per_slot_f = 2 * cap * D + cap + 2 * D + (size_t)h->n_max * D + 2 * np * D + np;
   std::vector<SlotState> slots(n);
   size_t qoff = 0, arow = 0;
   cudaStream_t st = h->graph_stream;
@@ -453,7 +540,8 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
     S.nf = f1 - f0;
     const long long base = (long long)(per_slot_f * i);
     S.a_off = base;
-    S.b_off = S.a_off + (long long)(cap * D);
+    S.at_off = S.a_off + (long long)(cap * D);
+    S.b_off = S.at_off + (long long)(cap * D);
     S.seg_off = S.b_off + (long long)cap;
     S.smp_off = S.seg_off + (long long)(2 * D);
     S.col_off = S.smp_off + (long long)((size_t)h->n_max * D);
@@ -487,8 +575,12 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
   }
   CSD_CUDA_TRY(cudaMemcpyAsync(h->slots_dev.ptr, slots.data(), n * sizeof(SlotState), cudaMemcpyHostToDevice, st));
   BatchIter zero{};
+  zero.num_act = n;
   *h->host_iter = zero;
   CSD_CUDA_TRY(cudaMemcpyAsync(h->iter.ptr, h->host_iter, sizeof(BatchIter), cudaMemcpyHostToDevice, st));
+  h->act_host.resize(n);
+  for (int i = 0; i < n; ++i) h->act_host[i] = i;
+  CSD_CUDA_TRY(cudaMemcpyAsync(h->act.ptr, h->act_host.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st));
   BatchArgs a{};
   a.slots = h->slots_dev.as<SlotState>();
   a.plants = h->plants_dev.as<DevPlant>();
@@ -510,6 +602,11 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
   a.fpool = h->fpool.as<float>();
   a.bpool = h->bpool.as<uint8_t>();
   a.it = h->iter.as<BatchIter>();
+  a.act = h->act.as<int>();
+  a.cfg_max = h->cfg_max;
+  a.part_max = h->part_max;
+  batch_transpose_kernel<<<n, 256, 0, st>>>(a);
+  CSD_CUDA_TRY(cudaGetLastError());
   csd_status_t s = build_graph(h, n, a);
   if (s) return s;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -519,7 +616,18 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
     CSD_CUDA_TRY(cudaEventRecord(ev0, st));
   }
   for (uint32_t k = 0; k < h->opt.max_iterations; ++k) {
-    CSD_CUDA_TRY(cudaGraphLaunch(h->graph, st));
+    if (h->profile) {
+      launch_iteration(h, n, a, st, h->ev);
+      CSD_CUDA_TRY(cudaGetLastError());
+      CSD_CUDA_TRY(cudaEventSynchronize(h->ev[6]));
+      for (int j = 0; j < 6; ++j) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->ev[j], h->ev[j + 1]);
+        h->stage_ms[j] += ms;
+      }
+    } else {
+      CSD_CUDA_TRY(cudaGraphLaunch(h->graph, st));
+    }
     CSD_CUDA_TRY(cudaMemcpyAsync(h->host_iter, h->iter.ptr, sizeof(BatchIter), cudaMemcpyDeviceToHost, st));
     CSD_CUDA_TRY(cudaStreamSynchronize(st));
     if (h->host_iter->last_active == 0) break;
@@ -533,6 +641,7 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
   }
   CSD_CUDA_TRY(cudaMemcpyAsync(slots.data(), h->slots_dev.ptr, n * sizeof(SlotState), cudaMemcpyDeviceToHost, st));
   CSD_CUDA_TRY(cudaStreamSynchronize(st));
+  h->host_slots.assign(slots.begin(), slots.end());
   size_t aoff = 0;
   for (int i = 0; i < n; ++i) {
     const SlotState& S = slots[i];
@@ -549,6 +658,29 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
     aoff += (size_t)h->capacity * S.dim;
   }
   CSD_CUDA_TRY(cudaStreamSynchronize(st));
+  return CSD_OK;
+}
+
+csd_status_t csd_batch_set_profiling(csd_batch_t h, int32_t enable) {
+  CSD_CHECK(h, CSD_ERR_INVALID, "null batch");
+  if (enable && !h->ev[0]) {
+    for (cudaEvent_t& e : h->ev) CSD_CUDA_TRY(cudaEventCreate(&e));
+  }
+  h->profile = enable != 0;
+  for (double& x : h->stage_ms) x = 0.0;
+  return CSD_OK;
+}
+
+csd_status_t csd_batch_stage_ms(csd_batch_t h, float* ms) {
+  CSD_CHECK(h && ms, CSD_ERR_INVALID, "null argument");
+  for (int j = 0; j < 6; ++j) ms[j] = (float)h->stage_ms[j];
+  return CSD_OK;
+}
+
+csd_status_t csd_batch_configs_checked(csd_batch_t h, int32_t n, int64_t* configs) {
+  CSD_CHECK(h && configs && n >= 0 && n <= (int)h->host_slots.size(), CSD_ERR_INVALID,
+            "slot count exceeds the last batch");
+  for (int i = 0; i < n; ++i) configs[i] = h->host_slots[i].configs;
   return CSD_OK;
 }
 

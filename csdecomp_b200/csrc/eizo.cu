@@ -65,8 +65,8 @@ __global__ void __launch_bounds__(1024) faces_kernel(int K, int dim, int max_fac
                                                      const float* __restrict__ cols, const float* __restrict__ proj,
                                                      float* __restrict__ dist, float* __restrict__ A,
                                                      float* __restrict__ b, int* __restrict__ num_faces,
-                                                     EizoCounters* cnt) {
-  faces_block(K, dim, max_faces, capacity, margin, ls, le, cols, proj, dist, A, b, num_faces, cnt);
+                                                     EizoCounters* cnt, float* __restrict__ At) {
+  faces_block(K, dim, max_faces, capacity, margin, ls, le, cols, proj, dist, A, b, num_faces, cnt, At);
 }
 
 }  // namespace csd
@@ -84,7 +84,7 @@ struct csd_inflator_s {
   std::vector<float> domain_A, domain_b;
   std::vector<uint32_t> vtab_host;
   int num_other = 0;
-  csd::DevBuf A, b, nf, samples, flags, cols, proj, dist, seg, vox, vtab, cnt;
+  csd::DevBuf A, At, b, nf, samples, flags, cols, proj, dist, seg, vox, vtab, cnt;
   csd::EizoCounters* host_cnt = nullptr;  // pinned
   int* host_nf = nullptr;                 // pinned
   ~csd_inflator_s() {
@@ -165,7 +165,8 @@ csd_status_t csd_inflator_create(csd_plant_t plant, const int32_t* ids, int32_t 
   csd_status_t s;
   if ((s = build_voxel_tables(plant, ids, nr, &h->vtab_host, &h->num_other))) return s;
   const size_t np = o->num_particles, mc = (size_t)h->max_configs;
-  if ((s = h->A.reserve((size_t)capacity * d * 4)) || (s = h->b.reserve((size_t)capacity * 4)) ||
+  if ((s = h->A.reserve((size_t)capacity * d * 4)) || (s = h->At.reserve((size_t)capacity * d * 4)) ||
+      (s = h->b.reserve((size_t)capacity * 4)) ||
       (s = h->nf.reserve(16)) || (s = h->samples.reserve(mc * d * 4)) || (s = h->flags.reserve(mc + 16)) ||
       (s = h->cols.reserve(np * d * 4)) || (s = h->proj.reserve(np * d * 4)) || (s = h->dist.reserve(np * 4)) ||
       (s = h->seg.reserve(2 * d * 4)) || (s = h->vox.reserve((size_t)std::max(1, max_voxels) * 12)) ||
@@ -174,6 +175,8 @@ csd_status_t csd_inflator_create(csd_plant_t plant, const int32_t* ids, int32_t 
   if (F0) {
     CSD_CUDA_TRY(cudaMemcpy(h->A.ptr, dA, (size_t)F0 * d * 4, cudaMemcpyHostToDevice));
     CSD_CUDA_TRY(cudaMemcpy(h->b.ptr, db, (size_t)F0 * 4, cudaMemcpyHostToDevice));
+    if ((s = launch_transpose_faces(h->A.as<float>(), F0, d, h->At.as<float>(), capacity, 0))) return s;
+    CSD_CUDA_TRY(cudaDeviceSynchronize());
   }
   if (!h->vtab_host.empty())
     CSD_CUDA_TRY(cudaMemcpy(h->vtab.ptr, h->vtab_host.data(), h->vtab_host.size() * 4, cudaMemcpyHostToDevice));
@@ -246,8 +249,8 @@ csd_status_t csd_inflator_inflate(csd_inflator_t h, const float* ls, const float
     float delta_k = (float)(6 * o.delta / (M_PI * M_PI * (it + 1) * (it + 1)));
     uint32_t M = csd_num_samples_unadaptive(o.epsilon, delta_k, o.tau);
     uint32_t N = std::max(M, o.num_particles);
-    if ((s = launch_hit_and_run(h->A.as<float>(), h->b.as<float>(), nullptr, 1, d, ls_d, (int)N, (int)o.mixing_steps,
-                                o.seed, 0u, 1, h->samples.as<float>(), nullptr, h->nf.as<int>(), st)))
+    if ((s = launch_hit_and_run_warp(h->At.as<float>(), h->capacity, h->b.as<float>(), h->nf.as<int>(), d, ls_d,
+                                     (int)N, (int)o.mixing_steps, o.seed, 0u, 1, h->samples.as<float>(), st)))
       return s;
     if ((s = launch_check_points(p, h->samples.as<float>(), N, vt, h->flags.as<uint8_t>(), st))) return s;
     compact_kernel<<<1, 1024, 0, st>>>(h->flags.as<uint8_t>(), h->samples.as<float>(), (int)N, (int)M,
@@ -285,7 +288,8 @@ csd_status_t csd_inflator_inflate(csd_inflator_t h, const float* ls, const float
       return s;
     faces_kernel<<<1, 1024, 0, st>>>((int)K, d, (int)o.max_hyperplanes_per_iteration, h->capacity,
                                      o.configuration_margin, ls_d, le_d, h->cols.as<float>(), h->proj.as<float>(),
-                                     h->dist.as<float>(), h->A.as<float>(), h->b.as<float>(), h->nf.as<int>(), cnt);
+                                     h->dist.as<float>(), h->A.as<float>(), h->b.as<float>(), h->nf.as<int>(), cnt,
+                                     h->At.as<float>());
     CSD_CUDA_TRY(cudaGetLastError());
     rec.num_collisions_updated = (int32_t)K;
     auto t1 = std::chrono::high_resolution_clock::now();
@@ -524,7 +528,8 @@ extern "C" csd_status_t csd_eizo_noalloc(csd_plant_t plant, const float* ls, con
     const uint32_t K = std::min(hc.total, o->num_particles);
     if ((s = launch_bisect(plant, (int)K, d, (int)o->bisection_steps, seg, seg + d, va, cols, proj, dist, st))) return s;
     faces_kernel<<<1, 1024, 0, st>>>((int)K, d, (int)o->max_hyperplanes_per_iteration, capacity,
-                                     o->configuration_margin, seg, seg + d, cols, proj, dist, A, b, nf, cnt);
+                                     o->configuration_margin, seg, seg + d, cols, proj, dist, A, b, nf, cnt,
+                                     nullptr);
     CSD_CUDA_TRY(cudaGetLastError());
     rec.num_collisions_updated = (int32_t)K;
     rec.iteration_time_ms =

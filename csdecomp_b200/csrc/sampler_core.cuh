@@ -49,4 +49,188 @@ __device__ __forceinline__ bool run_chain(const float* __restrict__ Ap, const fl
   return true;
 }
 
+// The same chain run by a group of G lanes (G = 8, 16 or 32; 32 / G chains
+// per warp). Jobs 0..ceil(dim/2)-1 are the Gaussian pairs and job ceil(dim/2)
+// the theta uniform, each drawn from the Philox block and words the serial
+// step_draws uses; lane gl of the group draws jobs gl, gl + G, ... and the
+// direction is broadcast by shuffles. The group's lanes split the faces
+// f = gl, gl + G, ...: each face's slack and A dir are accumulated in the
+// serial order, and the theta bounds are max/min reductions, which do not
+// depend on the order, so every chain ends bit for bit where run_chain ends.
+// At is the face matrix transposed, At[k * stride + f], with the stride ST
+// when ST > 0 (a shared-memory copy) and ldt otherwise. x is replicated in
+// the group's lanes. A chain whose line search fails keeps stepping without
+// moving (so the groups of a warp stay convergent for the shuffles) and
+// returns false.
+template <int MAXD, int G, int ST>
+__device__ __forceinline__ bool run_chain_group(const float* __restrict__ At, int ldt, const float* __restrict__ bp,
+                                                int F, int dim, int mixing, uint32_t k0, uint32_t k1,
+                                                uint32_t chain, uint32_t stream, float* x, int gl) {
+  constexpr int R = (MAXD / 2 + 1 + G - 1) / G;  // job rounds per lane
+  const int stride = ST > 0 ? ST : ldt;
+  const int npairs = (dim + 1) >> 1;
+  bool ok = true;
+  for (int step = 0; step < mixing; ++step) {
+    float c0[R], c1[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      c0[r] = 0.f;
+      c1[r] = 0.f;
+      const int job = gl + r * G;
+      if (job <= npairs) {
+        const int word = 2 * job;
+        uint32_t w[4];
+        philox4x32_10((uint32_t)step, chain, stream, (uint32_t)(word >> 2), k0, k1, w);
+        const uint32_t wa = (word & 2) ? w[2] : w[0];
+        const uint32_t wb = (word & 2) ? w[3] : w[1];
+        if (job < npairs) {
+          float u = u01_open0(wa);
+          float v = u01_open1(wb);
+          float rad = __fsqrt_rn(__fmul_rn(-2.0f, log_unit(u)));
+          float sn, cs;
+          sincos_2pi(v, &sn, &cs);
+          c0[r] = __fmul_rn(rad, cs);
+          c1[r] = __fmul_rn(rad, sn);
+        } else {
+          c0[r] = u01_open0(wa);
+        }
+      }
+    }
+    float dir[MAXD];
+#pragma unroll
+    for (int k = 0; k < MAXD; ++k) {
+      const int p = k >> 1;
+      dir[k] = __shfl_sync(0xffffffffu, (k & 1) ? c1[p / G] : c0[p / G], p % G, G);
+    }
+    float utv = c0[0];
+#pragma unroll
+    for (int r = 1; r < R; ++r)
+      if (npairs / G == r) utv = c0[r];
+    const float ut = __shfl_sync(0xffffffffu, utv, npairs % G, G);
+    float tmax = FLT_MAX, tmin = -FLT_MAX;
+    for (int f = gl; f < F; f += G) {
+      const float* col = At + f;
+      float a0 = col[0];
+      float ax = __fmul_rn(a0, x[0]);
+      float ad = __fmul_rn(a0, dir[0]);
+#pragma unroll
+      for (int k = 1; k < MAXD; ++k) {
+        if (k < dim) {
+          float ak = col[k * stride];
+          ax = __fmaf_rn(ak, x[k], ax);
+          ad = __fmaf_rn(ak, dir[k], ad);
+        }
+      }
+      float lb = __fsub_rn(bp[f], ax);
+      if (ad < 0.0f)
+        tmin = fmaxf(tmin, __fdiv_rn(lb, ad));
+      else if (ad > 0.0f)
+        tmax = fminf(tmax, __fdiv_rn(lb, ad));
+    }
+#pragma unroll
+    for (int o = G / 2; o; o >>= 1) {
+      tmin = fmaxf(tmin, __shfl_xor_sync(0xffffffffu, tmin, o, G));
+      tmax = fminf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o, G));
+    }
+    if (isinf(tmax) || isinf(tmin) || tmax < tmin) ok = false;
+    if (ok) {
+      double th = __dadd_rn(__dmul_rn((double)ut, __dsub_rn(__dmul_rn(0.999999, (double)tmax), (double)tmin)),
+                            (double)tmin);
+      float theta = __double2float_rn(th);
+#pragma unroll
+      for (int k = 0; k < MAXD; ++k)
+        if (k < dim) x[k] = __fmaf_rn(theta, dir[k], x[k]);
+    }
+  }
+  return ok;
+}
+
+// Writes coordinates gl, gl + G, ... of a group-replicated vector.
+template <int MAXD, int G>
+__device__ __forceinline__ void group_store(const float* x, int dim, int gl, float* __restrict__ dst, bool ok,
+                                            const float* __restrict__ fallback) {
+#pragma unroll
+  for (int r = 0; r < (MAXD + G - 1) / G; ++r) {
+    const int k = gl + r * G;
+    float v = 0.f;
+#pragma unroll
+    for (int j = 0; j < MAXD; ++j)
+      if (j == k) v = x[j];
+    if (k < dim) dst[k] = ok ? v : fallback[k];
+  }
+}
+
+// Shared-memory staging of one polytope for the group sampler: rows
+// k < dim of At at stride ST, then b at row MAXD. Sized (MAXD + 1) * ST floats.
+constexpr int kStageFaces8 = 2048;   // faces staged for dim <= 8
+constexpr int kStageFaces16 = 1024;  // faces staged for dim <= 16
+constexpr size_t kStageBytes = 9 * kStageFaces8 * sizeof(float);
+static_assert(9 * kStageFaces8 >= 17 * kStageFaces16, "staging buffer");
+
+template <int MAXD, int ST>
+__device__ __forceinline__ void stage_polytope(const float* __restrict__ At, int ldt, const float* __restrict__ b,
+                                               int F, int dim, float* sm) {
+  for (int i = threadIdx.x; i < dim * F; i += blockDim.x) {
+    const int k = i / F, f = i - k * F;
+    sm[k * ST + f] = At[(int64_t)k * ldt + f];
+  }
+  for (int f = threadIdx.x; f < F; f += blockDim.x) sm[MAXD * ST + f] = b[f];
+}
+
+// Chains [first, last) of one polytope by the whole block, G lanes per
+// chain; the trip count is uniform across the block (groups past `last`
+// repeat the last chain and store nothing). A failed chain stores `start`.
+template <int MAXD, int G, int ST>
+__device__ __forceinline__ void sample_chains(const float* __restrict__ At, int ldt, const float* __restrict__ b,
+                                              int F, int dim, const float* __restrict__ start, int first, int last,
+                                              int mixing, uint32_t k0, uint32_t k1, uint32_t stream,
+                                              float* __restrict__ out) {
+  const int lane = threadIdx.x & 31, gl = lane & (G - 1);
+  const int gid = (threadIdx.x >> 5) * (32 / G) + lane / G;
+  const int ngroups = (blockDim.x >> 5) * (32 / G);
+  for (int c0 = first; c0 < last; c0 += ngroups) {
+    const int chain = c0 + gid;
+    const int cc = chain < last ? chain : last - 1;
+    float x[MAXD];
+#pragma unroll
+    for (int k = 0; k < MAXD; ++k) x[k] = k < dim ? start[k] : 0.f;
+    const bool ok = run_chain_group<MAXD, G, ST>(At, ldt, b, F, dim, mixing, k0, k1, (uint32_t)cc, stream, x, gl);
+    if (chain < last) group_store<MAXD, G>(x, dim, gl, out + (int64_t)chain * dim, ok, start);
+  }
+}
+
+// Group width for `total` chains over `grid_warps` resident warps: 8 lanes
+// per chain when there are enough chains to fill the grid that way, wider
+// groups when there are few (the tail of an inflation).
+__host__ __device__ __forceinline__ int group_width(int64_t total, int64_t grid_warps) {
+  return total >= 8 * grid_warps ? 8 : total >= 4 * grid_warps ? 16 : 32;
+}
+
+// One polytope's chains [first, last) with the polytope staged in `sm` when
+// it fits (sm_ready: already staged), else read from global memory.
+template <int MAXD>
+__device__ __forceinline__ void sample_range(const float* __restrict__ At, int ldt, const float* __restrict__ b,
+                                             int F, int dim, const float* __restrict__ start, int first, int last,
+                                             int mixing, uint32_t k0, uint32_t k1, uint32_t stream,
+                                             float* __restrict__ out, int G, float* sm, bool staged) {
+  constexpr int ST = MAXD <= 8 ? kStageFaces8 : kStageFaces16;
+  if (staged) {
+    const float* sAt = sm;
+    const float* sb = sm + MAXD * ST;
+    if (G == 8)
+      sample_chains<MAXD, 8, ST>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
+    else if (G == 16)
+      sample_chains<MAXD, 16, ST>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
+    else
+      sample_chains<MAXD, 32, ST>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
+  } else {
+    if (G == 8)
+      sample_chains<MAXD, 8, 0>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out);
+    else if (G == 16)
+      sample_chains<MAXD, 16, 0>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out);
+    else
+      sample_chains<MAXD, 32, 0>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out);
+  }
+}
+
 }  // namespace csd

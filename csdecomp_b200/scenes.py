@@ -17,7 +17,7 @@ from __future__ import annotations
 
 import math
 from dataclasses import dataclass
-from typing import List, Optional, Tuple
+from typing import Callable, List, Optional, Tuple
 
 import numpy as np
 
@@ -197,7 +197,42 @@ def batch_scene(i: int, seed: int, keepout: float = 0.8) -> Scene:
                      keepout=keepout, arm_spacing=1.4, description=f"14-DOF two-arm, {n} world primitives")
 
 
+def batch_scene_seeds(count: int, seed: int = BATCH_SEED) -> List[int]:
+    rng = np.random.default_rng(seed)
+    return [int(rng.integers(1 << 30)) for _ in range(count)]
+
+
 def batch_scenes(count: int = 256, seed: int = BATCH_SEED, keepout: float = 0.8) -> List[Scene]:
     """`count` scenes for the batched-EI-ZO workload (see batch_scene)."""
+    return [batch_scene(i, s, keepout) for i, s in enumerate(batch_scene_seeds(count, seed))]
+
+
+def seed_edges(scene: Scene, count: int, seed: int, check_points: Callable, check_edges: Callable,
+               length: Tuple[float, float] = (0.05, 1.0), draws: int = 8, per_draw: int = 4096) -> list:
+    """Up to `count` free seed edges: a free q0 (uniform in the joint limits),
+    a direction uniform on the sphere and a length U[length]; kept iff q1 lies
+    strictly inside the limits and the edge is collision free. check_points(Q
+    [n, d]) -> uint8 [n] and check_edges(Q0, Q1) -> bool [n] are the checkers.
+    Returns fewer than `count` edges only when `draws` batches of `per_draw`
+    configurations did not yield enough."""
     rng = np.random.default_rng(seed)
-    return [batch_scene(i, int(rng.integers(1 << 30)), keepout) for i in range(count)]
+    lo, hi = scene.lower(), scene.upper()
+    out: list = []
+    for _ in range(draws):
+        q = scene.random_configs(per_draw, int(rng.integers(1 << 30)))
+        free = q[np.asarray(check_points(q)) == 1]
+        if len(free) == 0:
+            continue
+        d = rng.normal(size=free.shape)
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        q1 = (free + rng.uniform(length[0], length[1], len(free))[:, None] * d).astype(np.float32)
+        inside = np.all((q1 > lo) & (q1 < hi), axis=1)
+        a, b = np.ascontiguousarray(free[inside]), np.ascontiguousarray(q1[inside])
+        if len(a) == 0:
+            continue
+        ok = np.asarray(check_edges(a, b)).astype(bool)
+        for j in np.nonzero(ok)[0]:
+            out.append((a[j].copy(), b[j].copy()))
+            if len(out) == count:
+                return out
+    return out

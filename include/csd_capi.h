@@ -219,6 +219,17 @@ csd_status_t csd_batch_inflate(csd_batch_t batch, int32_t n, const int32_t* slot
                                const float* ends, const float* domain_A, const float* domain_b,
                                const int32_t* domain_face_offsets, float* A_out, float* b_out, int32_t* num_faces,
                                int32_t* num_iterations, float* device_ms);
+/* Configurations the last csd_batch_inflate checked per slot (hit-and-run
+ * samples plus bisection points), for throughput accounting. */
+csd_status_t csd_batch_configs_checked(csd_batch_t h, int32_t n, int64_t* configs);
+
+/* Profiling mode: while enabled, csd_batch_inflate launches each iteration's
+ * stages one by one (no graph) with events between them and accumulates the
+ * GPU time of each stage: [sample, check, compact, bisect, faces, step].
+ * Enabling (or disabling) resets the accumulators. */
+csd_status_t csd_batch_set_profiling(csd_batch_t h, int32_t enable);
+csd_status_t csd_batch_stage_ms(csd_batch_t h, float* stage_ms /* [6] */);
+
 csd_status_t csd_batch_destroy(csd_batch_t batch);
 
 /* Allocation-free EI-ZO (no counterpart in the reference). Same inputs,
