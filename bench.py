@@ -288,6 +288,7 @@ def main():
     dev_s, wall_s, configs, launches = 0.0, 0.0, 0, 0
     faces, iters, h2d, d2h = [], [], 0, 0
     first_regions = None
+    torch.cuda.nvtx.range_push("timed")
     with ClockSampler(local) as clk:
         for s in range(args.warmup, steps_total):
             q0s, q1s = step_inputs(s)
@@ -307,6 +308,7 @@ def main():
             h2d += sum(sc.dim * 8 + d.A().nbytes + d.b().nbytes for sc, d in zip(scs, doms)) + 8 * NUM_SLOTS + 4
             d2h += sum(r.A().nbytes + r.b().nbytes for r in regions) + 16 * n_graph + 120 * NUM_SLOTS
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     # plain GPU form (one CudaEdgeInflator call per region) on the first timed step's inputs
     plain_s, identical = 0.0, True
     st = torch.cuda.current_stream()

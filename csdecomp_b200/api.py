@@ -445,8 +445,12 @@ class BatchedEdgeInflator:
     slot has its own plant, segment and domain and yields exactly the region
     CudaEdgeInflator.inflateEdge would for the same inputs (no voxels)."""
 
+    SAMPLE_VARIANTS = ("1 face/trip, 2 blocks/SM", "2 faces/trip, 2 blocks/SM", "1 face/trip, 3 blocks/SM",
+                       "2 faces/trip, 3 blocks/SM")
+    CHECK_ITEM_CAPS = (32, 128, 512)
+
     def __init__(self, plants: Sequence[MinimalPlant], options: EizoOptions, max_slots: int,
-                 face_capacity: int = MAX_NUM_FACES):
+                 face_capacity: int = MAX_NUM_FACES, autotune_iterations: int = 4):
         self._plants = list(plants)
         self._handles = [plant_handle(p) for p in self._plants]
         self._options = options
@@ -459,6 +463,28 @@ class BatchedEdgeInflator:
                                          self._capacity, ctypes.byref(h)))
         self._handle = h
         self.last_iterations = None
+        if autotune_iterations:
+            self.autotune(autotune_iterations)
+
+    def autotune(self, iterations: int = 4) -> None:
+        """Time every sampler variant and check work-item cap on the first
+        `iterations` iterations of the next inflate and keep the fastest."""
+        C.check(C.lib().csd_batch_autotune(self._handle, int(iterations)))
+
+    def set_shapes(self, sample_variant: int, check_item_cap: int) -> None:
+        """Fix the sampler variant (index into SAMPLE_VARIANTS) and the check
+        work-item cap instead of tuning."""
+        C.check(C.lib().csd_batch_set_shapes(self._handle, int(sample_variant), int(check_item_cap)))
+
+    def tuning(self) -> dict:
+        sv, cap, nv = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        ms = np.zeros(16, np.float32)
+        C.check(C.lib().csd_batch_tuning(self._handle, ctypes.byref(sv), ctypes.byref(cap), C.ptr(ms),
+                                         ctypes.byref(nv)))
+        ns = len(self.SAMPLE_VARIANTS)
+        return {"sample_variant": self.SAMPLE_VARIANTS[sv.value], "check_item_cap": cap.value,
+                "sample_ms": dict(zip(self.SAMPLE_VARIANTS, ms[:ns].tolist())),
+                "check_ms": dict(zip(self.CHECK_ITEM_CAPS, ms[ns:nv.value].tolist()))}
 
     def inflate(self, slot_plant: Sequence[int], line_starts: Sequence[np.ndarray], line_ends: Sequence[np.ndarray],
                 domains: Sequence[HPolyhedron]) -> List[HPolyhedron]:
@@ -502,6 +528,17 @@ class BatchedEdgeInflator:
         """Launch stage by stage with events (no graph) and accumulate each
         stage's GPU time; toggling resets the accumulators."""
         C.check(C.lib().csd_batch_set_profiling(self._handle, int(bool(enable))))
+
+    def iteration_profile(self):
+        """(stage_ms [iterations, 6], active slots [iterations]) of the last
+        inflate in profiling mode."""
+        cnt = ctypes.c_int32(0)
+        C.check(C.lib().csd_batch_iteration_profile(self._handle, 0, None, None, ctypes.byref(cnt)))
+        ms = np.zeros((cnt.value, 6), np.float32)
+        act = np.zeros(cnt.value, np.int32)
+        C.check(C.lib().csd_batch_iteration_profile(self._handle, cnt.value, C.ptr(ms), C.ptr(act),
+                                                    ctypes.byref(cnt)))
+        return ms, act
 
     def stage_ms(self) -> dict:
         ms = np.zeros(6, np.float32)

@@ -90,7 +90,8 @@ static __device__ __forceinline__ int item_size(int64_t total, int cap, int nw) 
 // takes a contiguous run of items, stages each new slot's region (At, b) in
 // shared memory and runs its chains G lanes per chain (G from the total
 // chain count: 8 when the batch is full, up to 32 in the tail).
-__global__ void __launch_bounds__(256) batch_sample_kernel(BatchArgs a) {
+template <int U, int MINB>
+__global__ void __launch_bounds__(256, MINB) batch_sample_kernel(BatchArgs a) {
   extern __shared__ float smf[];
   const int N = a.n_tab[a.it->k];
   const int64_t total = (int64_t)a.it->num_act * N;
@@ -122,9 +123,9 @@ __global__ void __launch_bounds__(256) batch_sample_kernel(BatchArgs a) {
       staged = slot;
     }
     if (dim <= 8)
-      sample_range<8>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, G, smf, fits);
+      sample_range<8, U>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, G, smf, fits);
     else
-      sample_range<16>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, G, smf, fits);
+      sample_range<16, U>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, G, smf, fits);
   }
 }
 
@@ -305,6 +306,24 @@ __global__ void __launch_bounds__(1024) batch_step_kernel(BatchArgs a) {
   }
 }
 
+// Sampler variants the autotuner chooses from: U faces per lane and trip,
+// MINB resident blocks per SM (register cap).
+using SampleFn = void (*)(BatchArgs);
+struct SampleVariant {
+  SampleFn fn;
+  int u, minb;
+};
+static const SampleVariant kSampleVariants[] = {
+    {batch_sample_kernel<1, 2>, 1, 2},
+    {batch_sample_kernel<2, 2>, 2, 2},
+    {batch_sample_kernel<1, 3>, 1, 3},
+    {batch_sample_kernel<2, 3>, 2, 3},
+};
+constexpr int kNumSampleVariants = (int)(sizeof(kSampleVariants) / sizeof(kSampleVariants[0]));
+// Largest check work item (configurations) the autotuner chooses from.
+constexpr int kCheckItemCaps[] = {32, 128, 512};
+constexpr int kNumCheckVariants = (int)(sizeof(kCheckItemCaps) / sizeof(kCheckItemCaps[0]));
+
 }  // namespace csd
 
 // --------------------------------------------------------------------- handle
@@ -317,19 +336,26 @@ struct csd_batch_s {
   int static_floats = 0;
   size_t check_smem = 0;
   int check_grid = 0, bisect_grid = 0;
-  int cfg_max = 256, part_max = 64, sample_grid = 0;
+  int cfg_max = 128, part_max = 64;
+  int sample_variant = 0;
+  int sample_grid[csd::kNumSampleVariants] = {};
+  int tune_iters = 0;                               // iterations of the next inflate to tune on
+  double tune_ms[csd::kNumSampleVariants + csd::kNumCheckVariants] = {};
+  int tuned_iters = 0;
   std::vector<int> n_tab, m_tab;
   std::vector<float> thr_tab;
   csd::DevBuf plants_dev, slots_dev, tabs, fpool, bpool, iter, act;
   std::vector<csd::SlotState> host_slots;
   std::vector<int> act_host;
   cudaGraphExec_t graph = nullptr;
-  int graph_slots = -1;
+  int graph_slots = -1, graph_cfg = -1, graph_variant = -1;
   cudaStream_t graph_stream = nullptr;
   csd::BatchIter* host_iter = nullptr;
   bool profile = false;         // launch stage by stage with events instead of the graph
   cudaEvent_t ev[7] = {};
   double stage_ms[6] = {};
+  std::vector<float> iter_ms;   // profiling mode: [iteration][6] of the last inflate
+  std::vector<int> iter_active; // slots active at the start of each iteration
   ~csd_batch_s() {
     for (cudaEvent_t e : ev)
       if (e) cudaEventDestroy(e);
@@ -347,7 +373,7 @@ namespace {
 // between the stages for the profiling mode.
 void launch_iteration(csd_batch_s* h, int num_slots, const BatchArgs& a, cudaStream_t s, cudaEvent_t* ev) {
   if (ev) cudaEventRecord(ev[0], s);
-  batch_sample_kernel<<<h->sample_grid, 256, kStageBytes, s>>>(a);
+  kSampleVariants[h->sample_variant].fn<<<h->sample_grid[h->sample_variant], 256, kStageBytes, s>>>(a);
   if (ev) cudaEventRecord(ev[1], s);
   if (h->sm)
     batch_check_kernel<true><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->static_floats);
@@ -368,7 +394,8 @@ void launch_iteration(csd_batch_s* h, int num_slots, const BatchArgs& a, cudaStr
 }
 
 csd_status_t build_graph(csd_batch_s* h, int num_slots, const BatchArgs& a) {
-  if (h->graph && h->graph_slots == num_slots) return CSD_OK;
+  if (h->graph && h->graph_slots == num_slots && h->graph_cfg == a.cfg_max && h->graph_variant == h->sample_variant)
+    return CSD_OK;
   if (h->graph) {
     cudaGraphExecDestroy(h->graph);
     h->graph = nullptr;
@@ -389,6 +416,8 @@ csd_status_t build_graph(csd_batch_s* h, int num_slots, const BatchArgs& a) {
     return CSD_ERR_CUDA;
   }
   h->graph_slots = num_slots;
+  h->graph_cfg = a.cfg_max;
+  h->graph_variant = h->sample_variant;
   return CSD_OK;
 }
 
@@ -453,12 +482,12 @@ csd_status_t csd_batch_create(const csd_plant_t* plants, int32_t num_plants, int
   }
   h->check_grid = g1;
   h->bisect_grid = g2;
-  CSD_CUDA_TRY(cudaFuncSetAttribute(batch_sample_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)kStageBytes));
-  {
+  for (int v = 0; v < kNumSampleVariants; ++v) {
+    CSD_CUDA_TRY(cudaFuncSetAttribute(kSampleVariants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kStageBytes));
     int per_sm = 0;
-    CSD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_sample_kernel, 256, kStageBytes));
-    h->sample_grid = device_sm_count() * std::max(1, per_sm);
+    CSD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kSampleVariants[v].fn, 256, kStageBytes));
+    h->sample_grid[v] = device_sm_count() * std::max(1, per_sm);
   }
   // buffers
   const size_t D = (size_t)h->max_dim, np = o->num_particles, cap = (size_t)face_capacity;
@@ -615,8 +644,63 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
     CSD_CUDA_TRY(cudaEventCreate(&ev1));
     CSD_CUDA_TRY(cudaEventRecord(ev0, st));
   }
+  h->iter_ms.clear();
+  h->iter_active.clear();
+  int active_now = n;
   for (uint32_t k = 0; k < h->opt.max_iterations; ++k) {
-    if (h->profile) {
+    if (h->tune_iters > 0) {
+      // every sampler variant and check item size on this iteration's inputs
+      // (both stages are idempotent: a rerun writes the same samples and
+      // verdicts), then the rest of the iteration as usual
+      if (!h->ev[0])
+        for (cudaEvent_t& e : h->ev) CSD_CUDA_TRY(cudaEventCreate(&e));
+      std::vector<cudaEvent_t> tev(2 * (kNumSampleVariants + kNumCheckVariants));
+      for (cudaEvent_t& e : tev) CSD_CUDA_TRY(cudaEventCreate(&e));
+      int j = 0;
+      for (int v = 0; v < kNumSampleVariants; ++v, ++j) {
+        cudaEventRecord(tev[2 * j], st);
+        kSampleVariants[v].fn<<<h->sample_grid[v], 256, kStageBytes, st>>>(a);
+        cudaEventRecord(tev[2 * j + 1], st);
+      }
+      for (int c = 0; c < kNumCheckVariants; ++c, ++j) {
+        BatchArgs ac = a;
+        ac.cfg_max = kCheckItemCaps[c];
+        cudaEventRecord(tev[2 * j], st);
+        if (h->sm)
+          batch_check_kernel<true><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, st>>>(ac, h->static_floats);
+        else
+          batch_check_kernel<false><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, st>>>(ac, 0);
+        cudaEventRecord(tev[2 * j + 1], st);
+      }
+      batch_compact_kernel<<<n, 1024, 0, st>>>(a);
+      if (h->sm)
+        batch_bisect_kernel<true><<<h->bisect_grid, 32 * kWarpsPerBlock, h->check_smem, st>>>(a, h->static_floats);
+      else
+        batch_bisect_kernel<false><<<h->bisect_grid, 32 * kWarpsPerBlock, h->check_smem, st>>>(a, 0);
+      batch_faces_kernel<<<n, 1024, 0, st>>>(a);
+      batch_step_kernel<<<1, 1024, 0, st>>>(a);
+      CSD_CUDA_TRY(cudaGetLastError());
+      CSD_CUDA_TRY(cudaStreamSynchronize(st));
+      for (int q = 0; q < j; ++q) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, tev[2 * q], tev[2 * q + 1]);
+        h->tune_ms[q] += ms;
+      }
+      for (cudaEvent_t& e : tev) cudaEventDestroy(e);
+      ++h->tuned_iters;
+      if (--h->tune_iters == 0) {
+        int bs = 0, bc = 0;
+        for (int v = 1; v < kNumSampleVariants; ++v)
+          if (h->tune_ms[v] < h->tune_ms[bs]) bs = v;
+        for (int c = 1; c < kNumCheckVariants; ++c)
+          if (h->tune_ms[kNumSampleVariants + c] < h->tune_ms[kNumSampleVariants + bc]) bc = c;
+        h->sample_variant = bs;
+        h->cfg_max = kCheckItemCaps[bc];
+        a.cfg_max = h->cfg_max;
+        h->graph_slots = -1;  // recapture with the chosen shapes
+        if ((s = build_graph(h, n, a))) return s;
+      }
+    } else if (h->profile) {
       launch_iteration(h, n, a, st, h->ev);
       CSD_CUDA_TRY(cudaGetLastError());
       CSD_CUDA_TRY(cudaEventSynchronize(h->ev[6]));
@@ -624,13 +708,16 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
         float ms = 0.f;
         cudaEventElapsedTime(&ms, h->ev[j], h->ev[j + 1]);
         h->stage_ms[j] += ms;
+        h->iter_ms.push_back(ms);
       }
+      h->iter_active.push_back(active_now);
     } else {
       CSD_CUDA_TRY(cudaGraphLaunch(h->graph, st));
     }
     CSD_CUDA_TRY(cudaMemcpyAsync(h->host_iter, h->iter.ptr, sizeof(BatchIter), cudaMemcpyDeviceToHost, st));
     CSD_CUDA_TRY(cudaStreamSynchronize(st));
-    if (h->host_iter->last_active == 0) break;
+    active_now = h->host_iter->last_active;
+    if (active_now == 0) break;
   }
   if (device_ms) {
     CSD_CUDA_TRY(cudaEventRecord(ev1, st));
@@ -674,6 +761,46 @@ csd_status_t csd_batch_set_profiling(csd_batch_t h, int32_t enable) {
 csd_status_t csd_batch_stage_ms(csd_batch_t h, float* ms) {
   CSD_CHECK(h && ms, CSD_ERR_INVALID, "null argument");
   for (int j = 0; j < 6; ++j) ms[j] = (float)h->stage_ms[j];
+  return CSD_OK;
+}
+
+csd_status_t csd_batch_autotune(csd_batch_t h, int32_t iterations) {
+  CSD_CHECK(h && iterations >= 0, CSD_ERR_INVALID, "bad autotune arguments");
+  h->tune_iters = iterations;
+  h->tuned_iters = 0;
+  for (double& x : h->tune_ms) x = 0.0;
+  return CSD_OK;
+}
+
+csd_status_t csd_batch_set_shapes(csd_batch_t h, int32_t sample_variant, int32_t check_item_cap) {
+  CSD_CHECK(h && sample_variant >= 0 && sample_variant < kNumSampleVariants && check_item_cap >= 8 &&
+                check_item_cap % 8 == 0,
+            CSD_ERR_INVALID, "bad shapes: sampler variant in [0, 4), check item cap a positive multiple of 8");
+  h->sample_variant = sample_variant;
+  h->cfg_max = check_item_cap;
+  return CSD_OK;
+}
+
+csd_status_t csd_batch_tuning(csd_batch_t h, int32_t* sample_variant, int32_t* check_item_cap, float* variant_ms,
+                              int32_t* num_variants) {
+  CSD_CHECK(h, CSD_ERR_INVALID, "null batch");
+  if (sample_variant) *sample_variant = h->sample_variant;
+  if (check_item_cap) *check_item_cap = h->cfg_max;
+  if (num_variants) *num_variants = kNumSampleVariants + kNumCheckVariants;
+  if (variant_ms)
+    for (int q = 0; q < kNumSampleVariants + kNumCheckVariants; ++q) variant_ms[q] = (float)h->tune_ms[q];
+  return CSD_OK;
+}
+
+csd_status_t csd_batch_iteration_profile(csd_batch_t h, int32_t cap, float* stage_ms, int32_t* active,
+                                         int32_t* count) {
+  CSD_CHECK(h && count && (cap == 0 || (stage_ms && active)), CSD_ERR_INVALID, "null argument");
+  const int n = (int)h->iter_active.size();
+  *count = n;
+  for (int i = 0; i < std::min(n, (int)cap); ++i) {
+    active[i] = h->iter_active[i];
+    for (int j = 0; j < 6; ++j) stage_ms[i * 6 + j] = h->iter_ms[(size_t)i * 6 + j];
+  }
   return CSD_OK;
 }
 

@@ -65,12 +65,12 @@ __global__ void __launch_bounds__(256) hit_and_run_group_kernel(const float* __r
     const bool staged = F <= kStageFaces8;
     if (staged) stage_polytope<8, kStageFaces8>(At, ldt, b, F, dim, smf);
     __syncthreads();
-    sample_range<8>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out, G, smf, staged);
+    sample_range<8, 1>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out, G, smf, staged);
   } else {
     const bool staged = F <= kStageFaces16;
     if (staged) stage_polytope<16, kStageFaces16>(At, ldt, b, F, dim, smf);
     __syncthreads();
-    sample_range<16>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out, G, smf, staged);
+    sample_range<16, 1>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out, G, smf, staged);
   }
 }
 

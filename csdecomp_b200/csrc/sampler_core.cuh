@@ -62,7 +62,7 @@ __device__ __forceinline__ bool run_chain(const float* __restrict__ Ap, const fl
 // the group's lanes. A chain whose line search fails keeps stepping without
 // moving (so the groups of a warp stay convergent for the shuffles) and
 // returns false.
-template <int MAXD, int G, int ST>
+template <int MAXD, int G, int ST, int U = 1>
 __device__ __forceinline__ bool run_chain_group(const float* __restrict__ At, int ldt, const float* __restrict__ bp,
                                                 int F, int dim, int mixing, uint32_t k0, uint32_t k1,
                                                 uint32_t chain, uint32_t stream, float* x, int gl) {
@@ -108,24 +108,31 @@ __device__ __forceinline__ bool run_chain_group(const float* __restrict__ At, in
       if (npairs / G == r) utv = c0[r];
     const float ut = __shfl_sync(0xffffffffu, utv, npairs % G, G);
     float tmax = FLT_MAX, tmin = -FLT_MAX;
-    for (int f = gl; f < F; f += G) {
-      const float* col = At + f;
-      float a0 = col[0];
-      float ax = __fmul_rn(a0, x[0]);
-      float ad = __fmul_rn(a0, dir[0]);
+    // U faces per lane and trip (independent dot products for the scheduler)
+    for (int f0 = gl; f0 < F; f0 += G * U) {
 #pragma unroll
-      for (int k = 1; k < MAXD; ++k) {
-        if (k < dim) {
-          float ak = col[k * stride];
-          ax = __fmaf_rn(ak, x[k], ax);
-          ad = __fmaf_rn(ak, dir[k], ad);
+      for (int u = 0; u < U; ++u) {
+        const int f = f0 + u * G;
+        if (U == 1 || f < F) {
+          const float* col = At + f;
+          float a0 = col[0];
+          float ax = __fmul_rn(a0, x[0]);
+          float ad = __fmul_rn(a0, dir[0]);
+#pragma unroll
+          for (int k = 1; k < MAXD; ++k) {
+            if (k < dim) {
+              float ak = col[k * stride];
+              ax = __fmaf_rn(ak, x[k], ax);
+              ad = __fmaf_rn(ak, dir[k], ad);
+            }
+          }
+          float lb = __fsub_rn(bp[f], ax);
+          if (ad < 0.0f)
+            tmin = fmaxf(tmin, __fdiv_rn(lb, ad));
+          else if (ad > 0.0f)
+            tmax = fminf(tmax, __fdiv_rn(lb, ad));
         }
       }
-      float lb = __fsub_rn(bp[f], ax);
-      if (ad < 0.0f)
-        tmin = fmaxf(tmin, __fdiv_rn(lb, ad));
-      else if (ad > 0.0f)
-        tmax = fminf(tmax, __fdiv_rn(lb, ad));
     }
 #pragma unroll
     for (int o = G / 2; o; o >>= 1) {
@@ -180,7 +187,7 @@ __device__ __forceinline__ void stage_polytope(const float* __restrict__ At, int
 // Chains [first, last) of one polytope by the whole block, G lanes per
 // chain; the trip count is uniform across the block (groups past `last`
 // repeat the last chain and store nothing). A failed chain stores `start`.
-template <int MAXD, int G, int ST>
+template <int MAXD, int G, int ST, int U>
 __device__ __forceinline__ void sample_chains(const float* __restrict__ At, int ldt, const float* __restrict__ b,
                                               int F, int dim, const float* __restrict__ start, int first, int last,
                                               int mixing, uint32_t k0, uint32_t k1, uint32_t stream,
@@ -194,7 +201,7 @@ __device__ __forceinline__ void sample_chains(const float* __restrict__ At, int 
     float x[MAXD];
 #pragma unroll
     for (int k = 0; k < MAXD; ++k) x[k] = k < dim ? start[k] : 0.f;
-    const bool ok = run_chain_group<MAXD, G, ST>(At, ldt, b, F, dim, mixing, k0, k1, (uint32_t)cc, stream, x, gl);
+    const bool ok = run_chain_group<MAXD, G, ST, U>(At, ldt, b, F, dim, mixing, k0, k1, (uint32_t)cc, stream, x, gl);
     if (chain < last) group_store<MAXD, G>(x, dim, gl, out + (int64_t)chain * dim, ok, start);
   }
 }
@@ -208,7 +215,7 @@ __host__ __device__ __forceinline__ int group_width(int64_t total, int64_t grid_
 
 // One polytope's chains [first, last) with the polytope staged in `sm` when
 // it fits (sm_ready: already staged), else read from global memory.
-template <int MAXD>
+template <int MAXD, int U>
 __device__ __forceinline__ void sample_range(const float* __restrict__ At, int ldt, const float* __restrict__ b,
                                              int F, int dim, const float* __restrict__ start, int first, int last,
                                              int mixing, uint32_t k0, uint32_t k1, uint32_t stream,
@@ -218,18 +225,18 @@ __device__ __forceinline__ void sample_range(const float* __restrict__ At, int l
     const float* sAt = sm;
     const float* sb = sm + MAXD * ST;
     if (G == 8)
-      sample_chains<MAXD, 8, ST>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
+      sample_chains<MAXD, 8, ST, U>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
     else if (G == 16)
-      sample_chains<MAXD, 16, ST>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
+      sample_chains<MAXD, 16, ST, U>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
     else
-      sample_chains<MAXD, 32, ST>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
+      sample_chains<MAXD, 32, ST, U>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
   } else {
     if (G == 8)
-      sample_chains<MAXD, 8, 0>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out);
+      sample_chains<MAXD, 8, 0, U>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out);
     else if (G == 16)
-      sample_chains<MAXD, 16, 0>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out);
+      sample_chains<MAXD, 16, 0, U>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out);
     else
-      sample_chains<MAXD, 32, 0>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out);
+      sample_chains<MAXD, 32, 0, U>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out);
   }
 }
 

@@ -1,0 +1,204 @@
+"""Small, reproducible launches of the hot kernels for profiler captures.
+
+  python -m csdecomp_b200.profile_cases check_points [--configs N]
+      one warm-up and one timed check_points launch on N collision-free
+      configurations of the 7-DOF arm (80 spheres + 4 capsules) in 200 world
+      primitives (every pair evaluated: the full sweep)
+  python -m csdecomp_b200.profile_cases batch [--slots S] [--iterations I]
+      [--sample-variant V] [--check-item-cap C]
+      S inflations of the batched EI-ZO workload (first S scenes), at most I
+      iterations, launched stage by stage (profiling mode) with the given
+      sampler variant and check work-item cap (defaults: the shapes the
+      autotuner picks on a B200)
+
+  python -m csdecomp_b200.profile_cases point_check [--configs N]
+      config 1: 7-DOF arm, 40 spheres, 20 world boxes; N uniform configurations
+  python -m csdecomp_b200.profile_cases edge_check [--edges E]
+      config 2: 7-DOF arm, 80 spheres + 4 capsules, 200 world primitives; E
+      segments with endpoints uniform in the joint limits, 0.01 rad step
+  python -m csdecomp_b200.profile_cases eizo_single [--regions R]
+      config 3: R single inflations (CudaEdgeInflator) on the 7-DOF /
+      200-primitive scene, seed edges U[0.1, 0.5] rad
+
+Each prints the device time of what it ran (CUDA events, after one warm-up).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+
+import numpy as np
+
+
+def check_points(n: int) -> None:
+    import torch
+    import csdecomp_b200 as csd
+    from csdecomp_b200 import _capi as C
+    from csdecomp_b200 import scenes
+    sc = scenes.edge_check_scene(keepout=0.8)
+    h = csd.plant_handle(sc.plant)
+    q = sc.random_configs(200000, 77)
+    free = q[csd.CheckCollisionFreeCuda(q.T, sc.plant) == 1]
+    qf = np.ascontiguousarray(np.tile(free, (int(np.ceil(n / len(free))), 1))[:n])
+    tq = torch.from_numpy(qf).cuda()
+    out = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream()
+    ms = []
+    for _ in range(2):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        C.check(C.lib().csd_check_points(h.handle, C.ptr(tq.data_ptr()), ctypes.c_int64(n), None, 0,
+                                         ctypes.c_float(0), None, 0, C.ptr(out.data_ptr()), C.CSD_PTR_DEVICE,
+                                         ctypes.c_void_p(st.cuda_stream)))
+        e1.record(st)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    assert int(out.sum().item()) == n
+    print(json.dumps({"case": "check_points", "configs": n, "flop_per_config": h.flops()["total"],
+                      "launch_ms": ms[-1]}))
+
+
+def batch(slots: int, iterations: int, sample_variant: int, check_item_cap: int) -> None:
+    import csdecomp_b200 as csd
+    from csdecomp_b200 import scenes
+    eizo = dict(num_particles=2000, mixing_steps=50, bisection_steps=9, max_hyperplanes_per_iteration=10,
+                epsilon=0.01, delta=0.05, tau=0.5, max_iterations=iterations, configuration_margin=0.01, seed=1337)
+    scs, edges = [], []
+    seeds = scenes.batch_scene_seeds(4 * slots + 64)
+    for i, s in enumerate(seeds):
+        sc = scenes.batch_scene(i, s)
+        e = scenes.seed_edges(sc, 1, 3000 + 101 * i, lambda q: csd.CheckCollisionFreeCuda(q.T, sc.plant),
+                              lambda a, b: csd.CheckEdgesCollisionFreeCuda(a.T, b.T, sc.plant))
+        if e:
+            scs.append(sc)
+            edges.append(e[0])
+        if len(scs) == slots:
+            break
+    doms = []
+    for sc in scs:
+        d = csd.HPolyhedron()
+        d.MakeBox(sc.lower(), sc.upper())
+        doms.append(d)
+    b = csd.BatchedEdgeInflator([sc.plant for sc in scs], csd.EizoOptions(**eizo), max_slots=len(scs),
+                                face_capacity=4000, autotune_iterations=0)
+    b.set_shapes(sample_variant, check_item_cap)
+    b.set_profiling(True)
+    b.inflate(list(range(len(scs))), [e[0] for e in edges], [e[1] for e in edges], doms)
+    print(json.dumps({"case": "batch", "slots": len(scs), "stage_ms": b.stage_ms(),
+                      "iterations": b.last_iterations.tolist()}))
+
+
+def _timed(fn, reps: int = 3):
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    best = None
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        out = fn()
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    return best, out
+
+
+def point_check(n: int) -> None:
+    import torch
+    import csdecomp_b200 as csd
+    from csdecomp_b200 import _capi as C
+    from csdecomp_b200 import scenes
+    sc = scenes.point_check_scene()
+    h = csd.plant_handle(sc.plant)
+    q = torch.from_numpy(np.ascontiguousarray(sc.random_configs(n, 5))).cuda()
+    out = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream()
+
+    def run():
+        C.check(C.lib().csd_check_points(h.handle, C.ptr(q.data_ptr()), ctypes.c_int64(n), None, 0,
+                                         ctypes.c_float(0), None, 0, C.ptr(out.data_ptr()), C.CSD_PTR_DEVICE,
+                                         ctypes.c_void_p(st.cuda_stream)))
+    ms, _ = _timed(run)
+    print(json.dumps({"case": "point_check", "configs": n, "ms": ms, "configs_per_s": n / ms * 1e3,
+                      "free_fraction": float(out.float().mean().item())}))
+
+
+def edge_check(n: int) -> None:
+    import torch
+    import csdecomp_b200 as csd
+    from csdecomp_b200 import _capi as C
+    from csdecomp_b200 import scenes
+    sc = scenes.edge_check_scene()
+    h = csd.plant_handle(sc.plant)
+    a = torch.from_numpy(np.ascontiguousarray(sc.random_configs(n, 6))).cuda()
+    b = torch.from_numpy(np.ascontiguousarray(sc.random_configs(n, 7))).cuda()
+    out = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    pts = torch.zeros(n, dtype=torch.int64, device="cuda")
+    st = torch.cuda.current_stream()
+
+    def run():
+        C.check(C.lib().csd_check_edges(h.handle, C.ptr(a.data_ptr()), C.ptr(b.data_ptr()), ctypes.c_int64(n),
+                                        ctypes.c_float(0.01), C.CSD_EDGE_L2_REF, C.ptr(out.data_ptr()),
+                                        C.ptr(pts.data_ptr()), C.CSD_PTR_DEVICE, ctypes.c_void_p(st.cuda_stream)))
+    ms, _ = _timed(run)
+    print(json.dumps({"case": "edge_check", "edges": n, "ms": ms, "edges_per_s": n / ms * 1e3,
+                      "free_fraction": float(out.float().mean().item()),
+                      "points_checked": int(pts.sum().item())}))
+
+
+def eizo_single(regions: int) -> None:
+    import torch
+    import csdecomp_b200 as csd
+    from csdecomp_b200 import scenes
+    sc = scenes.edge_check_scene(keepout=0.8)
+    edges = scenes.seed_edges(sc, regions + 1, 3000, lambda q: csd.CheckCollisionFreeCuda(q.T, sc.plant),
+                              lambda x, y: csd.CheckEdgesCollisionFreeCuda(x.T, y.T, sc.plant), length=(0.1, 0.5))
+    dom = csd.HPolyhedron()
+    dom.MakeBox(sc.lower(), sc.upper())
+    opt = csd.EizoOptions(num_particles=2000, mixing_steps=50, bisection_steps=9, max_hyperplanes_per_iteration=10,
+                          epsilon=0.01, delta=0.05, tau=0.5, max_iterations=500, configuration_margin=0.01,
+                          seed=1337)
+    inf = csd.CudaEdgeInflator(sc.plant, sc.inspector.robot_geometry_ids, opt, dom)
+    inf.inflateEdge(edges[0][0], edges[0][1], None, 0.0, verbose=False)
+    st = torch.cuda.current_stream()
+    total, faces = 0.0, 0
+    for q0, q1 in edges[1:]:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        P = inf.inflateEdge(q0, q1, None, 0.0, verbose=False)
+        e1.record(st)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+        faces += P.A().shape[0]
+    print(json.dumps({"case": "eizo_single", "regions": regions, "ms": total, "regions_per_s": regions / total * 1e3,
+                      "mean_faces": faces / regions}))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["check_points", "batch", "point_check", "edge_check", "eizo_single"])
+    ap.add_argument("--configs", type=int, default=1 << 20)
+    ap.add_argument("--slots", type=int, default=24)
+    ap.add_argument("--edges", type=int, default=100000)
+    ap.add_argument("--regions", type=int, default=20)
+    ap.add_argument("--iterations", type=int, default=12)
+    ap.add_argument("--sample-variant", type=int, default=3)
+    ap.add_argument("--check-item-cap", type=int, default=128)
+    a = ap.parse_args()
+    if a.case == "check_points":
+        check_points(a.configs)
+    elif a.case == "point_check":
+        point_check(a.configs)
+    elif a.case == "edge_check":
+        edge_check(a.edges)
+    elif a.case == "eizo_single":
+        eizo_single(a.regions)
+    else:
+        batch(a.slots, a.iterations, a.sample_variant, a.check_item_cap)
+
+
+if __name__ == "__main__":
+    main()

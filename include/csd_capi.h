@@ -229,6 +229,24 @@ csd_status_t csd_batch_configs_checked(csd_batch_t h, int32_t n, int64_t* config
  * Enabling (or disabling) resets the accumulators. */
 csd_status_t csd_batch_set_profiling(csd_batch_t h, int32_t enable);
 csd_status_t csd_batch_stage_ms(csd_batch_t h, float* stage_ms /* [6] */);
+/* Autotuner: during the first `iterations` iterations of the next
+ * csd_batch_inflate, every sampler variant (faces per lane and trip x
+ * resident blocks per SM: [1x2, 2x2, 1x3, 2x3]) and every check work-item
+ * cap ([32, 128, 512] configurations) is timed on that iteration's own
+ * inputs; the fastest of each is kept for the graph and later calls.
+ * csd_batch_tuning reports the choice and the summed time of each variant
+ * (variant_ms: 4 sampler entries, then 3 check entries). */
+csd_status_t csd_batch_autotune(csd_batch_t h, int32_t iterations);
+/* Sets the shapes directly (e.g. a tuning result kept from an earlier run):
+ * sampler variant index as above, check work-item cap a multiple of 8. */
+csd_status_t csd_batch_set_shapes(csd_batch_t h, int32_t sample_variant, int32_t check_item_cap);
+csd_status_t csd_batch_tuning(csd_batch_t h, int32_t* sample_variant, int32_t* check_item_cap, float* variant_ms,
+                              int32_t* num_variants);
+/* Profiling mode, last csd_batch_inflate: per iteration the six stage times
+ * (stage_ms[i * 6 + j]) and the slots active when it started; *count
+ * receives the number of iterations (at most cap are written). */
+csd_status_t csd_batch_iteration_profile(csd_batch_t h, int32_t cap, float* stage_ms, int32_t* active,
+                                         int32_t* count);
 
 csd_status_t csd_batch_destroy(csd_batch_t batch);
 
