@@ -284,6 +284,41 @@ csd_status_t csd_fp32_fma_probe(int64_t iters, double* flops, double* seconds);
  * (FMA = 2 FLOP; sqrt, division and sincos not counted). */
 csd_status_t csd_plant_flops(csd_plant_t plant, double* fk_flops, double* placement_flops, double* pair_flops);
 
+/* ------------------------------------------------------------------------
+ * Collision-likelihood surrogate (no counterpart in the reference): a bank of
+ * BF16 MLPs, in -> 256 -> 256 -> 256 -> 1 with ReLU and FP32 accumulation, one
+ * per plant, run by hand-written tcgen05 kernels. Inputs are scaled by
+ * in_scale (1/pi maps [-pi, pi] joint limits to [-1, 1]) and zero padded to
+ * 16. Parameters per net (csd_mlp_num_params floats): W1 [256][16], b1 [256],
+ * W2 [256][256], b2, W3 [256][256], b3, w4 [256], b4 [1] (row-major
+ * [out][in]). The logit is P(collision) before the sigmoid.
+ * ------------------------------------------------------------------------ */
+typedef struct csd_mlp_s* csd_mlp_t;
+int32_t csd_mlp_num_params(void);
+csd_status_t csd_mlp_create(int32_t nets, const int32_t* dims, float in_scale, uint64_t seed, csd_mlp_t* out);
+csd_status_t csd_mlp_destroy(csd_mlp_t mlp);
+csd_status_t csd_mlp_get_params(csd_mlp_t mlp, float* params /* [nets][num_params] */);
+csd_status_t csd_mlp_set_params(csd_mlp_t mlp, const float* params);
+/* Logits of `groups` row blocks: block i has rows[i] rows of dims[net[i]]
+ * floats in x (blocks concatenated); logits likewise. flags: CSD_PTR_*. */
+csd_status_t csd_mlp_infer(csd_mlp_t mlp, int32_t groups, const int32_t* net, const int32_t* rows, const float* x,
+                           float* logits, int32_t flags, void* stream);
+/* One forward + backward pass (mean binary cross-entropy with logits) on a
+ * host batch of `batch` rows per net (x [nets][batch][dim], y [nets][batch]
+ * 0/1); gradients [nets][num_params] and per-net loss to host. batch is a
+ * multiple of 32. */
+csd_status_t csd_mlp_gradients(csd_mlp_t mlp, const float* x, const uint8_t* y, int32_t batch, float* grads,
+                               float* loss);
+/* Adam training, `steps` minibatches of `batch` rows per net taken in order
+ * from device arrays x [nets][n][dim] and y [nets][n] (n a multiple of batch;
+ * shuffle beforehand); loss_history (host, optional) receives the mean loss of
+ * every step. */
+csd_status_t csd_mlp_train(csd_mlp_t mlp, const float* x, const uint8_t* y, int32_t n, int32_t batch, int32_t steps,
+                           float lr, float* loss_history, void* stream);
+/* Test hook: D [M][N] f32 = A [M][K] * B [N][K]^T for bf16 bit patterns
+ * (N = 16 or 256, K a multiple of 8) through the tensor-core GEMM. */
+csd_status_t csd_mlp_gemm_test(const uint16_t* A, const uint16_t* B, int32_t M, int32_t N, int32_t K, float* D);
+
 #ifdef __cplusplus
 }
 #endif
