@@ -306,7 +306,7 @@ def main():
             faces += [r.A().shape[0] for r in regions]
             iters += [int(x) for x in batch.last_iterations]
             h2d += sum(sc.dim * 8 + d.A().nbytes + d.b().nbytes for sc, d in zip(scs, doms)) + 8 * NUM_SLOTS + 4
-            d2h += sum(r.A().nbytes + r.b().nbytes for r in regions) + 16 * n_graph + 120 * NUM_SLOTS
+            d2h += sum(r.A().nbytes + r.b().nbytes for r in regions) + 16 * n_graph + 144 * NUM_SLOTS
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
     # plain GPU form (one CudaEdgeInflator call per region) on the first timed step's inputs

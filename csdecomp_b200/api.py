@@ -471,6 +471,13 @@ class BatchedEdgeInflator:
         `iterations` iterations of the next inflate and keep the fastest."""
         C.check(C.lib().csd_batch_autotune(self._handle, int(iterations)))
 
+    def set_surrogate(self, surrogate, stop_probability: float = 0.1) -> None:
+        """Surrogate-guided checking with a CollisionSurrogate holding one net
+        per plant of this batch (None turns it off)."""
+        self._surrogate = surrogate  # keep the bank alive while the batch uses it
+        C.check(C.lib().csd_batch_set_surrogate(self._handle, surrogate.handle if surrogate is not None else None,
+                                                ctypes.c_float(stop_probability)))
+
     def set_shapes(self, sample_variant: int, check_item_cap: int) -> None:
         """Fix the sampler variant (index into SAMPLE_VARIANTS) and the check
         work-item cap instead of tuning."""
@@ -522,7 +529,7 @@ class BatchedEdgeInflator:
             aoff += self._capacity * d
         return out
 
-    STAGES = ("sample", "check", "compact", "bisect", "faces", "step")
+    STAGES = ("sample", "score", "sort", "check", "compact", "bisect", "faces", "step")
 
     def set_profiling(self, enable: bool) -> None:
         """Launch stage by stage with events (no graph) and accumulate each
@@ -534,14 +541,14 @@ class BatchedEdgeInflator:
         inflate in profiling mode."""
         cnt = ctypes.c_int32(0)
         C.check(C.lib().csd_batch_iteration_profile(self._handle, 0, None, None, ctypes.byref(cnt)))
-        ms = np.zeros((cnt.value, 6), np.float32)
+        ms = np.zeros((cnt.value, len(self.STAGES)), np.float32)
         act = np.zeros(cnt.value, np.int32)
         C.check(C.lib().csd_batch_iteration_profile(self._handle, cnt.value, C.ptr(ms), C.ptr(act),
                                                     ctypes.byref(cnt)))
         return ms, act
 
     def stage_ms(self) -> dict:
-        ms = np.zeros(6, np.float32)
+        ms = np.zeros(len(self.STAGES), np.float32)
         C.check(C.lib().csd_batch_stage_ms(self._handle, C.ptr(ms)))
         return dict(zip(self.STAGES, ms.tolist()))
 

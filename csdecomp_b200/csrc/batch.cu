@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "eizo_core.cuh"
+#include "mlp_core.cuh"
 #include "sampler_core.cuh"
 
 namespace csd {
@@ -42,9 +43,16 @@ struct SlotState {
   long long flag_off; // bytes: verdicts [n_max]
   long long configs;  // configurations checked: samples + bisection points
   EizoCounters cnt;
+  // surrogate mode: sorted-order checking of this iteration's samples
+  int pos;            // sorted positions checked so far
+  int need;           // more positions must be checked
+  int coll;           // colliding samples found
+  int m_chk;          // checked samples among the first M
+  int m_coll;         // colliding samples among the first M
+  int pad;
 };
 
-static_assert(sizeof(SlotState) == 120, "slot record size is part of the transfer accounting");
+static_assert(sizeof(SlotState) == 144, "slot record size is part of the transfer accounting");
 
 struct BatchIter {    // device-side iteration state
   int k;              // current iteration
@@ -75,7 +83,27 @@ struct BatchArgs {
   uint8_t* bpool;
   BatchIter* it;
   int* act;           // active-slot list of iteration k (slot indices, ascending)
+  // surrogate mode (mlp_wb null: off)
+  const void* mlp_wb;
+  const float* mlp_params;
+  float mlp_scale;
+  float stop_logit;   // keep checking a decided-inadmissible slot while the next score is at least this
+  float* scores;      // [slot][n_max] logits
+  int* order;         // [slot][n_max] sample indices, most likely colliding first
+  int rounds;         // check rounds per iteration
+  int round_base;     // positions of the first round; round r ends at base * (2^(r+1) - 1)
+  int* status;        // tensor-core barrier timeout
 };
+
+// Sorted positions [round_begin, round_end) checked in round r (the last round runs to N).
+static __device__ __forceinline__ int round_end(const BatchArgs& a, int r, int N) {
+  if (r >= a.rounds - 1) return N;
+  const long long e = (long long)a.round_base * ((2ll << r) - 1);
+  return e < N ? (int)e : N;
+}
+static __device__ __forceinline__ int round_begin(const BatchArgs& a, int r, int N) {
+  return r == 0 ? 0 : round_end(a, r - 1, N);
+}
 
 // Work-item size for `total` units over the grid: about four items per
 // block, a multiple of the block's warps, at most `cap`.
@@ -306,6 +334,245 @@ __global__ void __launch_bounds__(1024) batch_step_kernel(BatchArgs a) {
   }
 }
 
+// ---------------------------------------------------------- surrogate mode
+// Logits of the active slots' samples: one CTA per (128-sample tile, active
+// slot), the slot's plant indexing its net (fused tensor-core forward).
+__global__ void __launch_bounds__(mlp::kThreads) batch_score_kernel(BatchArgs a) {
+  extern __shared__ __align__(1024) char smem_raw[];
+  char* smem = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  __shared__ uint64_t bars[2];
+  __shared__ uint32_t tmem_base;
+  if ((int)blockIdx.y >= a.it->num_act) return;
+  const int N = a.n_tab[a.it->k];
+  const int row0 = blockIdx.x * 128;
+  if (row0 >= N) return;
+  const int slot = a.act[blockIdx.y];
+  const SlotState& S = a.slots[slot];
+  mlp::FwdGroup G{};
+  G.x = a.fpool + S.smp_off;
+  G.rows = N;
+  G.dim = S.dim;
+  G.net = S.plant;
+  G.logits = a.scores + (size_t)slot * a.n_max;
+  const mlp::FwdArgs fa{nullptr, reinterpret_cast<const mlp::bf16*>(a.mlp_wb), a.mlp_params, a.mlp_scale, a.status};
+  const int warp = threadIdx.x >> 5;
+  if (warp == 0) {
+    umma::tmem_alloc(&tmem_base, mlp::kH);
+    umma::tmem_relinquish();
+  }
+  if (threadIdx.x == 0) {
+    umma::bar_init(&bars[0], 1);
+    umma::bar_init(&bars[1], 1);
+    umma::bar_fence_init();
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  mlp::forward_tile(fa, G, row0, smem, bars, tmem_base);
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tmem_base, mlp::kH);
+}
+
+constexpr int kSortMax = 16384;  // samples per iteration the sort handles (shared-memory keys)
+
+// Block per active slot: bitonic sort of (descending logit, index) keys in
+// shared memory; writes the order and resets the slot's round counters.
+__global__ void __launch_bounds__(1024) batch_sort_kernel(BatchArgs a) {
+  extern __shared__ unsigned long long keys[];
+  if ((int)blockIdx.x >= a.it->num_act) return;
+  const int slot = a.act[blockIdx.x];
+  const int N = a.n_tab[a.it->k];
+  int P = 1;
+  while (P < N) P <<= 1;
+  const float* sc = a.scores + (size_t)slot * a.n_max;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) {
+    unsigned long long key = ~0ull;
+    if (i < N) {
+      uint32_t u = __float_as_uint(sc[i]);
+      u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);  // order-preserving for finite floats
+      key = ((unsigned long long)(~u) << 32) | (uint32_t)i;
+    }
+    keys[i] = key;
+  }
+  __syncthreads();
+  for (int kk = 2; kk <= P; kk <<= 1)
+    for (int j = kk >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const unsigned long long x = keys[i], y = keys[ixj];
+          if ((x > y) == ((i & kk) == 0)) {
+            keys[i] = y;
+            keys[ixj] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  int* ord = a.order + (size_t)slot * a.n_max;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) ord[i] = (int)(keys[i] & 0xffffffffu);
+  if (threadIdx.x == 0) {
+    SlotState& S = a.slots[slot];
+    S.pos = 0;
+    S.need = 1;
+    S.coll = 0;
+    S.m_chk = 0;
+    S.m_coll = 0;
+  }
+}
+
+// Round r of the sorted check: the positions of round r of every slot that
+// still needs checking, in (slot, chunk) items as batch_check_kernel.
+template <bool SM>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_check_sorted_kernel(BatchArgs a, int static_floats,
+                                                                                   int r) {
+  extern __shared__ float4 smem4[];
+  __shared__ uint64_t bar;
+  __shared__ DevPlant sp;
+  __shared__ int cur;
+  if (threadIdx.x == 0) cur = -1;
+  __syncthreads();
+  const int N = a.n_tab[a.it->k];
+  const int beg = round_begin(a, r, N), end = round_end(a, r, N), cnt = end - beg;
+  if (cnt <= 0) return;
+  const int na = a.it->num_act;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int c = item_size((int64_t)na * cnt, a.cfg_max, nw);
+  const int ips = (cnt + c - 1) / c;
+  const int64_t items = (int64_t)na * ips;
+  const VoxArgs none{nullptr, 0, 0.f, nullptr, nullptr, 0};
+  for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
+    const int slot = a.act[it / ips], first = beg + (int)(it % ips) * c;
+    const SlotState& S = a.slots[slot];
+    if (S.done || !S.need) continue;  // uniform across the block
+    if (!block_plant<SM>(a, S.plant, &sp, &cur, smem4, &bar)) return;
+    const WarpCtx<SM> w = batch_ctx<SM>(sp, smem4, static_floats);
+    const float* smp = a.fpool + S.smp_off;
+    const int* ord = a.order + (size_t)slot * a.n_max;
+    uint8_t* flags = a.bpool + S.flag_off;
+    const int last = min(end, first + c);
+    for (int p = first + warp; p < last; p += nw) {
+      const int i = ord[p];
+      if (lane < sp.dim) w.qs[lane] = smp[(int64_t)i * sp.dim + lane];
+      __syncwarp();
+      fk_warp(sp, w.qs, w.X, lane);
+      const bool hit = check_config(sp, w.stat, w.aabb, w.X, w.pose, lane, none);
+      if (lane == 0) flags[i] = hit ? 0 : 1;
+    }
+  }
+}
+
+// Block per slot after round r: counts what the round found and decides
+// whether the slot needs the next round. Undecided (first-M collisions within
+// the threshold, first-M samples left): continue. Decided inadmissible:
+// continue while fewer than num_particles collisions are known, positions
+// remain and the next position's logit is at least stop_logit. Decided
+// admissible (all first-M samples checked): stop.
+__global__ void __launch_bounds__(256) batch_tally_kernel(BatchArgs a, int r) {
+  __shared__ int red[3][8];
+  SlotState& S = a.slots[blockIdx.x];
+  if (S.done || !S.need) return;
+  const int k = a.it->k, N = a.n_tab[k], M = a.m_tab[k];
+  const int beg = round_begin(a, r, N), end = round_end(a, r, N);
+  const int* ord = a.order + (size_t)blockIdx.x * a.n_max;
+  const uint8_t* flags = a.bpool + S.flag_off;
+  int coll = 0, mchk = 0, mcoll = 0;
+  for (int p = beg + threadIdx.x; p < end; p += blockDim.x) {
+    const int i = ord[p];
+    const int c = flags[i] == 0;
+    coll += c;
+    mchk += i < M;
+    mcoll += c && i < M;
+  }
+  for (int o = 16; o; o >>= 1) {
+    coll += __shfl_xor_sync(0xffffffffu, coll, o);
+    mchk += __shfl_xor_sync(0xffffffffu, mchk, o);
+    mcoll += __shfl_xor_sync(0xffffffffu, mcoll, o);
+  }
+  const int warp = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    red[0][warp] = coll;
+    red[1][warp] = mchk;
+    red[2][warp] = mcoll;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+      coll += red[0][w];
+      mchk += red[1][w];
+      mcoll += red[2][w];
+    }
+    S.coll += coll;
+    S.m_chk += mchk;
+    S.m_coll += mcoll;
+    S.pos = end;
+    int need;
+    if ((float)S.m_coll > a.thr_tab[k])
+      need = S.coll < a.num_particles && end < N &&
+             a.scores[(size_t)blockIdx.x * a.n_max + ord[end]] >= a.stop_logit;
+    else
+      need = S.m_chk < M;
+    S.need = need;
+  }
+}
+
+// Block per slot: ordered compaction of the colliding samples over the
+// checked sorted positions, the admissibility decision and the particle count.
+__global__ void __launch_bounds__(1024) batch_compact_sorted_kernel(BatchArgs a) {
+  __shared__ int warp_n[32];
+  __shared__ int base;
+  SlotState& S = a.slots[blockIdx.x];
+  if (S.done) return;
+  if (S.status == 2) {
+    if (threadIdx.x == 0) S.done = 1;
+    return;
+  }
+  const int k = a.it->k;
+  const int npos = S.pos, dim = S.dim;
+  const int* ord = a.order + (size_t)blockIdx.x * a.n_max;
+  const uint8_t* flags = a.bpool + S.flag_off;
+  const float* smp = a.fpool + S.smp_off;
+  float* cols = a.fpool + S.col_off;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  if (tid == 0) base = 0;
+  __syncthreads();
+  for (int p0 = 0; p0 < npos; p0 += blockDim.x) {
+    const int p = p0 + tid;
+    int i = 0;
+    bool c = false;
+    if (p < npos) {
+      i = ord[p];
+      c = flags[i] == 0;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, c);
+    if (lane == 0) warp_n[warp] = __popc(m);
+    __syncthreads();
+    int off = base;
+    for (int w = 0; w < warp; ++w) off += warp_n[w];
+    const int rank = off + __popc(m & ((1u << lane) - 1u));
+    if (c && rank < a.num_particles)
+      for (int d = 0; d < dim; ++d) cols[(size_t)rank * dim + d] = smp[(size_t)i * dim + d];
+    __syncthreads();
+    if (tid == 0)
+      for (int w = 0; w < nw; ++w) base += warp_n[w];
+    __syncthreads();
+  }
+  if (tid == 0) {
+    S.configs += npos;
+    S.cnt.total = (uint32_t)base;
+    S.cnt.first_m = (uint32_t)S.m_coll;
+    if ((float)S.m_coll <= a.thr_tab[k]) {
+      S.done = 1;
+      S.iters = k + 1;
+      S.K = 0;
+    } else {
+      S.K = min(base, a.num_particles);
+      S.configs += (long long)S.K * a.bisection;
+    }
+  }
+}
+
 // Sampler variants the autotuner chooses from: U faces per lane and trip,
 // MINB resident blocks per SM (register cap).
 using SampleFn = void (*)(BatchArgs);
@@ -323,6 +590,8 @@ constexpr int kNumSampleVariants = (int)(sizeof(kSampleVariants) / sizeof(kSampl
 // Largest check work item (configurations) the autotuner chooses from.
 constexpr int kCheckItemCaps[] = {32, 128, 512};
 constexpr int kNumCheckVariants = (int)(sizeof(kCheckItemCaps) / sizeof(kCheckItemCaps[0]));
+// profiled stages: sample, score, sort, check, compact, bisect, faces, step
+constexpr int kStages = 8;
 
 }  // namespace csd
 
@@ -345,16 +614,22 @@ struct csd_batch_s {
   std::vector<int> n_tab, m_tab;
   std::vector<float> thr_tab;
   csd::DevBuf plants_dev, slots_dev, tabs, fpool, bpool, iter, act;
+  // surrogate mode
+  csd_mlp_t mlp = nullptr;
+  float stop_logit = 0.f;
+  int rounds = 5, round_base = 512;
+  csd::DevBuf scores, order, status;
   std::vector<csd::SlotState> host_slots;
   std::vector<int> act_host;
   cudaGraphExec_t graph = nullptr;
   int graph_slots = -1, graph_cfg = -1, graph_variant = -1;
+  const void* graph_mlp = nullptr;
   cudaStream_t graph_stream = nullptr;
   csd::BatchIter* host_iter = nullptr;
   bool profile = false;         // launch stage by stage with events instead of the graph
-  cudaEvent_t ev[7] = {};
-  double stage_ms[6] = {};
-  std::vector<float> iter_ms;   // profiling mode: [iteration][6] of the last inflate
+  cudaEvent_t ev[csd::kStages + 1] = {};
+  double stage_ms[csd::kStages] = {};
+  std::vector<float> iter_ms;   // profiling mode: [iteration][kStages] of the last inflate
   std::vector<int> iter_active; // slots active at the start of each iteration
   ~csd_batch_s() {
     for (cudaEvent_t e : ev)
@@ -369,32 +644,55 @@ using namespace csd;
 
 namespace {
 
-// One iteration's six launches on stream s; with ev (7 events) recorded
-// between the stages for the profiling mode.
-void launch_iteration(csd_batch_s* h, int num_slots, const BatchArgs& a, cudaStream_t s, cudaEvent_t* ev) {
+// One iteration's launches on stream s. ev (kStages + 1 events) brackets the
+// stages for the profiling mode; skip_sample leaves out the sampler (the
+// autotuner has just run it).
+void launch_iteration(csd_batch_s* h, int num_slots, const BatchArgs& a, cudaStream_t s, cudaEvent_t* ev,
+                      bool skip_sample = false) {
   if (ev) cudaEventRecord(ev[0], s);
-  kSampleVariants[h->sample_variant].fn<<<h->sample_grid[h->sample_variant], 256, kStageBytes, s>>>(a);
+  if (!skip_sample)
+    kSampleVariants[h->sample_variant].fn<<<h->sample_grid[h->sample_variant], 256, kStageBytes, s>>>(a);
   if (ev) cudaEventRecord(ev[1], s);
-  if (h->sm)
-    batch_check_kernel<true><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->static_floats);
-  else
-    batch_check_kernel<false><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, 0);
-  if (ev) cudaEventRecord(ev[2], s);
-  batch_compact_kernel<<<num_slots, 1024, 0, s>>>(a);
-  if (ev) cudaEventRecord(ev[3], s);
+  if (a.mlp_wb) {
+    batch_score_kernel<<<dim3((h->n_max + 127) / 128, num_slots), mlp::kThreads, mlp::kFwdSmem, s>>>(a);
+    if (ev) cudaEventRecord(ev[2], s);
+    batch_sort_kernel<<<num_slots, 1024, kSortMax * sizeof(unsigned long long), s>>>(a);
+    if (ev) cudaEventRecord(ev[3], s);
+    for (int r = 0; r < a.rounds; ++r) {
+      if (h->sm)
+        batch_check_sorted_kernel<true><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->static_floats,
+                                                                                                  r);
+      else
+        batch_check_sorted_kernel<false><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, 0, r);
+      batch_tally_kernel<<<num_slots, 256, 0, s>>>(a, r);
+    }
+    if (ev) cudaEventRecord(ev[4], s);
+    batch_compact_sorted_kernel<<<num_slots, 1024, 0, s>>>(a);
+  } else {
+    if (ev) cudaEventRecord(ev[2], s);
+    if (ev) cudaEventRecord(ev[3], s);
+    if (h->sm)
+      batch_check_kernel<true><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->static_floats);
+    else
+      batch_check_kernel<false><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, 0);
+    if (ev) cudaEventRecord(ev[4], s);
+    batch_compact_kernel<<<num_slots, 1024, 0, s>>>(a);
+  }
+  if (ev) cudaEventRecord(ev[5], s);
   if (h->sm)
     batch_bisect_kernel<true><<<h->bisect_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->static_floats);
   else
     batch_bisect_kernel<false><<<h->bisect_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, 0);
-  if (ev) cudaEventRecord(ev[4], s);
-  batch_faces_kernel<<<num_slots, 1024, 0, s>>>(a);
-  if (ev) cudaEventRecord(ev[5], s);
-  batch_step_kernel<<<1, 1024, 0, s>>>(a);
   if (ev) cudaEventRecord(ev[6], s);
+  batch_faces_kernel<<<num_slots, 1024, 0, s>>>(a);
+  if (ev) cudaEventRecord(ev[7], s);
+  batch_step_kernel<<<1, 1024, 0, s>>>(a);
+  if (ev) cudaEventRecord(ev[8], s);
 }
 
 csd_status_t build_graph(csd_batch_s* h, int num_slots, const BatchArgs& a) {
-  if (h->graph && h->graph_slots == num_slots && h->graph_cfg == a.cfg_max && h->graph_variant == h->sample_variant)
+  if (h->graph && h->graph_slots == num_slots && h->graph_cfg == a.cfg_max && h->graph_variant == h->sample_variant &&
+      h->graph_mlp == a.mlp_wb)
     return CSD_OK;
   if (h->graph) {
     cudaGraphExecDestroy(h->graph);
@@ -418,6 +716,7 @@ csd_status_t build_graph(csd_batch_s* h, int num_slots, const BatchArgs& a) {
   h->graph_slots = num_slots;
   h->graph_cfg = a.cfg_max;
   h->graph_variant = h->sample_variant;
+  h->graph_mlp = a.mlp_wb;
   return CSD_OK;
 }
 
@@ -495,7 +794,7 @@ csd_status_t csd_batch_create(const csd_plant_t* plants, int32_t num_plants, int
   if ((s = h->plants_dev.reserve(dps.size() * sizeof(DevPlant))) || (s = h->slots_dev.reserve(max_slots * sizeof(SlotState))) ||
       (s = h->tabs.reserve(h->n_tab.size() * 12 + 64)) || (s = h->fpool.reserve(per_slot_f * max_slots * 4 + 256)) ||
       (s = h->bpool.reserve((size_t)h->n_max * max_slots + 256)) || (s = h->iter.reserve(sizeof(BatchIter))) ||
-      (s = h->act.reserve((size_t)max_slots * 4)))
+      (s = h->act.reserve((size_t)max_slots * 4)) || (s = h->status.reserve(16)))
     return s;
   CSD_CUDA_TRY(cudaMemcpy(h->plants_dev.ptr, dps.data(), dps.size() * sizeof(DevPlant), cudaMemcpyHostToDevice));
   int* t = h->tabs.as<int>();
@@ -634,6 +933,19 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
   a.act = h->act.as<int>();
   a.cfg_max = h->cfg_max;
   a.part_max = h->part_max;
+  if (h->mlp) {
+    const MlpView mv = mlp_view(h->mlp);
+    a.mlp_wb = mv.wb;
+    a.mlp_params = mv.params;
+    a.mlp_scale = mv.in_scale;
+    a.stop_logit = h->stop_logit;
+    a.scores = h->scores.as<float>();
+    a.order = h->order.as<int>();
+    a.rounds = h->rounds;
+    a.round_base = h->round_base;
+  }
+  a.status = h->status.as<int>();
+  CSD_CUDA_TRY(cudaMemsetAsync(h->status.ptr, 0, 16, st));
   batch_transpose_kernel<<<n, 256, 0, st>>>(a);
   CSD_CUDA_TRY(cudaGetLastError());
   csd_status_t s = build_graph(h, n, a);
@@ -662,7 +974,7 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
         kSampleVariants[v].fn<<<h->sample_grid[v], 256, kStageBytes, st>>>(a);
         cudaEventRecord(tev[2 * j + 1], st);
       }
-      for (int c = 0; c < kNumCheckVariants; ++c, ++j) {
+      for (int c = 0; c < kNumCheckVariants && !a.mlp_wb; ++c, ++j) {
         BatchArgs ac = a;
         ac.cfg_max = kCheckItemCaps[c];
         cudaEventRecord(tev[2 * j], st);
@@ -672,13 +984,7 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
           batch_check_kernel<false><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, st>>>(ac, 0);
         cudaEventRecord(tev[2 * j + 1], st);
       }
-      batch_compact_kernel<<<n, 1024, 0, st>>>(a);
-      if (h->sm)
-        batch_bisect_kernel<true><<<h->bisect_grid, 32 * kWarpsPerBlock, h->check_smem, st>>>(a, h->static_floats);
-      else
-        batch_bisect_kernel<false><<<h->bisect_grid, 32 * kWarpsPerBlock, h->check_smem, st>>>(a, 0);
-      batch_faces_kernel<<<n, 1024, 0, st>>>(a);
-      batch_step_kernel<<<1, 1024, 0, st>>>(a);
+      launch_iteration(h, n, a, st, nullptr, true);
       CSD_CUDA_TRY(cudaGetLastError());
       CSD_CUDA_TRY(cudaStreamSynchronize(st));
       for (int q = 0; q < j; ++q) {
@@ -695,7 +1001,7 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
         for (int c = 1; c < kNumCheckVariants; ++c)
           if (h->tune_ms[kNumSampleVariants + c] < h->tune_ms[kNumSampleVariants + bc]) bc = c;
         h->sample_variant = bs;
-        h->cfg_max = kCheckItemCaps[bc];
+        if (!a.mlp_wb) h->cfg_max = kCheckItemCaps[bc];
         a.cfg_max = h->cfg_max;
         h->graph_slots = -1;  // recapture with the chosen shapes
         if ((s = build_graph(h, n, a))) return s;
@@ -703,8 +1009,8 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
     } else if (h->profile) {
       launch_iteration(h, n, a, st, h->ev);
       CSD_CUDA_TRY(cudaGetLastError());
-      CSD_CUDA_TRY(cudaEventSynchronize(h->ev[6]));
-      for (int j = 0; j < 6; ++j) {
+      CSD_CUDA_TRY(cudaEventSynchronize(h->ev[kStages]));
+      for (int j = 0; j < kStages; ++j) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, h->ev[j], h->ev[j + 1]);
         h->stage_ms[j] += ms;
@@ -727,7 +1033,13 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
     cudaEventDestroy(ev1);
   }
   CSD_CUDA_TRY(cudaMemcpyAsync(slots.data(), h->slots_dev.ptr, n * sizeof(SlotState), cudaMemcpyDeviceToHost, st));
+  int kstat = 0;
+  CSD_CUDA_TRY(cudaMemcpyAsync(&kstat, h->status.ptr, 4, cudaMemcpyDeviceToHost, st));
   CSD_CUDA_TRY(cudaStreamSynchronize(st));
+  if (kstat) {
+    set_error("a tensor-core barrier wait timed out in the scoring stage");
+    return CSD_ERR_CUDA;
+  }
   h->host_slots.assign(slots.begin(), slots.end());
   size_t aoff = 0;
   for (int i = 0; i < n; ++i) {
@@ -760,7 +1072,7 @@ csd_status_t csd_batch_set_profiling(csd_batch_t h, int32_t enable) {
 
 csd_status_t csd_batch_stage_ms(csd_batch_t h, float* ms) {
   CSD_CHECK(h && ms, CSD_ERR_INVALID, "null argument");
-  for (int j = 0; j < 6; ++j) ms[j] = (float)h->stage_ms[j];
+  for (int j = 0; j < kStages; ++j) ms[j] = (float)h->stage_ms[j];
   return CSD_OK;
 }
 
@@ -769,6 +1081,42 @@ csd_status_t csd_batch_autotune(csd_batch_t h, int32_t iterations) {
   h->tune_iters = iterations;
   h->tuned_iters = 0;
   for (double& x : h->tune_ms) x = 0.0;
+  return CSD_OK;
+}
+
+csd_status_t csd_batch_set_surrogate(csd_batch_t h, csd_mlp_t mlp, float stop_probability) {
+  CSD_CHECK(h, CSD_ERR_INVALID, "null batch");
+  if (!mlp) {
+    h->mlp = nullptr;
+    return CSD_OK;
+  }
+  CSD_CHECK(stop_probability > 0.f && stop_probability < 1.f, CSD_ERR_INVALID, "stop probability must be in (0, 1)");
+  const MlpView mv = mlp_view(mlp);
+  CSD_CHECK(mv.device == h->device, CSD_ERR_INVALID, "surrogate and batch must live on one device");
+  CSD_CHECK(mv.nets == (int)h->plants.size(), CSD_ERR_INVALID, "the surrogate needs one net per plant of the batch");
+  for (int i = 0; i < mv.nets; ++i)
+    CSD_CHECK(mv.dims[i] == h->plants[i]->dp.dim, CSD_ERR_DIMENSION, "net " + std::to_string(i) +
+                                                                         " does not match its plant's dimension");
+  CSD_CHECK(h->n_max <= kSortMax, CSD_ERR_CAPACITY, "more samples per iteration than the surrogate sort handles");
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != h->device) cudaSetDevice(h->device);
+  struct Restore {
+    int cur, dev;
+    ~Restore() {
+      if (cur != dev) cudaSetDevice(cur);
+    }
+  } restore{cur, h->device};
+  csd_status_t s;
+  if ((s = h->scores.reserve((size_t)h->max_slots * h->n_max * 4)) ||
+      (s = h->order.reserve((size_t)h->max_slots * h->n_max * 4)))
+    return s;
+  CSD_CUDA_TRY(cudaFuncSetAttribute(batch_score_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)mlp::kFwdSmem));
+  CSD_CUDA_TRY(cudaFuncSetAttribute(batch_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(kSortMax * sizeof(unsigned long long))));
+  h->mlp = mlp;
+  h->stop_logit = std::log(stop_probability / (1.f - stop_probability));
   return CSD_OK;
 }
 
@@ -799,7 +1147,7 @@ csd_status_t csd_batch_iteration_profile(csd_batch_t h, int32_t cap, float* stag
   *count = n;
   for (int i = 0; i < std::min(n, (int)cap); ++i) {
     active[i] = h->iter_active[i];
-    for (int j = 0; j < 6; ++j) stage_ms[i * 6 + j] = h->iter_ms[(size_t)i * 6 + j];
+    for (int j = 0; j < kStages; ++j) stage_ms[i * kStages + j] = h->iter_ms[(size_t)i * kStages + j];
   }
   return CSD_OK;
 }

@@ -122,4 +122,16 @@ csd_status_t launch_transpose_faces(const float* A, int F, int d, float* At, int
 
 int device_sm_count();
 
+// The surrogate bank's device tensors (mlp.cu): bf16 weights, f32 parameters,
+// input scale, and the input dimension of each net.
+struct MlpView {
+  const void* wb;
+  const float* params;
+  float in_scale;
+  int nets;
+  const int* dims;  // host array
+  int device;
+};
+MlpView mlp_view(csd_mlp_t h);
+
 }  // namespace csd

@@ -122,3 +122,24 @@ def gemm_test(a_bits: np.ndarray, b_bits: np.ndarray) -> np.ndarray:
     d = np.zeros((M, N), np.float32)
     C.check(C.lib().csd_mlp_gemm_test(C.ptr(a), C.ptr(b), M, N, K, C.ptr(d)))
     return d
+
+
+def training_set(scene, seed_edges, n: int, seed: int, sigma: float = 0.35, local_fraction: float = 0.5):
+    """n configurations of `scene` labelled by the exact checker (1 =
+    colliding): (1 - local_fraction) uniform in the joint limits, the rest
+    around the seed edges (a uniform point of a random edge plus N(0, sigma^2)
+    per joint, clipped to the limits). Returns (x [n, dim] f32, y [n] u8)."""
+    from .api import CheckCollisionFreeCuda
+    rng = np.random.default_rng(seed)
+    lo, hi = scene.lower(), scene.upper()
+    n_loc = int(round(n * local_fraction)) if seed_edges else 0
+    x = np.empty((n, scene.dim), np.float32)
+    x[:n - n_loc] = lo + (hi - lo) * rng.random((n - n_loc, scene.dim))
+    if n_loc:
+        e = rng.integers(0, len(seed_edges), n_loc)
+        t = rng.random(n_loc)[:, None]
+        a = np.stack([seed_edges[i][0] for i in e])
+        b = np.stack([seed_edges[i][1] for i in e])
+        x[n - n_loc:] = np.clip(a + t * (b - a) + rng.normal(0, sigma, (n_loc, scene.dim)), lo, hi)
+    y = (CheckCollisionFreeCuda(x.T, scene.plant) == 0).astype(np.uint8)
+    return x, y

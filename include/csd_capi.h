@@ -205,6 +205,7 @@ csd_status_t csd_eizo(csd_plant_t plant, const float* line_start, const float* l
  * per stage, replayed as a CUDA graph. Each slot computes exactly what
  * csd_inflator_inflate computes for the same inputs. No voxels. */
 typedef struct csd_batch_s* csd_batch_t;
+typedef struct csd_mlp_s* csd_mlp_t;  /* the surrogate bank, declared with csd_mlp_* below */
 csd_status_t csd_batch_create(const csd_plant_t* plants, int32_t num_plants, int32_t max_slots,
                               const csd_eizo_options_t* options, int32_t face_capacity, csd_batch_t* out);
 /* n slots: slot i uses plants[slot_plant[i]] (dim d_i); starts/ends hold the
@@ -225,10 +226,11 @@ csd_status_t csd_batch_configs_checked(csd_batch_t h, int32_t n, int64_t* config
 
 /* Profiling mode: while enabled, csd_batch_inflate launches each iteration's
  * stages one by one (no graph) with events between them and accumulates the
- * GPU time of each stage: [sample, check, compact, bisect, faces, step].
- * Enabling (or disabling) resets the accumulators. */
+ * GPU time of each stage: [sample, score, sort, check, compact, bisect,
+ * faces, step] (score and sort are zero without a surrogate). Enabling (or
+ * disabling) resets the accumulators. */
 csd_status_t csd_batch_set_profiling(csd_batch_t h, int32_t enable);
-csd_status_t csd_batch_stage_ms(csd_batch_t h, float* stage_ms /* [6] */);
+csd_status_t csd_batch_stage_ms(csd_batch_t h, float* stage_ms /* [8] */);
 /* Autotuner: during the first `iterations` iterations of the next
  * csd_batch_inflate, every sampler variant (faces per lane and trip x
  * resident blocks per SM: [1x2, 2x2, 1x3, 2x3]) and every check work-item
@@ -237,13 +239,23 @@ csd_status_t csd_batch_stage_ms(csd_batch_t h, float* stage_ms /* [6] */);
  * csd_batch_tuning reports the choice and the summed time of each variant
  * (variant_ms: 4 sampler entries, then 3 check entries). */
 csd_status_t csd_batch_autotune(csd_batch_t h, int32_t iterations);
+/* Surrogate-guided checking (mlp: one net per plant of the batch, same
+ * dimensions; NULL turns it off). Each iteration then scores every sample
+ * with the net, checks the samples in decreasing predicted collision
+ * probability in up to 5 rounds, and stops checking a slot once its
+ * admissibility is decided and, if inadmissible, num_particles collisions are
+ * known or the next sample's predicted probability is below
+ * stop_probability. Every verdict used is the exact checker's; the
+ * admissibility test (first M samples) is unchanged; the bisected particles
+ * are the collisions found, in that order. */
+csd_status_t csd_batch_set_surrogate(csd_batch_t h, csd_mlp_t mlp, float stop_probability);
 /* Sets the shapes directly (e.g. a tuning result kept from an earlier run):
  * sampler variant index as above, check work-item cap a multiple of 8. */
 csd_status_t csd_batch_set_shapes(csd_batch_t h, int32_t sample_variant, int32_t check_item_cap);
 csd_status_t csd_batch_tuning(csd_batch_t h, int32_t* sample_variant, int32_t* check_item_cap, float* variant_ms,
                               int32_t* num_variants);
-/* Profiling mode, last csd_batch_inflate: per iteration the six stage times
- * (stage_ms[i * 6 + j]) and the slots active when it started; *count
+/* Profiling mode, last csd_batch_inflate: per iteration the eight stage times
+ * (stage_ms[i * 8 + j]) and the slots active when it started; *count
  * receives the number of iterations (at most cap are written). */
 csd_status_t csd_batch_iteration_profile(csd_batch_t h, int32_t cap, float* stage_ms, int32_t* active,
                                          int32_t* count);
@@ -293,7 +305,6 @@ csd_status_t csd_plant_flops(csd_plant_t plant, double* fk_flops, double* placem
  * W2 [256][256], b2, W3 [256][256], b3, w4 [256], b4 [1] (row-major
  * [out][in]). The logit is P(collision) before the sigmoid.
  * ------------------------------------------------------------------------ */
-typedef struct csd_mlp_s* csd_mlp_t;
 int32_t csd_mlp_num_params(void);
 csd_status_t csd_mlp_create(int32_t nets, const int32_t* dims, float in_scale, uint64_t seed, csd_mlp_t* out);
 csd_status_t csd_mlp_destroy(csd_mlp_t mlp);
