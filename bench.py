@@ -36,6 +36,11 @@ WORKLOAD = ("batched EI-ZO: 256 inflations per step, one per seeded scene (even:
             "U[0.05,1.0] rad in free space; domain = joint-limit box; 2000 particles, mixing 50, 9 bisection steps, "
             "<=10 faces/iteration, eps=0.01, delta=0.05, tau=0.5")
 SEED_EDGE_SEED = 3000
+SURROGATE_ROWS = 16384        # labelled configurations per scene (4.2 M over the 256 scenes)
+SURROGATE_EPOCHS = 6
+SURROGATE_SEED = 5000
+SURROGATE_STOP = 0.01         # predicted collision probability below which a decided slot stops checking
+SURROGATE_ROUNDS = 3
 RANK_SCENE_STRIDE = 7919
 
 
@@ -271,44 +276,74 @@ def main():
         d.MakeBox(sc.lower(), sc.upper())
         doms.append(d)
     opt = csd.EizoOptions(**EIZO_KW)
-    batch = csd.BatchedEdgeInflator([sc.plant for sc in scs], opt, max_slots=NUM_SLOTS, face_capacity=FACE_CAPACITY)
     slot_plant = list(range(NUM_SLOTS))
 
     def step_inputs(s):
         return [e[s][0] for _, e in items], [e[s][1] for _, e in items]
 
-    for s in range(args.warmup):
-        q0s, q1s = step_inputs(s)
-        batch.inflate(slot_plant, q0s, q1s, doms)
+    # surrogate: one net per scene, trained on configurations labelled by the exact checker
+    from csdecomp_b200.surrogate import CollisionSurrogate, training_set
     torch.cuda.synchronize()
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    if dist:
-        dist.barrier()
+    t0 = time.perf_counter()
+    xs, ys = [], []
+    for i, (sc, e) in enumerate(items):
+        x, y = training_set(sc, e, SURROGATE_ROWS, seed=SURROGATE_SEED + i)
+        xs.append(x)
+        ys.append(y)
+    t_label = time.perf_counter() - t0
+    bank = CollisionSurrogate([sc.dim for sc in scs], seed=SURROGATE_SEED)
+    t0 = time.perf_counter()
+    hist = bank.train(xs, ys, batch=512, epochs=SURROGATE_EPOCHS, lr=2e-3)
     torch.cuda.synchronize()
-    dev_s, wall_s, configs, launches = 0.0, 0.0, 0, 0
-    faces, iters, h2d, d2h = [], [], 0, 0
-    first_regions = None
-    torch.cuda.nvtx.range_push("timed")
-    with ClockSampler(local) as clk:
+    t_train = time.perf_counter() - t0
+    pos = float(np.mean([y.mean() for y in ys]))
+
+    def timed_run(batch):
+        """W warm-up steps (the first autotunes), then the K timed steps."""
+        for s in range(args.warmup):
+            q0s, q1s = step_inputs(s)
+            batch.inflate(slot_plant, q0s, q1s, doms)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        r = dict(dev_s=0.0, wall_s=0.0, configs=0, launches=0, faces=[], iters=[], h2d=0, d2h=0, first=None)
         for s in range(args.warmup, steps_total):
             q0s, q1s = step_inputs(s)
             flush.fill_(1)  # L2 flush between steps (outside the timed window)
             torch.cuda.synchronize()
             w0 = time.perf_counter()
             regions = batch.inflate(slot_plant, q0s, q1s, doms)
-            wall_s += time.perf_counter() - w0
-            dev_s += batch.last_device_ms * 1e-3
-            if first_regions is None:
-                first_regions = regions
-            configs += int(batch.last_configs_checked.sum())
+            r["wall_s"] += time.perf_counter() - w0
+            r["dev_s"] += batch.last_device_ms * 1e-3
+            if r["first"] is None:
+                r["first"] = regions
+            r["configs"] += int(batch.last_configs_checked.sum())
             n_graph = int(batch.last_iterations.max())
-            launches += 6 * n_graph
-            faces += [r.A().shape[0] for r in regions]
-            iters += [int(x) for x in batch.last_iterations]
-            h2d += sum(sc.dim * 8 + d.A().nbytes + d.b().nbytes for sc, d in zip(scs, doms)) + 8 * NUM_SLOTS + 4
-            d2h += sum(r.A().nbytes + r.b().nbytes for r in regions) + 16 * n_graph + 144 * NUM_SLOTS
-    torch.cuda.synchronize()
+            r["launches"] += n_graph * (6 if batch_surrogate(batch) is None else 7 + 2 * SURROGATE_ROUNDS)
+            r["faces"] += [p.A().shape[0] for p in regions]
+            r["iters"] += [int(x) for x in batch.last_iterations]
+            r["h2d"] += sum(sc.dim * 8 + d.A().nbytes + d.b().nbytes for sc, d in zip(scs, doms)) + 8 * NUM_SLOTS + 4
+            r["d2h"] += sum(p.A().nbytes + p.b().nbytes for p in regions) + 16 * n_graph + 144 * NUM_SLOTS
+        torch.cuda.synchronize()
+        return r
+
+    def batch_surrogate(batch):
+        return getattr(batch, "_surrogate", None)
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    batched = csd.BatchedEdgeInflator([sc.plant for sc in scs], opt, max_slots=NUM_SLOTS, face_capacity=FACE_CAPACITY)
+    rb = timed_run(batched)
+    tuned_plain = batched.tuning()
+    surrogate_batch = csd.BatchedEdgeInflator([sc.plant for sc in scs], opt, max_slots=NUM_SLOTS,
+                                              face_capacity=FACE_CAPACITY)
+    surrogate_batch.set_surrogate(bank, SURROGATE_STOP)
+    torch.cuda.nvtx.range_push("timed")
+    with ClockSampler(local) as clk:
+        rs = timed_run(surrogate_batch)
     torch.cuda.nvtx.range_pop()
+    tuned_surr = surrogate_batch.tuning()
+    first_regions = rb["first"]
     # plain GPU form (one CudaEdgeInflator call per region) on the first timed step's inputs
     plain_s, identical = 0.0, True
     st = torch.cuda.current_stream()
@@ -326,34 +361,55 @@ def main():
         identical &= bool(np.array_equal(P.A(), first_regions[i].A()) and np.array_equal(P.b(), first_regions[i].b()))
         del inf
     if dist:
-        dev_s, wall_s, configs_all = reduce_timing(dist, dev, dev_s, wall_s, float(configs))
+        dev_s, wall_s, configs_all = reduce_timing(dist, dev, rs["dev_s"], rs["wall_s"], float(rs["configs"]))
+        b_dev, _, b_cfg = reduce_timing(dist, dev, rb["dev_s"], rb["wall_s"], float(rb["configs"]))
         plain_s, _, _ = reduce_timing(dist, dev, plain_s, 0.0, 0.0)
         dist.barrier()
     else:
-        configs_all = float(configs)
+        dev_s, wall_s, configs_all = rs["dev_s"], rs["wall_s"], float(rs["configs"])
+        b_dev, b_cfg = rb["dev_s"], float(rb["configs"])
     regions_all = NUM_SLOTS * args.steps * world
     if rank == 0:
         value = regions_all / dev_s
+        batched_value = regions_all / b_dev
         plain = NUM_SLOTS * world / plain_s
         line = {"metric": METRIC, "value": value, "unit": "regions/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 * dev_s / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-                "config": {"workload": WORKLOAD, "form": "batched (BatchedEdgeInflator, 256 slots, CUDA graph)",
-                           "surrogate": "not used", "parallelism": f"{world} independent ranks",
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32 (checks), bf16 (surrogate MLP)",
+                "data": "synthetic (seeded)",
+                "config": {"workload": WORKLOAD,
+                           "form": "surrogate + batched (BatchedEdgeInflator with a trained CollisionSurrogate, "
+                                   "256 slots, CUDA graph)",
+                           "parallelism": f"{world} independent ranks",
                            "l2": "flushed between steps (256 MB write)", "scenes_skipped": skipped,
-                           "face_capacity": FACE_CAPACITY},
+                           "face_capacity": FACE_CAPACITY,
+                           "surrogate": {"nets": len(scs), "architecture": "in->256->256->256->1 BF16, FP32 accumulate",
+                                         "training_rows": SURROGATE_ROWS * len(scs), "colliding_fraction": pos,
+                                         "epochs": SURROGATE_EPOCHS, "label_s": t_label, "train_s": t_train,
+                                         "final_loss": float(hist[-20:].mean()), "first_loss": float(hist[:20].mean()),
+                                         "stop_probability": SURROGATE_STOP,
+                                         "note": "trained once before the timed steps; every verdict is the exact "
+                                                 "checker's, admissibility uses the unchanged first-M test"},
+                           "autotuned": {"batched": tuned_plain["sample_variant"] + f", check cap {tuned_plain['check_item_cap']}",
+                                         "surrogate": tuned_surr["sample_variant"]}},
                 "configs_per_s": configs_all / dev_s,
+                "configs_checked_per_step": configs_all / args.steps / world,
+                "batched_gpu": {"value": batched_value, "unit": "regions/s", "configs_per_s": b_cfg / b_dev,
+                                "configs_checked_per_step": b_cfg / args.steps / world,
+                                "note": "same steps without the surrogate; regions identical to the plain form"},
                 "plain_gpu": {"value": plain, "unit": "regions/s",
                               "sample": "the first timed step's 256 inflations, one CudaEdgeInflator.inflateEdge "
-                                        "call each", "identical_regions": identical,
-                              "batched_over_plain": value / plain},
-                "faces": {"mean": float(np.mean(faces)), "max": int(np.max(faces)), "min": int(np.min(faces))},
-                "iterations": {"mean": float(np.mean(iters)), "max": int(np.max(iters))},
+                                        "call each", "identical_to_batched": identical},
+                "surrogate_batched_over_plain": value / plain,
+                "batched_over_plain": batched_value / plain,
+                "faces": {"mean": float(np.mean(rs["faces"])), "max": int(np.max(rs["faces"])),
+                          "min": int(np.min(rs["faces"]))},
+                "iterations": {"mean": float(np.mean(rs["iters"])), "max": int(np.max(rs["iters"]))},
                 "e2e": {"value": regions_all / wall_s, "unit": "regions/s",
-                        "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
-                        "path": "BatchedEdgeInflator.inflate with host numpy segments and polytopes in, host "
-                                "polytopes out"},
-                "gpu_launches": launches,
+                        "h2d_bytes_per_step": rs["h2d"] // args.steps, "d2h_bytes_per_step": rs["d2h"] // args.steps,
+                        "path": "BatchedEdgeInflator.inflate (surrogate set) with host numpy segments and polytopes "
+                                "in, host polytopes out"},
+                "gpu_launches": rs["launches"],
                 "clocks": clk.summary()}
         line["roofline"] = roofline_point_check(csd, scenes.edge_check_scene(keepout=0.8), torch, dev)
         if world == 1:

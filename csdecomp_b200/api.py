@@ -478,6 +478,10 @@ class BatchedEdgeInflator:
         C.check(C.lib().csd_batch_set_surrogate(self._handle, surrogate.handle if surrogate is not None else None,
                                                 ctypes.c_float(stop_probability)))
 
+    def set_surrogate_rounds(self, rounds: int, first_round: int) -> None:
+        """Round schedule of the surrogate-guided check (see csd_capi.h)."""
+        C.check(C.lib().csd_batch_set_surrogate_rounds(self._handle, int(rounds), int(first_round)))
+
     def set_shapes(self, sample_variant: int, check_item_cap: int) -> None:
         """Fix the sampler variant (index into SAMPLE_VARIANTS) and the check
         work-item cap instead of tuning."""

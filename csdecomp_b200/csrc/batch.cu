@@ -411,7 +411,11 @@ __global__ void __launch_bounds__(1024) batch_sort_kernel(BatchArgs a) {
       __syncthreads();
     }
   int* ord = a.order + (size_t)slot * a.n_max;
-  for (int i = threadIdx.x; i < N; i += blockDim.x) ord[i] = (int)(keys[i] & 0xffffffffu);
+  uint8_t* flags = a.bpool + a.slots[slot].flag_off;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    ord[i] = (int)(keys[i] & 0xffffffffu);
+    flags[i] = 2;  // unchecked this iteration
+  }
   if (threadIdx.x == 0) {
     SlotState& S = a.slots[slot];
     S.pos = 0;
@@ -517,8 +521,10 @@ __global__ void __launch_bounds__(256) batch_tally_kernel(BatchArgs a, int r) {
   }
 }
 
-// Block per slot: ordered compaction of the colliding samples over the
-// checked sorted positions, the admissibility decision and the particle count.
+// Block per slot: ordered compaction (by sample index, as the plain form) of
+// the colliding samples among those checked, the admissibility decision and
+// the particle count. If no colliding sample was left unchecked, the
+// particles are exactly the plain form's.
 __global__ void __launch_bounds__(1024) batch_compact_sorted_kernel(BatchArgs a) {
   __shared__ int warp_n[32];
   __shared__ int base;
@@ -528,23 +534,17 @@ __global__ void __launch_bounds__(1024) batch_compact_sorted_kernel(BatchArgs a)
     if (threadIdx.x == 0) S.done = 1;
     return;
   }
-  const int k = a.it->k;
-  const int npos = S.pos, dim = S.dim;
-  const int* ord = a.order + (size_t)blockIdx.x * a.n_max;
+  const int k = a.it->k, N = a.n_tab[k];
+  const int dim = S.dim;
   const uint8_t* flags = a.bpool + S.flag_off;
   const float* smp = a.fpool + S.smp_off;
   float* cols = a.fpool + S.col_off;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   if (tid == 0) base = 0;
   __syncthreads();
-  for (int p0 = 0; p0 < npos; p0 += blockDim.x) {
-    const int p = p0 + tid;
-    int i = 0;
-    bool c = false;
-    if (p < npos) {
-      i = ord[p];
-      c = flags[i] == 0;
-    }
+  for (int i0 = 0; i0 < N; i0 += blockDim.x) {
+    const int i = i0 + tid;
+    const bool c = i < N && flags[i] == 0;
     const unsigned m = __ballot_sync(0xffffffffu, c);
     if (lane == 0) warp_n[warp] = __popc(m);
     __syncthreads();
@@ -559,7 +559,7 @@ __global__ void __launch_bounds__(1024) batch_compact_sorted_kernel(BatchArgs a)
     __syncthreads();
   }
   if (tid == 0) {
-    S.configs += npos;
+    S.configs += S.pos;
     S.cnt.total = (uint32_t)base;
     S.cnt.first_m = (uint32_t)S.m_coll;
     if ((float)S.m_coll <= a.thr_tab[k]) {
@@ -617,7 +617,7 @@ struct csd_batch_s {
   // surrogate mode
   csd_mlp_t mlp = nullptr;
   float stop_logit = 0.f;
-  int rounds = 5, round_base = 512;
+  int rounds = 3, round_base = 1024;
   csd::DevBuf scores, order, status;
   std::vector<csd::SlotState> host_slots;
   std::vector<int> act_host;
@@ -772,12 +772,15 @@ csd_status_t csd_batch_create(const csd_plant_t* plants, int32_t num_plants, int
   h->check_smem = (size_t)max_wf * sizeof(float) * kWarpsPerBlock + (h->sm ? (size_t)max_static : 0);
   csd_status_t s;
   int g1 = 0, g2 = 0;
+  int g3 = 0;
   if (h->sm) {
     if ((s = grid_for(batch_check_kernel<true>, h->check_smem, 1ll << 40, &g1, kWarpsPerBlock))) return s;
     if ((s = grid_for(batch_bisect_kernel<true>, h->check_smem, 1ll << 40, &g2, kWarpsPerBlock))) return s;
+    if ((s = grid_for(batch_check_sorted_kernel<true>, h->check_smem, 1ll << 40, &g3, kWarpsPerBlock))) return s;
   } else {
     if ((s = grid_for(batch_check_kernel<false>, h->check_smem, 1ll << 40, &g1, kWarpsPerBlock))) return s;
     if ((s = grid_for(batch_bisect_kernel<false>, h->check_smem, 1ll << 40, &g2, kWarpsPerBlock))) return s;
+    if ((s = grid_for(batch_check_sorted_kernel<false>, h->check_smem, 1ll << 40, &g3, kWarpsPerBlock))) return s;
   }
   h->check_grid = g1;
   h->bisect_grid = g2;
@@ -1117,6 +1120,15 @@ csd_status_t csd_batch_set_surrogate(csd_batch_t h, csd_mlp_t mlp, float stop_pr
                                     (int)(kSortMax * sizeof(unsigned long long))));
   h->mlp = mlp;
   h->stop_logit = std::log(stop_probability / (1.f - stop_probability));
+  return CSD_OK;
+}
+
+csd_status_t csd_batch_set_surrogate_rounds(csd_batch_t h, int32_t rounds, int32_t first_round) {
+  CSD_CHECK(h && rounds >= 1 && rounds <= 8 && first_round >= 32, CSD_ERR_INVALID,
+            "rounds must be in [1, 8] and the first round at least 32 samples");
+  h->rounds = rounds;
+  h->round_base = first_round;
+  h->graph_slots = -1;
   return CSD_OK;
 }
 

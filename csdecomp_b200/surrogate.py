@@ -104,7 +104,7 @@ class CollisionSurrogate:
 
     def __del__(self):
         h = getattr(self, "_handle", None)
-        if h and C._lib is not None:
+        if h and C is not None and C._lib is not None:
             try:
                 C._lib.csd_mlp_destroy(h)
             except Exception:  # pragma: no cover

@@ -242,13 +242,18 @@ csd_status_t csd_batch_autotune(csd_batch_t h, int32_t iterations);
 /* Surrogate-guided checking (mlp: one net per plant of the batch, same
  * dimensions; NULL turns it off). Each iteration then scores every sample
  * with the net, checks the samples in decreasing predicted collision
- * probability in up to 5 rounds, and stops checking a slot once its
+ * probability in rounds (csd_batch_set_surrogate_rounds), and stops checking a slot once its
  * admissibility is decided and, if inadmissible, num_particles collisions are
  * known or the next sample's predicted probability is below
  * stop_probability. Every verdict used is the exact checker's; the
  * admissibility test (first M samples) is unchanged; the bisected particles
- * are the collisions found, in that order. */
+ * are the first num_particles collisions found, in sample order (the plain
+ * form's particles whenever no colliding sample was left unchecked). */
 csd_status_t csd_batch_set_surrogate(csd_batch_t h, csd_mlp_t mlp, float stop_probability);
+/* Round schedule of the surrogate-guided check: round r covers sorted
+ * positions up to first_round * (2^(r+1) - 1), the last round the rest
+ * (defaults: 3 rounds, first round 1024 samples). */
+csd_status_t csd_batch_set_surrogate_rounds(csd_batch_t h, int32_t rounds, int32_t first_round);
 /* Sets the shapes directly (e.g. a tuning result kept from an earlier run):
  * sampler variant index as above, check work-item cap a multiple of 8. */
 csd_status_t csd_batch_set_shapes(csd_batch_t h, int32_t sample_variant, int32_t check_item_cap);
