@@ -18,6 +18,8 @@
 #pragma once
 #include <algorithm>
 
+#include <cfloat>
+
 #include "csd_internal.h"
 
 namespace csd {
@@ -197,15 +199,16 @@ static __device__ __forceinline__ void own_sphere(const DevPlant& p, const float
 // Tile t (moving spheres 32t .. 32t+31) against its static geometries and
 // moving-sphere partners. Returns the warp-uniform "some pair collides".
 static __device__ bool sweep_tile(const DevPlant& p, const float4* stat, const float4* aabb, const float* pose, int t,
-                                  int lane) {
+                                  int lane, bool skip_dense) {
   const TileInfo ti = p.tiles[t];
   float c[4];
   own_sphere(p, pose, t * kWarp + lane, c);
   const float r2 = c[3] * c[3];
   bool hit = false;
   const int s0 = 0, s1 = p.num_ssph, s2 = s1 + p.num_sabox, s3 = s2 + p.num_srbox, s4 = s3 + p.num_scap;
-  // static spheres
-  if (ti.dense[SC_SPH]) {
+  // static spheres (with skip_dense: swept with the aligned boxes by sweep_dense_spheres)
+  if (skip_dense) {
+  } else if (ti.dense[SC_SPH]) {
     int s = s0;
     for (; s + 8 <= s1; s += 8) {
 #pragma unroll
@@ -238,7 +241,8 @@ static __device__ bool sweep_tile(const DevPlant& p, const float4* stat, const f
   }
   if (__any_sync(kFull, hit)) return true;
   // axis-aligned static boxes
-  if (ti.dense[SC_ABOX]) {
+  if (skip_dense) {
+  } else if (ti.dense[SC_ABOX]) {
     int i = 0;
     for (; i + 8 <= p.num_sabox; i += 8) {
 #pragma unroll
@@ -298,6 +302,91 @@ static __device__ bool sweep_tile(const DevPlant& p, const float4* stat, const f
   return __any_sync(kFull, hit);
 }
 
+// NaN-propagating minimum (a NaN distance counts as a collision, as in the
+// compare-based tests).
+static __device__ __forceinline__ float fmin_nan(float a, float b) {
+  float r;
+  asm("min.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+  return r;
+}
+
+// Moving spheres against the static spheres and axis-aligned boxes when every
+// tile is dense for both classes: lane holds spheres lane, lane + 32, ...
+// (R of them), so each broadcast static feeds R tests. A pair collides iff
+// d^2 - (r_a + r_b)^2 < 0 (one rounding, by FMA) and hits accumulate as a
+// NaN-propagating minimum voted every 8 statics.
+template <int R>
+static __device__ bool sweep_dense_spheres(const DevPlant& p, const float4* stat, const float4* aabb, const float* pose,
+                                           int lane) {
+  float cx[R], cy[R], cz[R], cr[R];
+#pragma unroll
+  for (int j = 0; j < R; ++j) {
+    float c[4];
+    own_sphere(p, pose, j * kWarp + lane, c);
+    cx[j] = c[0];
+    cy[j] = c[1];
+    cz[j] = c[2];
+    cr[j] = c[3];
+  }
+  float m = FLT_MAX;
+  const int ns = p.num_ssph;
+  int s = 0;
+  for (; s + 8 <= ns; s += 8) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const float4 S = stat[4 * (s + u)];
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        const float d0 = cx[j] - S.x, d1 = cy[j] - S.y, d2 = cz[j] - S.z;
+        const float dd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+        const float rr = cr[j] + S.w;
+        m = fmin_nan(m, fmaf(-rr, rr, dd));
+      }
+    }
+    if (__any_sync(kFull, !(m >= 0.f))) return true;
+  }
+  for (; s < ns; ++s) {
+    const float4 S = stat[4 * s];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const float d0 = cx[j] - S.x, d1 = cy[j] - S.y, d2 = cz[j] - S.z;
+      const float dd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
+      const float rr = cr[j] + S.w;
+      m = fmin_nan(m, fmaf(-rr, rr, dd));
+    }
+  }
+  if (__any_sync(kFull, !(m >= 0.f))) return true;
+  const int nb = p.num_sabox;
+  int i = 0;
+  for (; i + 8 <= nb; i += 8) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const float4 P = aabb[2 * (i + u)], H = aabb[2 * (i + u) + 1];
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        const float e0 = fmaxf(fabsf(cx[j] - P.x) - H.x, 0.f);
+        const float e1 = fmaxf(fabsf(cy[j] - P.y) - H.y, 0.f);
+        const float e2 = fmaxf(fabsf(cz[j] - P.z) - H.z, 0.f);
+        const float ee = fmaf(e2, e2, fmaf(e1, e1, e0 * e0));
+        m = fmin_nan(m, fmaf(-cr[j], cr[j], ee));
+      }
+    }
+    if (__any_sync(kFull, !(m >= 0.f))) return true;
+  }
+  for (; i < nb; ++i) {
+    const float4 P = aabb[2 * i], H = aabb[2 * i + 1];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      const float e0 = fmaxf(fabsf(cx[j] - P.x) - H.x, 0.f);
+      const float e1 = fmaxf(fabsf(cy[j] - P.y) - H.y, 0.f);
+      const float e2 = fmaxf(fabsf(cz[j] - P.z) - H.z, 0.f);
+      const float ee = fmaf(e2, e2, fmaf(e1, e1, e0 * e0));
+      m = fmin_nan(m, fmaf(-cr[j], cr[j], ee));
+    }
+  }
+  return __any_sync(kFull, !(m >= 0.f));
+}
+
 template <int T>
 struct Words {
   static constexpr int n = T == G_SPHERE ? 4 : T == G_CAPSULE ? 8 : 16;
@@ -307,11 +396,16 @@ struct Words {
 template <int TA, int TB, bool BSTATIC>
 static __device__ bool generic_segment(const DevPlant& p, const float4* stat, const float* pose, const GenSeg& sg,
                                        int lane) {
+  // the next pass's pair indices are loaded one pass ahead (their latency
+  // would otherwise stall every pass)
+  GenericPair nxt{0u, 0u};
+  if (sg.begin + lane < sg.end) nxt = p.generic[sg.begin + lane];
   for (int base = sg.begin; base < sg.end; base += kWarp) {
     const int k = base + lane;
+    const GenericPair gp = nxt;
+    if (k + kWarp < sg.end) nxt = p.generic[k + kWarp];
     bool hit = false;
     if (k < sg.end) {
-      const GenericPair gp = p.generic[k];
       float A[Words<TA>::n], B[Words<TB>::n];
       const float4* pa = reinterpret_cast<const float4*>(pose + pose_offset(p, (int)gp.a));
 #pragma unroll
@@ -333,6 +427,82 @@ static __device__ bool generic_segment(const DevPlant& p, const float4* stat, co
   return false;
 }
 
+// Capsule x box segment with a broad phase: a lane tests its pair's capsule
+// bounding sphere (centre, radius + half length) against the box; pairs that
+// pass are compacted into a warp-wide batch (lane r of the batch holds the
+// r-th candidate) and the exact segment-box test runs on full batches.
+template <bool BSTATIC>
+static __device__ bool cap_box_exact(const DevPlant& p, const float4* stat, const float* pose, int k) {
+  bool hit = false;
+  if (k >= 0) {
+    const GenericPair gp = p.generic[k];
+    float A[8], B[16];
+    const float4* pa = reinterpret_cast<const float4*>(pose + pose_offset(p, (int)gp.a));
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      float4 v = pa[i];
+      A[4 * i] = v.x; A[4 * i + 1] = v.y; A[4 * i + 2] = v.z; A[4 * i + 3] = v.w;
+    }
+    const float4* pb = BSTATIC ? stat + 4 * (gp.b & 0x7fffffffu)
+                               : reinterpret_cast<const float4*>(pose + pose_offset(p, (int)gp.b));
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      float4 v = pb[i];
+      B[4 * i] = v.x; B[4 * i + 1] = v.y; B[4 * i + 2] = v.z; B[4 * i + 3] = v.w;
+    }
+    hit = cap_box_hit(A, B);
+  }
+  return __any_sync(kFull, hit);
+}
+
+template <bool BSTATIC>
+static __device__ bool cap_box_segment(const DevPlant& p, const float4* stat, const float* pose, const GenSeg& sg,
+                                       int lane) {
+  int pend = -1;  // pair index this lane holds in the pending batch
+  int npend = 0;  // warp-uniform batch fill
+  GenericPair nxt{0u, 0u};
+  if (sg.begin + lane < sg.end) nxt = p.generic[sg.begin + lane];
+  for (int base = sg.begin; base < sg.end; base += kWarp) {
+    const int k = base + lane;
+    const GenericPair gp = nxt;
+    if (k + kWarp < sg.end) nxt = p.generic[k + kWarp];
+    bool cand = false;
+    if (k < sg.end) {
+      const int oa = pose_offset(p, (int)gp.a);
+      const float4 ca = *reinterpret_cast<const float4*>(pose + oa);
+      const float hl = pose[oa + 7];
+      const float4* pb = BSTATIC ? stat + 4 * (gp.b & 0x7fffffffu)
+                                 : reinterpret_cast<const float4*>(pose + pose_offset(p, (int)gp.b));
+      float B[16];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        float4 v = pb[i];
+        B[4 * i] = v.x; B[4 * i + 1] = v.y; B[4 * i + 2] = v.z; B[4 * i + 3] = v.w;
+      }
+      const float c[3] = {ca.x, ca.y, ca.z};
+      cand = sph_box_hit(c, ca.w + hl, B);
+    }
+    const unsigned m = __ballot_sync(kFull, cand);
+    const int cnt = __popc(m);
+    const int take = min(cnt, kWarp - npend);
+    const int r = lane - npend;
+    const int src = (r >= 0 && r < take) ? (int)__fns(m, 0, r + 1) : 0;
+    const int kk = __shfl_sync(kFull, k, src);
+    if (r >= 0 && r < take) pend = kk;
+    npend += take;
+    if (npend == kWarp) {
+      if (cap_box_exact<BSTATIC>(p, stat, pose, pend)) return true;
+      const int over = cnt - take;
+      const int src2 = lane < over ? (int)__fns(m, 0, take + lane + 1) : 0;
+      const int k2 = __shfl_sync(kFull, k, src2);
+      pend = lane < over ? k2 : -1;
+      npend = over;
+    }
+  }
+  if (npend > 0) return cap_box_exact<BSTATIC>(p, stat, pose, lane < npend ? pend : -1);
+  return false;
+}
+
 // Remaining pairs (the moving geometry first; moving-moving pairs ordered
 // sphere < capsule < box), dispatched once per segment.
 static __device__ bool sweep_generic(const DevPlant& p, const float4* stat, const float* pose, int lane) {
@@ -345,7 +515,7 @@ static __device__ bool sweep_generic(const DevPlant& p, const float4* stat, cons
       case G_SPHERE * 4 + G_CAPSULE: h = generic_segment<G_SPHERE, G_CAPSULE, false>(p, stat, pose, sg, lane); break;
       case G_SPHERE * 4 + G_BOX: h = generic_segment<G_SPHERE, G_BOX, false>(p, stat, pose, sg, lane); break;
       case G_CAPSULE * 4 + G_CAPSULE: h = generic_segment<G_CAPSULE, G_CAPSULE, false>(p, stat, pose, sg, lane); break;
-      case G_CAPSULE * 4 + G_BOX: h = generic_segment<G_CAPSULE, G_BOX, false>(p, stat, pose, sg, lane); break;
+      case G_CAPSULE * 4 + G_BOX: h = cap_box_segment<false>(p, stat, pose, sg, lane); break;
       case G_BOX * 4 + G_BOX: h = generic_segment<G_BOX, G_BOX, false>(p, stat, pose, sg, lane); break;
       case G_BOX * 4 + G_SPHERE: h = generic_segment<G_BOX, G_SPHERE, false>(p, stat, pose, sg, lane); break;
       case G_BOX * 4 + G_CAPSULE: h = generic_segment<G_BOX, G_CAPSULE, false>(p, stat, pose, sg, lane); break;
@@ -353,7 +523,7 @@ static __device__ bool sweep_generic(const DevPlant& p, const float4* stat, cons
       case G_SPHERE * 4 + G_SPHERE: h = generic_segment<G_SPHERE, G_SPHERE, false>(p, stat, pose, sg, lane); break;
       // moving-static
       case 16 + G_CAPSULE * 4 + G_SPHERE: h = generic_segment<G_CAPSULE, G_SPHERE, true>(p, stat, pose, sg, lane); break;
-      case 16 + G_CAPSULE * 4 + G_BOX: h = generic_segment<G_CAPSULE, G_BOX, true>(p, stat, pose, sg, lane); break;
+      case 16 + G_CAPSULE * 4 + G_BOX: h = cap_box_segment<true>(p, stat, pose, sg, lane); break;
       case 16 + G_CAPSULE * 4 + G_CAPSULE: h = generic_segment<G_CAPSULE, G_CAPSULE, true>(p, stat, pose, sg, lane); break;
       case 16 + G_BOX * 4 + G_SPHERE: h = generic_segment<G_BOX, G_SPHERE, true>(p, stat, pose, sg, lane); break;
       case 16 + G_BOX * 4 + G_BOX: h = generic_segment<G_BOX, G_BOX, true>(p, stat, pose, sg, lane); break;
@@ -416,8 +586,19 @@ static __device__ bool check_config(const DevPlant& p, const float4* stat, const
   place_all(p, X, pose, lane);
   __syncwarp();
   if (p.always_colliding) return true;
+  const bool dense = p.dense_spheres && p.num_tiles >= 1 && p.num_tiles <= 4;
+  if (dense) {
+    bool h;
+    switch (p.num_tiles) {
+      case 1: h = sweep_dense_spheres<1>(p, stat, aabb, pose, lane); break;
+      case 2: h = sweep_dense_spheres<2>(p, stat, aabb, pose, lane); break;
+      case 3: h = sweep_dense_spheres<3>(p, stat, aabb, pose, lane); break;
+      default: h = sweep_dense_spheres<4>(p, stat, aabb, pose, lane); break;
+    }
+    if (h) return true;
+  }
   for (int t = 0; t < p.num_tiles; ++t)
-    if (sweep_tile(p, stat, aabb, pose, t, lane)) return true;
+    if (sweep_tile(p, stat, aabb, pose, t, lane, dense)) return true;
   if (sweep_generic(p, stat, pose, lane)) return true;
   if (va.nv > 0 && sweep_voxels(p, stat, pose, va, lane)) return true;
   return false;

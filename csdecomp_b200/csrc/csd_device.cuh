@@ -97,6 +97,8 @@ struct DevPlant {
   int always_colliding;  // a static-static pair collides
   int num_links;         // all links of the reference tree (FK output)
   int static_bytes;      // bytes of statics + aabb staged in shared memory (multiple of 16)
+  int dense_spheres;     // every tile pairs every lane with every static sphere and aligned box
+  int pad_dense;
   const FkJoint* fk;
   const MovingGeom* moving;
   const float4* statics;       // [num_static][4] float4 (WG format); followed by aabb

@@ -381,6 +381,7 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   std::vector<uint32_t> masks((size_t)T * S, 0u);               // tile x static
   std::vector<uint32_t> self_masks((size_t)T * nmsph, 0u);      // tile x moving-sphere partner
   std::vector<GenericPair> generic;
+  std::vector<GenericPair> self_pairs;  // moving sphere x moving sphere
   int always = 0, tile_pairs = 0;
   auto ref = [&](int g) -> uint32_t {
     int m = hp.moving_of_geom[g];
@@ -407,11 +408,24 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
     if (ma >= 0 && mb >= 0 && ma < nmsph && mb < nmsph && ma != mb) {
       int lo = std::min(ma, mb), hi = std::max(ma, mb);
       self_masks[(size_t)(lo / kWarp) * nmsph + hi] |= 1u << (lo % kWarp);
+      self_pairs.push_back({(uint32_t)lo, (uint32_t)hi});
       continue;
     }
     // generic: the moving geometry first
     if (ma < 0 || (mb >= 0 && mb < ma)) std::swap(a, b);
     generic.push_back({ref(a), ref(b)});
+  }
+  // Self pairs as masked tile entries cost about one warp pass per (tile,
+  // partner) with a nonzero mask; as generic pairs, one pass per 32 pairs
+  // with two pose loads each. Keep the cheaper form.
+  {
+    size_t entries_needed = 0;
+    for (uint32_t w : self_masks) entries_needed += w != 0u;
+    const size_t generic_passes = (self_pairs.size() + kWarp - 1) / kWarp;
+    if (15 * entries_needed > 18 * generic_passes) {
+      std::fill(self_masks.begin(), self_masks.end(), 0u);
+      generic.insert(generic.end(), self_pairs.begin(), self_pairs.end());
+    }
   }
   auto type_of_ref = [&](uint32_t r) {
     return (r & 0x80000000u) ? hp.static_type[r & 0x7fffffffu] : hp.moving[r].type;
@@ -549,6 +563,11 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   dp.static_bytes = (int)static_bytes;
   dp.pose_words = pose_words;
   dp.always_colliding = always;
+  {
+    int dense = T > 0;
+    for (int t = 0; t < T; ++t) dense &= tiles[t].dense[SC_SPH] && tiles[t].dense[SC_ABOX];
+    dp.dense_spheres = dense;
+  }
   dp.num_links = L;
   dp.fk = (const FkJoint*)(base + o_fk);
   dp.moving = (const MovingGeom*)(base + o_mv);
