@@ -88,7 +88,7 @@ EXPORTS = (
     "csd_batch_set_profiling", "csd_batch_stage_ms", "csd_batch_iteration_profile",
     "csd_batch_autotune", "csd_batch_tuning", "csd_batch_set_shapes", "csd_batch_set_surrogate",
     "csd_batch_set_surrogate_rounds",    "csd_batch_destroy",
-    "csd_num_samples_unadaptive", "csd_fp32_fma_probe", "csd_plant_flops",
+    "csd_num_samples_unadaptive", "csd_fp32_fma_probe", "csd_plant_flops", "csd_plant_set_culling",
     "csd_mlp_num_params", "csd_mlp_create", "csd_mlp_destroy", "csd_mlp_get_params", "csd_mlp_set_params",
     "csd_mlp_infer", "csd_mlp_gradients", "csd_mlp_train", "csd_mlp_gemm_test",
 )
@@ -155,6 +155,10 @@ class PlantHandle:
         self.handle = h
         self.dim = dim
         self.num_links = num_links
+
+    def set_culling(self, enable: bool) -> None:
+        """Link-level broad phase of the collision checks on (default) or off."""
+        check(lib().csd_plant_set_culling(self.handle, int(bool(enable))))
 
     def flops(self) -> dict:
         fk, pl, pa = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()

@@ -195,11 +195,76 @@ static __device__ __forceinline__ void own_sphere(const DevPlant& p, const float
   }
 }
 
+// ------------------------------------------------------------ broad phase
+// Link-level culling of one configuration. Lane k (< num_slots) places its
+// slot's bounding sphere in the world; `link` (lane k) has bit j set when the
+// spheres of slots k and j overlap, `stat` (lane g) has bit i set when static
+// 32 g + i overlaps some slot sphere. The spheres are padded on the host, so a
+// culled pair is separated by at least 1e-4 m. With culling off every bit is
+// set.
+struct Cull {
+  uint32_t link;
+  uint32_t stat;
+};
+
+static __device__ __forceinline__ Cull broad_phase(const DevPlant& p, const float4* aabb, const float* X, int lane) {
+  Cull c{~0u, ~0u};
+  if (!p.cull) return c;
+  float cx = 0.f, cy = 0.f, cz = 0.f, cr = -1.f;
+  if (lane < p.num_slots) {
+    const float4 b = __ldg(p.slot_bs + lane);
+    const float* x = X + lane * 12;
+    cx = fmaf(x[6], b.z, fmaf(x[3], b.y, fmaf(x[0], b.x, x[9])));
+    cy = fmaf(x[7], b.z, fmaf(x[4], b.y, fmaf(x[1], b.x, x[10])));
+    cz = fmaf(x[8], b.z, fmaf(x[5], b.y, fmaf(x[2], b.x, x[11])));
+    cr = b.w;
+  }
+  uint32_t lw = 0;
+  for (int j = 0; j < p.num_slots; ++j) {
+    const float ox = __shfl_sync(kFull, cx, j), oy = __shfl_sync(kFull, cy, j), oz = __shfl_sync(kFull, cz, j);
+    const float orr = __shfl_sync(kFull, cr, j);
+    const float dx = cx - ox, dy = cy - oy, dz = cz - oz, t = cr + orr;
+    if (cr >= 0.f && orr >= 0.f && fmaf(dz, dz, fmaf(dy, dy, dx * dx)) <= t * t) lw |= 1u << j;
+  }
+  c.link = lw;
+  const float4* sbs = aabb + 2 * p.num_sabox;
+  uint32_t sw = 0;
+  for (int g = 0; g * kWarp < p.num_static; ++g) {
+    const int st = g * kWarp + lane;
+    float4 S = make_float4(0.f, 0.f, 0.f, -1.f);
+    if (st < p.num_static) S = sbs[st];
+    bool near = false;
+    for (int k = 0; k < p.num_slots; ++k) {
+      const float kx = __shfl_sync(kFull, cx, k), ky = __shfl_sync(kFull, cy, k), kz = __shfl_sync(kFull, cz, k);
+      const float kr = __shfl_sync(kFull, cr, k);
+      const float dx = kx - S.x, dy = ky - S.y, dz = kz - S.z, t = kr + S.w;
+      near |= kr >= 0.f && S.w >= 0.f && fmaf(dz, dz, fmaf(dy, dy, dx * dx)) <= t * t;
+    }
+    const uint32_t bits = __ballot_sync(kFull, near);
+    if (lane == g) sw = bits;
+  }
+  c.stat = sw;
+  return c;
+}
+
+// Flag bit of static s (every lane may ask for a different s; all lanes call).
+static __device__ __forceinline__ bool static_near(const Cull& c, int s) {
+  return (__shfl_sync(kFull, c.stat, (s >> 5) & 31) >> (s & 31)) & 1u;
+}
+
+// Flag bits of statics [w0, w0 + 32) restricted to [lo, hi) (w0 a multiple of 32).
+static __device__ __forceinline__ uint32_t near_bits(const Cull& c, int w0, int lo, int hi) {
+  uint32_t b = __shfl_sync(kFull, c.stat, (w0 >> 5) & 31);
+  if (lo > w0) b &= ~((1u << (lo - w0)) - 1u);
+  if (hi - w0 < 32) b &= (1u << (hi - w0)) - 1u;
+  return b;
+}
+
 // ------------------------------------------------------------------- sweeps
 // Tile t (moving spheres 32t .. 32t+31) against its static geometries and
 // moving-sphere partners. Returns the warp-uniform "some pair collides".
 static __device__ bool sweep_tile(const DevPlant& p, const float4* stat, const float4* aabb, const float* pose, int t,
-                                  int lane, bool skip_dense) {
+                                  int lane, bool skip_dense, const Cull& cu) {
   const TileInfo ti = p.tiles[t];
   float c[4];
   own_sphere(p, pose, t * kWarp + lane, c);
@@ -231,6 +296,7 @@ static __device__ bool sweep_tile(const DevPlant& p, const float4* stat, const f
   } else {
     for (int e = ti.ent[SC_SPH]; e < ti.ent[SC_SPH + 1]; ++e) {
       TileEntry en = p.entries[e];
+      if (!static_near(cu, (int)en.s)) continue;
       float4 S = stat[4 * en.s];
       float d0 = c[0] - S.x, d1 = c[1] - S.y, d2 = c[2] - S.z;
       float dd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
@@ -253,6 +319,7 @@ static __device__ bool sweep_tile(const DevPlant& p, const float4* stat, const f
   } else {
     for (int e = ti.ent[SC_ABOX]; e < ti.ent[SC_ABOX + 1]; ++e) {
       TileEntry en = p.entries[e];
+      if (!static_near(cu, (int)en.s)) continue;
       const int i = en.s - s1;
       hit |= ((en.mask >> lane) & 1u) && sph_abox_hit(c, c[3], aabb[2 * i], aabb[2 * i + 1]);
       if ((e & 7) == 7 && __any_sync(kFull, hit)) return true;
@@ -268,6 +335,7 @@ static __device__ bool sweep_tile(const DevPlant& p, const float4* stat, const f
       s = en.s;
       mask = en.mask;
     }
+    if (!static_near(cu, s)) continue;
     float B[16];
     load4f(stat + 4 * s, 4, B);
     hit |= ((mask >> lane) & 1u) && sph_box_hit(c, c[3], B);
@@ -282,6 +350,7 @@ static __device__ bool sweep_tile(const DevPlant& p, const float4* stat, const f
       s = en.s;
       mask = en.mask;
     }
+    if (!static_near(cu, s)) continue;
     float C[8];
     load4f(stat + 4 * s, 2, C);
     hit |= ((mask >> lane) & 1u) && sph_cap_hit(c, C);
@@ -317,7 +386,7 @@ static __device__ __forceinline__ float fmin_nan(float a, float b) {
 // NaN-propagating minimum voted every 8 statics.
 template <int R>
 static __device__ bool sweep_dense_spheres(const DevPlant& p, const float4* stat, const float4* aabb, const float* pose,
-                                           int lane) {
+                                           int lane, const Cull& cu) {
   float cx[R], cy[R], cz[R], cr[R];
 #pragma unroll
   for (int j = 0; j < R; ++j) {
@@ -329,12 +398,14 @@ static __device__ bool sweep_dense_spheres(const DevPlant& p, const float4* stat
     cr[j] = c[3];
   }
   float m = FLT_MAX;
-  const int ns = p.num_ssph;
-  int s = 0;
-  for (; s + 8 <= ns; s += 8) {
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const float4 S = stat[4 * (s + u)];
+  int cnt = 0;
+  const int ns = p.num_ssph, nb = p.num_sabox;
+  for (int w0 = 0; w0 < ns; w0 += kWarp) {
+    uint32_t bits = near_bits(cu, w0, 0, ns);
+    while (bits) {
+      const int st = w0 + __ffs(bits) - 1;
+      bits &= bits - 1u;
+      const float4 S = stat[4 * st];
 #pragma unroll
       for (int j = 0; j < R; ++j) {
         const float d0 = cx[j] - S.x, d1 = cy[j] - S.y, d2 = cz[j] - S.z;
@@ -342,26 +413,16 @@ static __device__ bool sweep_dense_spheres(const DevPlant& p, const float4* stat
         const float rr = cr[j] + S.w;
         m = fmin_nan(m, fmaf(-rr, rr, dd));
       }
-    }
-    if (__any_sync(kFull, !(m >= 0.f))) return true;
-  }
-  for (; s < ns; ++s) {
-    const float4 S = stat[4 * s];
-#pragma unroll
-    for (int j = 0; j < R; ++j) {
-      const float d0 = cx[j] - S.x, d1 = cy[j] - S.y, d2 = cz[j] - S.z;
-      const float dd = fmaf(d2, d2, fmaf(d1, d1, d0 * d0));
-      const float rr = cr[j] + S.w;
-      m = fmin_nan(m, fmaf(-rr, rr, dd));
+      if ((++cnt & 7) == 0 && __any_sync(kFull, !(m >= 0.f))) return true;
     }
   }
   if (__any_sync(kFull, !(m >= 0.f))) return true;
-  const int nb = p.num_sabox;
-  int i = 0;
-  for (; i + 8 <= nb; i += 8) {
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const float4 P = aabb[2 * (i + u)], H = aabb[2 * (i + u) + 1];
+  for (int w0 = ns & ~(kWarp - 1); w0 < ns + nb; w0 += kWarp) {
+    uint32_t bits = near_bits(cu, w0, ns, ns + nb);
+    while (bits) {
+      const int i = w0 + __ffs(bits) - 1 - ns;
+      bits &= bits - 1u;
+      const float4 P = aabb[2 * i], H = aabb[2 * i + 1];
 #pragma unroll
       for (int j = 0; j < R; ++j) {
         const float e0 = fmaxf(fabsf(cx[j] - P.x) - H.x, 0.f);
@@ -370,18 +431,7 @@ static __device__ bool sweep_dense_spheres(const DevPlant& p, const float4* stat
         const float ee = fmaf(e2, e2, fmaf(e1, e1, e0 * e0));
         m = fmin_nan(m, fmaf(-cr[j], cr[j], ee));
       }
-    }
-    if (__any_sync(kFull, !(m >= 0.f))) return true;
-  }
-  for (; i < nb; ++i) {
-    const float4 P = aabb[2 * i], H = aabb[2 * i + 1];
-#pragma unroll
-    for (int j = 0; j < R; ++j) {
-      const float e0 = fmaxf(fabsf(cx[j] - P.x) - H.x, 0.f);
-      const float e1 = fmaxf(fabsf(cy[j] - P.y) - H.y, 0.f);
-      const float e2 = fmaxf(fabsf(cz[j] - P.z) - H.z, 0.f);
-      const float ee = fmaf(e2, e2, fmaf(e1, e1, e0 * e0));
-      m = fmin_nan(m, fmaf(-cr[j], cr[j], ee));
+      if ((++cnt & 7) == 0 && __any_sync(kFull, !(m >= 0.f))) return true;
     }
   }
   return __any_sync(kFull, !(m >= 0.f));
@@ -393,9 +443,18 @@ struct Words {
 };
 
 // One type-uniform segment of generic pairs, one pair per lane.
+// Whether a generic pair survives the broad phase: its static is near some
+// link, or its two moving geometries' link spheres overlap (all lanes call).
+template <bool BSTATIC>
+static __device__ __forceinline__ bool pair_near(const DevPlant& p, const Cull& cu, const GenericPair& gp, bool valid) {
+  if (BSTATIC) return static_near(cu, valid ? (int)(gp.b & 0x7fffffffu) : 0) && valid;
+  const int sa = valid ? (int)__ldg(p.moving_slot + gp.a) : 0, sb = valid ? (int)__ldg(p.moving_slot + gp.b) : 0;
+  return ((__shfl_sync(kFull, cu.link, sa & 31) >> (sb & 31)) & 1u) && valid;
+}
+
 template <int TA, int TB, bool BSTATIC>
 static __device__ bool generic_segment(const DevPlant& p, const float4* stat, const float* pose, const GenSeg& sg,
-                                       int lane) {
+                                       int lane, const Cull& cu) {
   // the next pass's pair indices are loaded one pass ahead (their latency
   // would otherwise stall every pass)
   GenericPair nxt{0u, 0u};
@@ -404,8 +463,10 @@ static __device__ bool generic_segment(const DevPlant& p, const float4* stat, co
     const int k = base + lane;
     const GenericPair gp = nxt;
     if (k + kWarp < sg.end) nxt = p.generic[k + kWarp];
+    const bool keep = pair_near<BSTATIC>(p, cu, gp, k < sg.end);
+    if (!__any_sync(kFull, keep)) continue;
     bool hit = false;
-    if (k < sg.end) {
+    if (keep) {
       float A[Words<TA>::n], B[Words<TB>::n];
       const float4* pa = reinterpret_cast<const float4*>(pose + pose_offset(p, (int)gp.a));
 #pragma unroll
@@ -457,7 +518,7 @@ static __device__ bool cap_box_exact(const DevPlant& p, const float4* stat, cons
 
 template <bool BSTATIC>
 static __device__ bool cap_box_segment(const DevPlant& p, const float4* stat, const float* pose, const GenSeg& sg,
-                                       int lane) {
+                                       int lane, const Cull& cu) {
   int pend = -1;  // pair index this lane holds in the pending batch
   int npend = 0;  // warp-uniform batch fill
   GenericPair nxt{0u, 0u};
@@ -466,8 +527,9 @@ static __device__ bool cap_box_segment(const DevPlant& p, const float4* stat, co
     const int k = base + lane;
     const GenericPair gp = nxt;
     if (k + kWarp < sg.end) nxt = p.generic[k + kWarp];
+    const bool keep = pair_near<BSTATIC>(p, cu, gp, k < sg.end);
     bool cand = false;
-    if (k < sg.end) {
+    if (keep) {
       const int oa = pose_offset(p, (int)gp.a);
       const float4 ca = *reinterpret_cast<const float4*>(pose + oa);
       const float hl = pose[oa + 7];
@@ -505,30 +567,31 @@ static __device__ bool cap_box_segment(const DevPlant& p, const float4* stat, co
 
 // Remaining pairs (the moving geometry first; moving-moving pairs ordered
 // sphere < capsule < box), dispatched once per segment.
-static __device__ bool sweep_generic(const DevPlant& p, const float4* stat, const float* pose, int lane) {
+static __device__ bool sweep_generic(const DevPlant& p, const float4* stat, const float* pose, int lane,
+                                     const Cull& cu) {
   for (int sgi = 0; sgi < p.num_segs; ++sgi) {
     const GenSeg sg = p.segs[sgi];
     const int key = sg.b_static * 16 + sg.ta * 4 + sg.tb;
     bool h = false;
     switch (key) {
       // moving-moving
-      case G_SPHERE * 4 + G_CAPSULE: h = generic_segment<G_SPHERE, G_CAPSULE, false>(p, stat, pose, sg, lane); break;
-      case G_SPHERE * 4 + G_BOX: h = generic_segment<G_SPHERE, G_BOX, false>(p, stat, pose, sg, lane); break;
-      case G_CAPSULE * 4 + G_CAPSULE: h = generic_segment<G_CAPSULE, G_CAPSULE, false>(p, stat, pose, sg, lane); break;
-      case G_CAPSULE * 4 + G_BOX: h = cap_box_segment<false>(p, stat, pose, sg, lane); break;
-      case G_BOX * 4 + G_BOX: h = generic_segment<G_BOX, G_BOX, false>(p, stat, pose, sg, lane); break;
-      case G_BOX * 4 + G_SPHERE: h = generic_segment<G_BOX, G_SPHERE, false>(p, stat, pose, sg, lane); break;
-      case G_BOX * 4 + G_CAPSULE: h = generic_segment<G_BOX, G_CAPSULE, false>(p, stat, pose, sg, lane); break;
-      case G_CAPSULE * 4 + G_SPHERE: h = generic_segment<G_CAPSULE, G_SPHERE, false>(p, stat, pose, sg, lane); break;
-      case G_SPHERE * 4 + G_SPHERE: h = generic_segment<G_SPHERE, G_SPHERE, false>(p, stat, pose, sg, lane); break;
+      case G_SPHERE * 4 + G_CAPSULE: h = generic_segment<G_SPHERE, G_CAPSULE, false>(p, stat, pose, sg, lane, cu); break;
+      case G_SPHERE * 4 + G_BOX: h = generic_segment<G_SPHERE, G_BOX, false>(p, stat, pose, sg, lane, cu); break;
+      case G_CAPSULE * 4 + G_CAPSULE: h = generic_segment<G_CAPSULE, G_CAPSULE, false>(p, stat, pose, sg, lane, cu); break;
+      case G_CAPSULE * 4 + G_BOX: h = cap_box_segment<false>(p, stat, pose, sg, lane, cu); break;
+      case G_BOX * 4 + G_BOX: h = generic_segment<G_BOX, G_BOX, false>(p, stat, pose, sg, lane, cu); break;
+      case G_BOX * 4 + G_SPHERE: h = generic_segment<G_BOX, G_SPHERE, false>(p, stat, pose, sg, lane, cu); break;
+      case G_BOX * 4 + G_CAPSULE: h = generic_segment<G_BOX, G_CAPSULE, false>(p, stat, pose, sg, lane, cu); break;
+      case G_CAPSULE * 4 + G_SPHERE: h = generic_segment<G_CAPSULE, G_SPHERE, false>(p, stat, pose, sg, lane, cu); break;
+      case G_SPHERE * 4 + G_SPHERE: h = generic_segment<G_SPHERE, G_SPHERE, false>(p, stat, pose, sg, lane, cu); break;
       // moving-static
-      case 16 + G_CAPSULE * 4 + G_SPHERE: h = generic_segment<G_CAPSULE, G_SPHERE, true>(p, stat, pose, sg, lane); break;
-      case 16 + G_CAPSULE * 4 + G_BOX: h = cap_box_segment<true>(p, stat, pose, sg, lane); break;
-      case 16 + G_CAPSULE * 4 + G_CAPSULE: h = generic_segment<G_CAPSULE, G_CAPSULE, true>(p, stat, pose, sg, lane); break;
-      case 16 + G_BOX * 4 + G_SPHERE: h = generic_segment<G_BOX, G_SPHERE, true>(p, stat, pose, sg, lane); break;
-      case 16 + G_BOX * 4 + G_BOX: h = generic_segment<G_BOX, G_BOX, true>(p, stat, pose, sg, lane); break;
-      case 16 + G_BOX * 4 + G_CAPSULE: h = generic_segment<G_BOX, G_CAPSULE, true>(p, stat, pose, sg, lane); break;
-      default: h = generic_segment<G_SPHERE, G_SPHERE, true>(p, stat, pose, sg, lane); break;
+      case 16 + G_CAPSULE * 4 + G_SPHERE: h = generic_segment<G_CAPSULE, G_SPHERE, true>(p, stat, pose, sg, lane, cu); break;
+      case 16 + G_CAPSULE * 4 + G_BOX: h = cap_box_segment<true>(p, stat, pose, sg, lane, cu); break;
+      case 16 + G_CAPSULE * 4 + G_CAPSULE: h = generic_segment<G_CAPSULE, G_CAPSULE, true>(p, stat, pose, sg, lane, cu); break;
+      case 16 + G_BOX * 4 + G_SPHERE: h = generic_segment<G_BOX, G_SPHERE, true>(p, stat, pose, sg, lane, cu); break;
+      case 16 + G_BOX * 4 + G_BOX: h = generic_segment<G_BOX, G_BOX, true>(p, stat, pose, sg, lane, cu); break;
+      case 16 + G_BOX * 4 + G_CAPSULE: h = generic_segment<G_BOX, G_CAPSULE, true>(p, stat, pose, sg, lane, cu); break;
+      default: h = generic_segment<G_SPHERE, G_SPHERE, true>(p, stat, pose, sg, lane, cu); break;
     }
     if (h) return true;
   }
@@ -586,20 +649,21 @@ static __device__ bool check_config(const DevPlant& p, const float4* stat, const
   place_all(p, X, pose, lane);
   __syncwarp();
   if (p.always_colliding) return true;
+  const Cull cu = broad_phase(p, aabb, X, lane);
   const bool dense = p.dense_spheres && p.num_tiles >= 1 && p.num_tiles <= 4;
   if (dense) {
     bool h;
     switch (p.num_tiles) {
-      case 1: h = sweep_dense_spheres<1>(p, stat, aabb, pose, lane); break;
-      case 2: h = sweep_dense_spheres<2>(p, stat, aabb, pose, lane); break;
-      case 3: h = sweep_dense_spheres<3>(p, stat, aabb, pose, lane); break;
-      default: h = sweep_dense_spheres<4>(p, stat, aabb, pose, lane); break;
+      case 1: h = sweep_dense_spheres<1>(p, stat, aabb, pose, lane, cu); break;
+      case 2: h = sweep_dense_spheres<2>(p, stat, aabb, pose, lane, cu); break;
+      case 3: h = sweep_dense_spheres<3>(p, stat, aabb, pose, lane, cu); break;
+      default: h = sweep_dense_spheres<4>(p, stat, aabb, pose, lane, cu); break;
     }
     if (h) return true;
   }
   for (int t = 0; t < p.num_tiles; ++t)
-    if (sweep_tile(p, stat, aabb, pose, t, lane, dense)) return true;
-  if (sweep_generic(p, stat, pose, lane)) return true;
+    if (sweep_tile(p, stat, aabb, pose, t, lane, dense, cu)) return true;
+  if (sweep_generic(p, stat, pose, lane, cu)) return true;
   if (va.nv > 0 && sweep_voxels(p, stat, pose, va, lane)) return true;
   return false;
 }

@@ -98,11 +98,14 @@ struct DevPlant {
   int num_links;         // all links of the reference tree (FK output)
   int static_bytes;      // bytes of statics + aabb staged in shared memory (multiple of 16)
   int dense_spheres;     // every tile pairs every lane with every static sphere and aligned box
-  int pad_dense;
+  int cull;              // link-level broad phase on (slot and static bounding spheres)
   const FkJoint* fk;
   const MovingGeom* moving;
   const float4* statics;       // [num_static][4] float4 (WG format); followed by aabb
-  const float4* aabb;          // [num_sabox][2]: [p 0 | h 0] of axis-aligned static boxes
+  const float4* aabb;          // [num_sabox][2]: [p 0 | h 0] of axis-aligned static boxes; followed by
+                               // [num_static] static bounding spheres (world centre, radius)
+  const float4* slot_bs;       // [num_slots] bounding sphere of each slot's geometry (slot frame); radius < 0: none
+  const uint8_t* moving_slot;  // [num_moving] slot of each moving geometry
   const int* static_type;      // [num_static]
   const TileInfo* tiles;
   const TileEntry* entries;

@@ -83,6 +83,7 @@ struct csd_plant_s {
   csd::DevPlant dp{};
   csd::HostPlant host;
   void* blob = nullptr;  // device tables
+  bool cull_eligible = false;  // <= 32 slots and <= 1024 statics
   // scratch for host-pointer calls and per-call voxel tables
   csd::DevBuf in_buf, in_buf2, out_buf, out_buf2, vox_buf, vox_tab, counter;
   ~csd_plant_s();

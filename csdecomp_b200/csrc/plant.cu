@@ -8,6 +8,7 @@
 // world-fixed geometry is posed once, and the pair list is split into
 // moving-sphere x static tiles (lane masks) and a generic remainder.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -433,8 +434,16 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   auto seg_key = [&](const GenericPair& x) {
     return ((x.b >> 31) * 16 + type_of_ref(x.a) * 4 + type_of_ref(x.b));
   };
-  std::stable_sort(generic.begin(), generic.end(),
-                   [&](const GenericPair& x, const GenericPair& y) { return seg_key(x) < seg_key(y); });
+  // by segment, then by the moving geometry's slot and the partner (so that
+  // consecutive pairs mostly share a link pair for the broad phase)
+  auto slot_of_ref = [&](uint32_t r) { return (r & 0x80000000u) ? -1 : hp.moving[r].slot; };
+  std::stable_sort(generic.begin(), generic.end(), [&](const GenericPair& x, const GenericPair& y) {
+    const uint32_t kx = seg_key(x), ky = seg_key(y);
+    if (kx != ky) return kx < ky;
+    const int ax = slot_of_ref(x.a), ay = slot_of_ref(y.a);
+    if (ax != ay) return ax < ay;
+    return slot_of_ref(x.b) < slot_of_ref(y.b);
+  });
   std::vector<GenSeg> segs;
   for (size_t i = 0; i < generic.size();) {
     size_t j = i;
@@ -499,6 +508,73 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
     }
   }
 
+  // ---- broad-phase tables. Bounding spheres (FP64, then padded by a relative
+  // 1e-6 and 1e-4 m so that FP32 evaluation never culls a pair closer than
+  // that): per slot over its geometries in the slot frame, per static in the
+  // world.
+  const int NSL = (int)fk.size();
+  std::vector<float> slot_bs((size_t)std::max(NSL, 1) * 4, 0.f);
+  {
+    std::vector<std::vector<std::array<double, 4>>> pts(std::max(NSL, 1));
+    for (const MovingGeom& g : hp.moving) {
+      auto add = [&](double x, double y, double z, double r) { pts[g.slot].push_back({x, y, z, r}); };
+      if (g.type == G_SPHERE) {
+        add(g.p[0], g.p[1], g.p[2], g.r);
+      } else if (g.type == G_CAPSULE) {
+        for (int sg = -1; sg <= 1; sg += 2)
+          add(g.p[0] + sg * g.hl * g.z[0], g.p[1] + sg * g.hl * g.z[1], g.p[2] + sg * g.hl * g.z[2], g.r);
+      } else {
+        for (int c = 0; c < 8; ++c) {
+          double v[3] = {g.p[0], g.p[1], g.p[2]};
+          for (int a = 0; a < 3; ++a) {
+            const double e = ((c >> a) & 1 ? 1.0 : -1.0) * g.h[a];
+            for (int r = 0; r < 3; ++r) v[r] += g.R[3 * a + r] * e;
+          }
+          add(v[0], v[1], v[2], 0.0);
+        }
+      }
+    }
+    for (int k = 0; k < NSL; ++k) {
+      if (pts[k].empty()) {
+        slot_bs[4 * k + 3] = -1.f;
+        continue;
+      }
+      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+      for (auto& q : pts[k])
+        for (int a = 0; a < 3; ++a) {
+          lo[a] = std::min(lo[a], q[a] - q[3]);
+          hi[a] = std::max(hi[a], q[a] + q[3]);
+        }
+      double c[3], rad = 0;
+      for (int a = 0; a < 3; ++a) c[a] = 0.5 * (lo[a] + hi[a]);
+      for (auto& q : pts[k])
+        rad = std::max(rad, std::sqrt((q[0] - c[0]) * (q[0] - c[0]) + (q[1] - c[1]) * (q[1] - c[1]) +
+                                      (q[2] - c[2]) * (q[2] - c[2])) + q[3]);
+      for (int a = 0; a < 3; ++a) slot_bs[4 * k + a] = (float)c[a];
+      slot_bs[4 * k + 3] = (float)(rad * (1 + 1e-6) + 1e-4);
+    }
+  }
+  std::vector<float> static_bs((size_t)S * 4, 0.f);
+  for (int st = 0; st < S; ++st) {
+    const float* W = hp.statics.data() + 16 * st;
+    double c[3] = {W[0], W[1], W[2]}, rad;
+    const int ty = hp.static_type[st];
+    if (ty == G_SPHERE) {
+      rad = W[3];
+    } else if (ty == G_CAPSULE) {
+      rad = (double)W[3] + W[7];
+    } else {  // box rows [axis_i | -axis_i . centre]: centre = sum_i (axis_i . centre) axis_i
+      for (int r = 0; r < 3; ++r) c[r] = 0;
+      for (int a = 0; a < 3; ++a)
+        for (int r = 0; r < 3; ++r) c[r] += -(double)W[4 * a + 3] * W[4 * a + r];
+      rad = std::sqrt((double)W[12] * W[12] + (double)W[13] * W[13] + (double)W[14] * W[14]);
+    }
+    for (int a = 0; a < 3; ++a) static_bs[4 * st + a] = (float)c[a];
+    static_bs[4 * st + 3] = (float)(rad * (1 + 1e-6) + 1e-4);
+  }
+  std::vector<uint8_t> moving_slot(std::max<size_t>(hp.moving.size(), 1), 0);
+  for (size_t m = 0; m < hp.moving.size(); ++m) moving_slot[m] = (uint8_t)hp.moving[m].slot;
+
   // ---- FK output tables
   std::vector<int> link_slot(L);
   std::vector<float> link_fixed((size_t)L * 12, 0.f);
@@ -517,7 +593,8 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   };
   size_t o_fk = section(fk.size() * sizeof(FkJoint));
   size_t o_mv = section(hp.moving.size() * sizeof(MovingGeom));
-  const size_t static_bytes = hp.statics.size() * sizeof(float) + aabb.size() * sizeof(float);
+  const size_t static_bytes =
+      hp.statics.size() * sizeof(float) + aabb.size() * sizeof(float) + static_bs.size() * sizeof(float);
   size_t o_st = section(static_bytes);
   size_t o_sty = section(hp.static_type.size() * sizeof(int));
   size_t o_ti = section(tiles.size() * sizeof(TileInfo));
@@ -527,6 +604,8 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   size_t o_status = section(16);
   size_t o_ls = section(link_slot.size() * sizeof(int));
   size_t o_lf = section(link_fixed.size() * sizeof(float));
+  size_t o_sbs = section(slot_bs.size() * sizeof(float));
+  size_t o_msl = section(moving_slot.size());
   std::vector<char> host_blob(off, 0);
   auto put = [&](size_t o, const void* src, size_t n) {
     if (n) std::memcpy(host_blob.data() + o, src, n);
@@ -535,6 +614,9 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   put(o_mv, hp.moving.data(), hp.moving.size() * sizeof(MovingGeom));
   put(o_st, hp.statics.data(), hp.statics.size() * sizeof(float));
   put(o_st + hp.statics.size() * sizeof(float), aabb.data(), aabb.size() * sizeof(float));
+  put(o_st + (hp.statics.size() + aabb.size()) * sizeof(float), static_bs.data(), static_bs.size() * sizeof(float));
+  put(o_sbs, slot_bs.data(), slot_bs.size() * sizeof(float));
+  put(o_msl, moving_slot.data(), moving_slot.size());
   put(o_sty, hp.static_type.data(), hp.static_type.size() * sizeof(int));
   put(o_ti, tiles.data(), tiles.size() * sizeof(TileInfo));
   put(o_en, entries.data(), entries.size() * sizeof(TileEntry));
@@ -569,6 +651,10 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
     dp.dense_spheres = dense;
   }
   dp.num_links = L;
+  dp.cull = NSL >= 1 && NSL <= 32 && S <= 32 * 32;
+  h->cull_eligible = dp.cull != 0;
+  dp.slot_bs = (const float4*)(base + o_sbs);
+  dp.moving_slot = (const uint8_t*)(base + o_msl);
   dp.fk = (const FkJoint*)(base + o_fk);
   dp.moving = (const MovingGeom*)(base + o_mv);
   dp.statics = (const float4*)(base + o_st);
@@ -592,6 +678,12 @@ csd_status_t csd_plant_destroy(csd_plant_t p) {
   if (cur != dev) cudaSetDevice(dev);
   delete p;
   if (cur != dev) cudaSetDevice(cur);
+  return CSD_OK;
+}
+
+csd_status_t csd_plant_set_culling(csd_plant_t p, int32_t enable) {
+  CSD_CHECK(p, CSD_ERR_INVALID, "null plant");
+  p->dp.cull = (enable && p->cull_eligible) ? 1 : 0;
   return CSD_OK;
 }
 

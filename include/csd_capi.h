@@ -296,6 +296,16 @@ uint32_t csd_num_samples_unadaptive(float epsilon, float delta, float tau);
 /* Diagnostics (no counterpart in the reference): FP32 FMA throughput of the
  * current device, the denominator of the collision kernels' roofline. */
 csd_status_t csd_fp32_fma_probe(int64_t iters, double* flops, double* seconds);
+/* Link-level broad phase of the collision checks (no counterpart in the
+ * reference, which tests every pair): per configuration, each moving link's
+ * bounding sphere is placed in the world and pairs whose link or static
+ * bounding spheres are apart by more than 1e-4 m are skipped. Verdicts are
+ * unchanged. On by default for plants with at most 32 moving links and 1024
+ * static geometries; enable = 0 evaluates every pair (the full sweep that
+ * csd_plant_flops counts). Takes effect for later calls and for batches
+ * created afterwards. */
+csd_status_t csd_plant_set_culling(csd_plant_t plant, int32_t enable);
+
 /* Algorithmic FP32 work of checking one configuration of this plant without
  * early exit: forward kinematics, geometry placement and all pair tests
  * (FMA = 2 FLOP; sqrt, division and sincos not counted). */
