@@ -202,6 +202,7 @@ def roofline_point_check(csd, scene, torch, dev):
     fl = h.flops()
     q = scene.random_configs(200000, 77)
     free = q[csd.CheckCollisionFreeCuda(q.T, scene.plant) == 1]
+    h.set_culling(False)  # the full sweep that the FLOP count describes
     n = 1 << 20
     reps = int(np.ceil(n / len(free)))
     qf = np.ascontiguousarray(np.tile(free, (reps, 1))[:n])
@@ -226,6 +227,16 @@ def roofline_point_check(csd, scene, torch, dev):
         e1.synchronize()
         times.append(e0.elapsed_time(e1) * 1e-3)
     assert int(out.sum().item()) == n, "roofline configurations must all be free"
+    culled = []
+    h.set_culling(True)
+    for _ in range(3):
+        flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        launch()
+        e1.record(st)
+        e1.synchronize()
+        culled.append(e0.elapsed_time(e1) * 1e-3)
     t = float(np.mean(times))
     flops = fl["total"] * n
     fma_flops, fma_s = ctypes.c_double(), ctypes.c_double()
@@ -234,7 +245,9 @@ def roofline_point_check(csd, scene, torch, dev):
     achieved = flops / t
     return {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
             "frac": achieved / peak, "traffic": None,
-            "kernel": "check_points_kernel (fused FK + pair sweep; the batched check stage runs the same device code)",
+            "kernel": "check_points_kernel (fused FK + pair sweep; the batched check stage runs the same device code), "
+                      "link-level broad phase off",
+            "launch_ms_with_broad_phase": float(np.mean(culled)) * 1e3,
             "per_config_flop": fl, "configs_per_launch": n, "launch_ms": t * 1e3,
             "peak_source": "measured FP32 FMA probe (csd_fp32_fma_probe) in this run",
             "workload": "1,048,576 collision-free configurations of the 7-DOF arm (80 spheres + 4 capsules) in "
@@ -344,6 +357,24 @@ def main():
     torch.cuda.nvtx.range_pop()
     tuned_surr = surrogate_batch.tuning()
     first_regions = rb["first"]
+    # roofline of the dominant kernel (the sampler): one profiled pass of the first timed step
+    batched.set_profiling(True)
+    q0s, q1s = step_inputs(args.warmup)
+    batched.inflate(slot_plant, q0s, q1s, doms)
+    stages = batched.stage_ms()
+    s_ms = stages["sample"]
+    s_flop = batched.sample_flops()
+    batched.set_profiling(False)
+    sampler_roofline = {"bound": "fp32", "achieved": s_flop / (s_ms * 1e-3) / 1e12, "peak": None, "unit": "TFLOP/s",
+                        "frac": None, "traffic": None,
+                        "kernel": "batch_sample_kernel (hit-and-run, G lanes per chain, faces staged in shared memory; "
+                                  "autotuned variant " + tuned_plain["sample_variant"] + ")",
+                        "flop_per_unit": "4 d F per chain and mixing step (two length-d dot products per face, "
+                                         "FMA = 2), summed over the slots and iterations of the step",
+                        "flop_per_step": s_flop, "kernel_ms_per_step": s_ms,
+                        "share_of_step": s_ms / sum(stages.values()), "stage_ms": stages,
+                        "timing": "CUDA events around every sampler launch of one profiled pass over the first timed "
+                                  "step (stages launched one by one, same inputs and shapes as the graph)"}
     # plain GPU form (one CudaEdgeInflator call per region) on the first timed step's inputs
     plain_s, identical = 0.0, True
     st = torch.cuda.current_stream()
@@ -411,7 +442,11 @@ def main():
                                 "in, host polytopes out"},
                 "gpu_launches": rs["launches"],
                 "clocks": clk.summary()}
-        line["roofline"] = roofline_point_check(csd, scenes.edge_check_scene(keepout=0.8), torch, dev)
+        line["roofline_checker"] = roofline_point_check(csd, scenes.edge_check_scene(keepout=0.8), torch, dev)
+        sampler_roofline["peak"] = line["roofline_checker"]["peak"]
+        sampler_roofline["frac"] = sampler_roofline["achieved"] / sampler_roofline["peak"]
+        sampler_roofline["peak_source"] = line["roofline_checker"]["peak_source"]
+        line["roofline"] = sampler_roofline
         if world == 1:
             sample = [(sc, e[args.warmup]) for sc, e in items[:8]]
             rate, n, dt = cpu_eizo(sample, os.cpu_count() or 1, 20.0)

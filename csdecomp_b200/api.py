@@ -446,7 +446,7 @@ class BatchedEdgeInflator:
     CudaEdgeInflator.inflateEdge would for the same inputs (no voxels)."""
 
     SAMPLE_VARIANTS = ("1 face/trip, 2 blocks/SM", "2 faces/trip, 2 blocks/SM", "1 face/trip, 3 blocks/SM",
-                       "2 faces/trip, 3 blocks/SM")
+                       "2 faces/trip, 3 blocks/SM", "4 faces/trip, 2 blocks/SM", "4 faces/trip, 3 blocks/SM")
     CHECK_ITEM_CAPS = (32, 128, 512)
 
     def __init__(self, plants: Sequence[MinimalPlant], options: EizoOptions, max_slots: int,
@@ -550,6 +550,12 @@ class BatchedEdgeInflator:
         C.check(C.lib().csd_batch_iteration_profile(self._handle, cnt.value, C.ptr(ms), C.ptr(act),
                                                     ctypes.byref(cnt)))
         return ms, act
+
+    def sample_flops(self) -> float:
+        """Sampler FLOPs of the last inflate in profiling mode (4 d F per chain step)."""
+        v = ctypes.c_double(0)
+        C.check(C.lib().csd_batch_sample_flops(self._handle, ctypes.byref(v)))
+        return v.value
 
     def stage_ms(self) -> dict:
         ms = np.zeros(len(self.STAGES), np.float32)

@@ -120,7 +120,7 @@ static __device__ __forceinline__ int item_size(int64_t total, int cap, int nw) 
 // chain count: 8 when the batch is full, up to 32 in the tail).
 template <int U, int MINB>
 __global__ void __launch_bounds__(256, MINB) batch_sample_kernel(BatchArgs a) {
-  extern __shared__ float smf[];
+  extern __shared__ __align__(16) float smf[];  // the face loop reads float2/float4 vectors
   const int N = a.n_tab[a.it->k];
   const int64_t total = (int64_t)a.it->num_act * N;
   const int G = group_width(total, (int64_t)gridDim.x * (blockDim.x >> 5));
@@ -585,6 +585,8 @@ static const SampleVariant kSampleVariants[] = {
     {batch_sample_kernel<2, 2>, 2, 2},
     {batch_sample_kernel<1, 3>, 1, 3},
     {batch_sample_kernel<2, 3>, 2, 3},
+    {batch_sample_kernel<4, 2>, 4, 2},
+    {batch_sample_kernel<4, 3>, 4, 3},
 };
 constexpr int kNumSampleVariants = (int)(sizeof(kSampleVariants) / sizeof(kSampleVariants[0]));
 // Largest check work item (configurations) the autotuner chooses from.
@@ -631,6 +633,7 @@ struct csd_batch_s {
   double stage_ms[csd::kStages] = {};
   std::vector<float> iter_ms;   // profiling mode: [iteration][kStages] of the last inflate
   std::vector<int> iter_active; // slots active at the start of each iteration
+  double sample_flop = 0.0;     // profiling mode: sampler FLOPs of the last inflate (4 d F per chain step)
   ~csd_batch_s() {
     for (cudaEvent_t e : ev)
       if (e) cudaEventDestroy(e);
@@ -961,6 +964,9 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
   }
   h->iter_ms.clear();
   h->iter_active.clear();
+  h->sample_flop = 0.0;
+  std::vector<SlotState> prof_slots;
+  if (h->profile) prof_slots = slots;  // the records as uploaded: faces of the domain
   int active_now = n;
   for (uint32_t k = 0; k < h->opt.max_iterations; ++k) {
     if (h->tune_iters > 0) {
@@ -1020,6 +1026,12 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
         h->iter_ms.push_back(ms);
       }
       h->iter_active.push_back(active_now);
+      // sampler work of this iteration, from the records before it ran
+      for (const SlotState& S : prof_slots)
+        if (!S.done)
+          h->sample_flop += (double)h->n_tab[k] * h->opt.mixing_steps * 4.0 * S.dim * S.nf;
+      CSD_CUDA_TRY(cudaMemcpyAsync(prof_slots.data(), h->slots_dev.ptr, n * sizeof(SlotState),
+                                   cudaMemcpyDeviceToHost, st));
     } else {
       CSD_CUDA_TRY(cudaGraphLaunch(h->graph, st));
     }
@@ -1135,7 +1147,7 @@ csd_status_t csd_batch_set_surrogate_rounds(csd_batch_t h, int32_t rounds, int32
 csd_status_t csd_batch_set_shapes(csd_batch_t h, int32_t sample_variant, int32_t check_item_cap) {
   CSD_CHECK(h && sample_variant >= 0 && sample_variant < kNumSampleVariants && check_item_cap >= 8 &&
                 check_item_cap % 8 == 0,
-            CSD_ERR_INVALID, "bad shapes: sampler variant in [0, 4), check item cap a positive multiple of 8");
+            CSD_ERR_INVALID, "bad shapes: sampler variant in [0, 6), check item cap a positive multiple of 8");
   h->sample_variant = sample_variant;
   h->cfg_max = check_item_cap;
   return CSD_OK;
@@ -1149,6 +1161,12 @@ csd_status_t csd_batch_tuning(csd_batch_t h, int32_t* sample_variant, int32_t* c
   if (num_variants) *num_variants = kNumSampleVariants + kNumCheckVariants;
   if (variant_ms)
     for (int q = 0; q < kNumSampleVariants + kNumCheckVariants; ++q) variant_ms[q] = (float)h->tune_ms[q];
+  return CSD_OK;
+}
+
+csd_status_t csd_batch_sample_flops(csd_batch_t h, double* flops) {
+  CSD_CHECK(h && flops, CSD_ERR_INVALID, "null argument");
+  *flops = h->sample_flop;
   return CSD_OK;
 }
 

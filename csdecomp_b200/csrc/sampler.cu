@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(256) hit_and_run_group_kernel(const float* __r
                                                                 const float* __restrict__ start, int S, int mixing,
                                                                 uint32_t k0, uint32_t k1, uint32_t stream,
                                                                 float* __restrict__ out) {
-  extern __shared__ float smf[];
+  extern __shared__ __align__(16) float smf[];  // the face loop reads float2/float4 vectors
   const int F = *num_faces_dev;
   const int G = group_width(S, (int64_t)gridDim.x * (blockDim.x >> 5));
   const int per = (S + gridDim.x - 1) / gridDim.x;

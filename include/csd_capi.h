@@ -233,11 +233,11 @@ csd_status_t csd_batch_set_profiling(csd_batch_t h, int32_t enable);
 csd_status_t csd_batch_stage_ms(csd_batch_t h, float* stage_ms /* [8] */);
 /* Autotuner: during the first `iterations` iterations of the next
  * csd_batch_inflate, every sampler variant (faces per lane and trip x
- * resident blocks per SM: [1x2, 2x2, 1x3, 2x3]) and every check work-item
+ * resident blocks per SM: [1x2, 2x2, 1x3, 2x3, 4x2, 4x3]) and every check work-item
  * cap ([32, 128, 512] configurations) is timed on that iteration's own
  * inputs; the fastest of each is kept for the graph and later calls.
  * csd_batch_tuning reports the choice and the summed time of each variant
- * (variant_ms: 4 sampler entries, then 3 check entries). */
+ * (variant_ms: 6 sampler entries, then 3 check entries). */
 csd_status_t csd_batch_autotune(csd_batch_t h, int32_t iterations);
 /* Surrogate-guided checking (mlp: one net per plant of the batch, same
  * dimensions; NULL turns it off). Each iteration then scores every sample
@@ -264,6 +264,10 @@ csd_status_t csd_batch_tuning(csd_batch_t h, int32_t* sample_variant, int32_t* c
  * receives the number of iterations (at most cap are written). */
 csd_status_t csd_batch_iteration_profile(csd_batch_t h, int32_t cap, float* stage_ms, int32_t* active,
                                          int32_t* count);
+/* Profiling mode, last csd_batch_inflate: algorithmic FLOPs of the sampling
+ * stage, 4 d F per chain and mixing step (two length-d dot products per face,
+ * FMA = 2), summed over the active slots' N_k chains of every iteration. */
+csd_status_t csd_batch_sample_flops(csd_batch_t h, double* flops);
 
 csd_status_t csd_batch_destroy(csd_batch_t batch);
 
