@@ -205,14 +205,18 @@ static __device__ __forceinline__ void own_sphere(const DevPlant& p, const float
 struct Cull {
   uint32_t link;
   uint32_t stat;
+  const uint8_t* msl;  // slot of each moving geometry (staged copy)
 };
 
 static __device__ __forceinline__ Cull broad_phase(const DevPlant& p, const float4* aabb, const float* X, int lane) {
-  Cull c{~0u, ~0u};
+  // the staged region continues after the aligned boxes: static spheres, slot spheres, geometry slots
+  const float4* sbs = aabb + 2 * p.num_sabox;
+  const float4* slb = sbs + p.num_static;
+  Cull c{~0u, ~0u, reinterpret_cast<const uint8_t*>(slb + p.num_slots)};
   if (!p.cull) return c;
   float cx = 0.f, cy = 0.f, cz = 0.f, cr = -1.f;
   if (lane < p.num_slots) {
-    const float4 b = __ldg(p.slot_bs + lane);
+    const float4 b = slb[lane];
     const float* x = X + lane * 12;
     cx = fmaf(x[6], b.z, fmaf(x[3], b.y, fmaf(x[0], b.x, x[9])));
     cy = fmaf(x[7], b.z, fmaf(x[4], b.y, fmaf(x[1], b.x, x[10])));
@@ -227,7 +231,6 @@ static __device__ __forceinline__ Cull broad_phase(const DevPlant& p, const floa
     if (cr >= 0.f && orr >= 0.f && fmaf(dz, dz, fmaf(dy, dy, dx * dx)) <= t * t) lw |= 1u << j;
   }
   c.link = lw;
-  const float4* sbs = aabb + 2 * p.num_sabox;
   uint32_t sw = 0;
   for (int g = 0; g * kWarp < p.num_static; ++g) {
     const int st = g * kWarp + lane;
@@ -448,7 +451,7 @@ struct Words {
 template <bool BSTATIC>
 static __device__ __forceinline__ bool pair_near(const DevPlant& p, const Cull& cu, const GenericPair& gp, bool valid) {
   if (BSTATIC) return static_near(cu, valid ? (int)(gp.b & 0x7fffffffu) : 0) && valid;
-  const int sa = valid ? (int)__ldg(p.moving_slot + gp.a) : 0, sb = valid ? (int)__ldg(p.moving_slot + gp.b) : 0;
+  const int sa = valid ? (int)cu.msl[gp.a] : 0, sb = valid ? (int)cu.msl[gp.b] : 0;
   return ((__shfl_sync(kFull, cu.link, sa & 31) >> (sb & 31)) & 1u) && valid;
 }
 

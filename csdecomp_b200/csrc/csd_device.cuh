@@ -103,7 +103,8 @@ struct DevPlant {
   const MovingGeom* moving;
   const float4* statics;       // [num_static][4] float4 (WG format); followed by aabb
   const float4* aabb;          // [num_sabox][2]: [p 0 | h 0] of axis-aligned static boxes; followed by
-                               // [num_static] static bounding spheres (world centre, radius)
+                               // [num_static] static bounding spheres (world centre, radius), then the
+                               // slot spheres and the geometry slots below (one staged region)
   const float4* slot_bs;       // [num_slots] bounding sphere of each slot's geometry (slot frame); radius < 0: none
   const uint8_t* moving_slot;  // [num_moving] slot of each moving geometry
   const int* static_type;      // [num_static]

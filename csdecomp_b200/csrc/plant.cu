@@ -513,7 +513,7 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   // that): per slot over its geometries in the slot frame, per static in the
   // world.
   const int NSL = (int)fk.size();
-  std::vector<float> slot_bs((size_t)std::max(NSL, 1) * 4, 0.f);
+  std::vector<float> slot_bs((size_t)NSL * 4, 0.f);
   {
     std::vector<std::vector<std::array<double, 4>>> pts(std::max(NSL, 1));
     for (const MovingGeom& g : hp.moving) {
@@ -593,8 +593,10 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   };
   size_t o_fk = section(fk.size() * sizeof(FkJoint));
   size_t o_mv = section(hp.moving.size() * sizeof(MovingGeom));
-  const size_t static_bytes =
-      hp.statics.size() * sizeof(float) + aabb.size() * sizeof(float) + static_bs.size() * sizeof(float);
+  // staged region: statics | aligned boxes | static spheres | slot spheres | geometry slots (16-byte padded)
+  const size_t ms_bytes = (moving_slot.size() + 15) & ~size_t(15);
+  const size_t static_bytes = hp.statics.size() * sizeof(float) + aabb.size() * sizeof(float) +
+                              static_bs.size() * sizeof(float) + slot_bs.size() * sizeof(float) + ms_bytes;
   size_t o_st = section(static_bytes);
   size_t o_sty = section(hp.static_type.size() * sizeof(int));
   size_t o_ti = section(tiles.size() * sizeof(TileInfo));
@@ -604,8 +606,6 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   size_t o_status = section(16);
   size_t o_ls = section(link_slot.size() * sizeof(int));
   size_t o_lf = section(link_fixed.size() * sizeof(float));
-  size_t o_sbs = section(slot_bs.size() * sizeof(float));
-  size_t o_msl = section(moving_slot.size());
   std::vector<char> host_blob(off, 0);
   auto put = [&](size_t o, const void* src, size_t n) {
     if (n) std::memcpy(host_blob.data() + o, src, n);
@@ -614,8 +614,11 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   put(o_mv, hp.moving.data(), hp.moving.size() * sizeof(MovingGeom));
   put(o_st, hp.statics.data(), hp.statics.size() * sizeof(float));
   put(o_st + hp.statics.size() * sizeof(float), aabb.data(), aabb.size() * sizeof(float));
-  put(o_st + (hp.statics.size() + aabb.size()) * sizeof(float), static_bs.data(), static_bs.size() * sizeof(float));
-  put(o_sbs, slot_bs.data(), slot_bs.size() * sizeof(float));
+  const size_t o_sph = o_st + (hp.statics.size() + aabb.size()) * sizeof(float);
+  const size_t o_slb = o_sph + static_bs.size() * sizeof(float);
+  const size_t o_msl = o_slb + slot_bs.size() * sizeof(float);
+  put(o_sph, static_bs.data(), static_bs.size() * sizeof(float));
+  put(o_slb, slot_bs.data(), slot_bs.size() * sizeof(float));
   put(o_msl, moving_slot.data(), moving_slot.size());
   put(o_sty, hp.static_type.data(), hp.static_type.size() * sizeof(int));
   put(o_ti, tiles.data(), tiles.size() * sizeof(TileInfo));
@@ -653,7 +656,7 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   dp.num_links = L;
   dp.cull = NSL >= 1 && NSL <= 32 && S <= 32 * 32;
   h->cull_eligible = dp.cull != 0;
-  dp.slot_bs = (const float4*)(base + o_sbs);
+  dp.slot_bs = (const float4*)(base + o_slb);
   dp.moving_slot = (const uint8_t*)(base + o_msl);
   dp.fk = (const FkJoint*)(base + o_fk);
   dp.moving = (const MovingGeom*)(base + o_mv);

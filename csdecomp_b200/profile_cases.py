@@ -1,9 +1,9 @@
 """Small, reproducible launches of the hot kernels for profiler captures.
 
-  python -m csdecomp_b200.profile_cases check_points [--configs N]
+  python -m csdecomp_b200.profile_cases check_points [--configs N] [--no-cull]
       one warm-up and one timed check_points launch on N collision-free
       configurations of the 7-DOF arm (80 spheres + 4 capsules) in 200 world
-      primitives (every pair evaluated: the full sweep)
+      primitives (with --no-cull every pair is evaluated: the full sweep)
   python -m csdecomp_b200.profile_cases batch [--slots S] [--iterations I]
       [--sample-variant V] [--check-item-cap C]
       S inflations of the batched EI-ZO workload (first S scenes), at most I
@@ -31,7 +31,7 @@ import json
 import numpy as np
 
 
-def check_points(n: int) -> None:
+def check_points(n: int, cull: bool = True) -> None:
     import torch
     import csdecomp_b200 as csd
     from csdecomp_b200 import _capi as C
@@ -40,6 +40,7 @@ def check_points(n: int) -> None:
     h = csd.plant_handle(sc.plant)
     q = sc.random_configs(200000, 77)
     free = q[csd.CheckCollisionFreeCuda(q.T, sc.plant) == 1]
+    h.set_culling(cull)
     qf = np.ascontiguousarray(np.tile(free, (int(np.ceil(n / len(free))), 1))[:n])
     tq = torch.from_numpy(qf).cuda()
     out = torch.zeros(n, dtype=torch.uint8, device="cuda")
@@ -55,8 +56,8 @@ def check_points(n: int) -> None:
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
     assert int(out.sum().item()) == n
-    print(json.dumps({"case": "check_points", "configs": n, "flop_per_config": h.flops()["total"],
-                      "launch_ms": ms[-1]}))
+    print(json.dumps({"case": "check_points", "configs": n, "broad_phase": cull,
+                      "flop_per_config": h.flops()["total"], "launch_ms": ms[-1]}))
 
 
 def batch(slots: int, iterations: int, sample_variant: int, check_item_cap: int) -> None:
@@ -181,6 +182,7 @@ def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["check_points", "batch", "point_check", "edge_check", "eizo_single"])
     ap.add_argument("--configs", type=int, default=1 << 20)
+    ap.add_argument("--no-cull", action="store_true", help="check_points: link-level broad phase off (full sweep)")
     ap.add_argument("--slots", type=int, default=24)
     ap.add_argument("--edges", type=int, default=100000)
     ap.add_argument("--regions", type=int, default=20)
@@ -189,7 +191,7 @@ def main() -> None:
     ap.add_argument("--check-item-cap", type=int, default=128)
     a = ap.parse_args()
     if a.case == "check_points":
-        check_points(a.configs)
+        check_points(a.configs, not a.no_cull)
     elif a.case == "point_check":
         point_check(a.configs)
     elif a.case == "edge_check":

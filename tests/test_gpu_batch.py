@@ -64,3 +64,27 @@ def test_batch_rejects_segment_outside_domain():
     far = np.full(7, 5.0, np.float32)
     with pytest.raises(RuntimeError):
         batch.inflate([0], [far], [far], [box(s7)])
+
+
+def test_every_sampler_variant_gives_the_same_regions():
+    """The autotuner may pick any sampler variant: all must agree bit for bit."""
+    s7 = scenes.arm_scene(31, num_spheres=40, num_capsules=2, num_world_boxes=30, num_world_spheres=30, keepout=0.8)
+    s14 = scenes.arm_scene(32, num_spheres=40, num_capsules=2, num_world_boxes=20, num_world_spheres=20, arms=2,
+                           keepout=0.9, arm_spacing=1.4)
+    opt = csd.EizoOptions(num_particles=600, mixing_steps=20, max_iterations=40)
+    e7 = free_edges(s7, 2, 0.3, 1)
+    e14 = free_edges(s14, 2, 0.3, 2)
+    slots = [0, 1, 0, 1]
+    edges = [e7[0], e14[0], e7[1], e14[1]]
+    scn = [s7, s14]
+    ref = None
+    for v in range(len(csd.BatchedEdgeInflator.SAMPLE_VARIANTS)):
+        b = csd.BatchedEdgeInflator([s7.plant, s14.plant], opt, max_slots=4, face_capacity=400, autotune_iterations=0)
+        b.set_shapes(v, 128)
+        got = b.inflate(slots, [e[0] for e in edges], [e[1] for e in edges], [box(scn[i]) for i in slots])
+        if ref is None:
+            ref = got
+            continue
+        for g, r in zip(got, ref):
+            np.testing.assert_array_equal(g.A(), r.A(), err_msg=f"variant {v}")
+            np.testing.assert_array_equal(g.b(), r.b(), err_msg=f"variant {v}")

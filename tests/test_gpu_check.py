@@ -196,3 +196,27 @@ def test_errors():
     with pytest.raises(csd.CsdError) as ei:
         csd.CheckCollisionFreeCuda(np.zeros((7, 1), np.float32), bad.plant)
     assert ei.value.code == 5
+
+
+@pytest.mark.parametrize("arms", [1, 2])
+def test_broad_phase_leaves_every_verdict_unchanged(arms):
+    """The link-level broad phase only skips pairs whose bounding spheres are
+    more than 1e-4 m apart, so verdicts with it on and off are identical."""
+    sc = scenes.arm_scene(77 + arms, num_spheres=60, num_capsules=4, num_world_boxes=120, num_world_spheres=120,
+                          arms=arms, keepout=0.6, arm_spacing=1.4)
+    q = sc.random_configs(60000, 5)
+    h = csd.plant_handle(sc.plant)
+    h.set_culling(True)
+    on = csd.CheckCollisionFreeCuda(q.T, sc.plant)
+    h.set_culling(False)
+    off = csd.CheckCollisionFreeCuda(q.T, sc.plant)
+    h.set_culling(True)
+    np.testing.assert_array_equal(on, off)
+    assert 0.02 < on.mean() < 0.98  # both verdicts occur
+    a = sc.random_configs(3000, 6)
+    b = np.clip(a + np.random.default_rng(7).normal(0, 0.3, a.shape), sc.lower(), sc.upper()).astype(np.float32)
+    e_on = csd.CheckEdgesCollisionFreeCuda(a.T, b.T, sc.plant)
+    h.set_culling(False)
+    e_off = csd.CheckEdgesCollisionFreeCuda(a.T, b.T, sc.plant)
+    h.set_culling(True)
+    np.testing.assert_array_equal(e_on, e_off)
