@@ -11,7 +11,8 @@ from .api import (MAX_DIM, BatchedEdgeInflator, MAX_NUM_FACES, MAX_NUM_VOXELS, C
                   CheckCollisionFreeVoxels, CheckCollisionFreeVoxelsCuda, CheckEdgeCollisionFree,
                   CheckEdgesCollisionFreeCuda, ComputeForwardKinematicsCuda, CudaEdgeInflator, EizoCuda, EizoInfo,
                   EizoIterationInfo, EizoOptions, HPolyhedron, MinimalHPolyhedron, PairCollisionFree, Voxels,
-                  UniformSampleInHPolyhedraCuda, computeLinkFrameToWorldTransformsMinimal, numSamplesUnadaptive,
+                  UniformSampleInHPolyhedraCuda, VisibilityGraph, computeLinkFrameToWorldTransformsMinimal,
+                  numSamplesUnadaptive,
                   plant_handle, printEizoSummary)
 from ._capi import CSD_EDGE_L2_REF, CSD_EDGE_LINF, CSD_EDGE_VG, CsdError
 

@@ -135,6 +135,35 @@ def CheckEdgeCollisionFree(configuration_1: np.ndarray, configuration_2: np.ndar
                                             step_size)[0])
 
 
+def VisibilityGraph(configurations: np.ndarray, plant: MinimalPlant, step_size: float,
+                    max_configs_per_batch: int = 10000000):
+    """VisibilityGraph (cuda_visibility_graph.cu:175-375): the collision-free
+    edges among the columns of `configurations` (dim x n) as an n x n
+    scipy.sparse matrix with a 1 at (i, j), i < j, for every free edge (the
+    upper triangle, as the reference's triplets). Edges use the reference's
+    visibility-graph discretisation (both endpoints, ceil(dist/step) + 2
+    points). The edges are generated and checked on the device, so
+    max_configs_per_batch (the reference's batching knob) only has its range
+    checked."""
+    import scipy.sparse as sp
+    h = plant_handle(plant)
+    q = _configs(configurations, h.dim)
+    n = q.shape[0]
+    if n < 2:
+        raise ValueError("a visibility graph needs at least two configurations")
+    if not step_size >= 1e-12:
+        raise ValueError("step_size must be at least 1e-12")
+    if not 1 < max_configs_per_batch <= 10000000:
+        raise ValueError("max_configs_per_batch must be in (1, 1e7]")
+    E = n * (n - 1) // 2
+    adj = np.zeros(E, np.uint8)
+    C.check(C.lib().csd_visibility_graph(h.handle, C.ptr(q), n, ctypes.c_float(step_size), C.ptr(adj),
+                                         C.CSD_PTR_HOST, None))
+    iu, ju = np.triu_indices(n, 1)
+    keep = adj.astype(bool)
+    return sp.csr_matrix((np.ones(int(keep.sum()), np.uint8), (iu[keep], ju[keep])), shape=(n, n))
+
+
 def PairCollisionFree(geom_a: CollisionGeometry, x_w_la: np.ndarray, geom_b: CollisionGeometry,
                       x_w_lb: np.ndarray) -> bool:
     """pairCollisionFree (collision_checker.cpp:91-203)."""

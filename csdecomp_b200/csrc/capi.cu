@@ -154,6 +154,30 @@ csd_status_t csd_check_edges(csd_plant_t p, const float* starts, const float* en
   return CSD_OK;
 }
 
+csd_status_t csd_visibility_graph(csd_plant_t p, const float* nodes, int32_t n, float step, uint8_t* adjacency,
+                                  int32_t flags, void* stream) {
+  CSD_CHECK(p && n >= 2 && nodes && adjacency, CSD_ERR_INVALID, "a visibility graph needs at least two nodes");
+  CSD_CHECK(step >= 1e-12f && std::isfinite(step), CSD_ERR_INVALID, "step size must be positive");
+  DeviceGuard g(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int d = p->dp.dim;
+  const int64_t E = (int64_t)n * (n - 1) / 2;
+  csd_status_t s;
+  if ((s = p->counter.reserve(64))) return s;
+  if (flags == CSD_PTR_DEVICE)
+    return launch_check_edges(p, nodes, nodes, E, step, CSD_EDGE_VG, adjacency, nullptr, p->counter.as<unsigned int>(),
+                              st, n);
+  const size_t qb = (size_t)n * d * sizeof(float);
+  if ((s = p->in_buf.reserve(qb + 16)) || (s = p->out_buf.reserve((size_t)E + 16))) return s;
+  CSD_CUDA_TRY(cudaMemcpyAsync(p->in_buf.ptr, nodes, qb, cudaMemcpyHostToDevice, st));
+  if ((s = launch_check_edges(p, p->in_buf.as<float>(), p->in_buf.as<float>(), E, step, CSD_EDGE_VG,
+                              p->out_buf.as<uint8_t>(), nullptr, p->counter.as<unsigned int>(), st, n)))
+    return s;
+  CSD_CUDA_TRY(cudaMemcpyAsync(adjacency, p->out_buf.ptr, (size_t)E, cudaMemcpyDeviceToHost, st));
+  CSD_CUDA_TRY(cudaStreamSynchronize(st));
+  return CSD_OK;
+}
+
 csd_status_t csd_pair_collision_free(int32_t ta, const float* da, const float* XLBa, const float* XWLa, int32_t tb,
                                      const float* db, const float* XLBb, const float* XWLb, uint8_t* out) {
   CSD_CHECK(da && XLBa && XWLa && db && XLBb && XWLb && out, CSD_ERR_INVALID, "null argument");

@@ -105,13 +105,29 @@ __device__ __forceinline__ void edge_point(const float* q1, const float* q2, int
 // One warp per edge, edges taken from a work counter. Points are visited
 // coarse to fine: with G = ceil(n/32), the visit order is g, G+g, 2G+g, ...
 // for g = 0, 1, ..., so the first 32 visits sample the whole edge evenly.
+// Pair index e of the upper triangle (i < j, row-major) of n nodes -> (i, j):
+// e = i n - i (i + 1) / 2 + (j - i - 1). The double-precision estimate of i
+// is corrected with exact integer row starts.
+static __device__ __forceinline__ void edge_pair(int64_t e, int64_t n, int64_t* i, int64_t* j) {
+  auto row_start = [n](int64_t r) { return r * n - r * (r + 1) / 2; };
+  const double b = 2.0 * (double)n - 1.0;
+  int64_t r = (int64_t)floor((b - sqrt(b * b - 8.0 * (double)e)) * 0.5);
+  r = r < 0 ? 0 : r > n - 2 ? n - 2 : r;
+  while (r > 0 && row_start(r) > e) --r;
+  while (r < n - 2 && row_start(r + 1) <= e) ++r;
+  *i = r;
+  *j = e - row_start(r) + r + 1;
+}
+
+// nodes > 0: the edges are every pair i < j of the `nodes` configurations in
+// `starts` (ends unused), in upper-triangle row-major order.
 template <bool SM>
 __global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) check_edges_kernel(DevPlant p, const float* __restrict__ starts,
                                                                          const float* __restrict__ ends, int64_t n,
                                                                          float step, int mode,
                                                                          uint8_t* __restrict__ out,
                                                                          int64_t* __restrict__ pts,
-                                                                         unsigned long long* counter) {
+                                                                         unsigned long long* counter, int64_t nodes) {
   extern __shared__ float4 smem4[];
   __shared__ uint64_t bar;
   const WarpCtx<SM> w = warp_setup<SM>(p, smem4, &bar);
@@ -125,7 +141,14 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) check_edges_kernel(Dev
     e = __shfl_sync(kFull, e, 0);
     if (e >= (unsigned long long)n) break;
     __syncwarp();
-    if (lane < d) {
+    if (nodes > 0) {
+      int64_t i = 0, j = 0;
+      edge_pair((int64_t)e, nodes, &i, &j);
+      if (lane < d) {
+        w.q1[lane] = starts[i * d + lane];
+        w.q2[lane] = starts[j * d + lane];
+      }
+    } else if (lane < d) {
       w.q1[lane] = starts[e * d + lane];
       w.q2[lane] = ends[e * d + lane];
     }
@@ -237,7 +260,8 @@ csd_status_t launch_fk(const csd_plant_s* p, const float* q, int64_t n, float* t
 }
 
 csd_status_t launch_check_edges(const csd_plant_s* p, const float* s0, const float* e0, int64_t n, float step,
-                                int mode, uint8_t* out, int64_t* pts, unsigned int* counter, cudaStream_t st) {
+                                int mode, uint8_t* out, int64_t* pts, unsigned int* counter, cudaStream_t st,
+                                int64_t nodes) {
   if (n <= 0) return CSD_OK;
   size_t smem = 0;
   int grid = 0;
@@ -246,10 +270,12 @@ csd_status_t launch_check_edges(const csd_plant_s* p, const float* s0, const flo
   unsigned long long* ctr = reinterpret_cast<unsigned long long*>(counter);
   if (statics_in_smem(p)) {
     if ((s = launch_grid(p, check_edges_kernel<true>, true, n, &smem, &grid))) return s;
-    check_edges_kernel<true><<<grid, 32 * kWarpsPerBlock, smem, st>>>(p->dp, s0, e0, n, step, mode, out, pts, ctr);
+    check_edges_kernel<true><<<grid, 32 * kWarpsPerBlock, smem, st>>>(p->dp, s0, e0, n, step, mode, out, pts, ctr,
+                                                                       nodes);
   } else {
     if ((s = launch_grid(p, check_edges_kernel<false>, false, n, &smem, &grid))) return s;
-    check_edges_kernel<false><<<grid, 32 * kWarpsPerBlock, smem, st>>>(p->dp, s0, e0, n, step, mode, out, pts, ctr);
+    check_edges_kernel<false><<<grid, 32 * kWarpsPerBlock, smem, st>>>(p->dp, s0, e0, n, step, mode, out, pts, ctr,
+                                                                        nodes);
   }
   CSD_CUDA_TRY(cudaGetLastError());
   return CSD_OK;

@@ -109,7 +109,7 @@ csd_status_t launch_check_points(const csd_plant_s* p, const float* q, int64_t n
                                  uint8_t* out, cudaStream_t st);
 csd_status_t launch_fk(const csd_plant_s* p, const float* q, int64_t n, float* tf, cudaStream_t st);
 csd_status_t launch_check_edges(const csd_plant_s* p, const float* s, const float* e, int64_t n, float step,
-                                int mode, uint8_t* out, int64_t* pts, unsigned int* counter, cudaStream_t st);
+                                int mode, uint8_t* out, int64_t* pts, unsigned int* counter, cudaStream_t st, int64_t nodes = 0);
 // sampler.cu
 csd_status_t launch_hit_and_run(const float* A, const float* b, const int32_t* face_off, int num_poly, int dim,
                                 const float* starts, int samples_per_poly, int mixing, uint64_t seed,

@@ -20,6 +20,10 @@
       config 3: R single inflations (CudaEdgeInflator) on the 7-DOF /
       200-primitive scene, seed edges U[0.1, 0.5] rad
 
+  python -m csdecomp_b200.profile_cases visibility_graph [--nodes n]
+      VisibilityGraph over n free configurations of the config-3 scene, 0.01 rad
+      step (n (n - 1) / 2 edges checked on the device)
+
 Each prints the device time of what it ran (CUDA events, after one warm-up).
 """
 from __future__ import annotations
@@ -178,14 +182,29 @@ def eizo_single(regions: int) -> None:
                       "mean_faces": faces / regions}))
 
 
+def visibility_graph(n: int) -> None:
+    import torch
+    import csdecomp_b200 as csd
+    from csdecomp_b200 import scenes
+    sc = scenes.edge_check_scene(keepout=0.8)
+    q = sc.random_configs(8 * n, 21)
+    nodes = q[csd.CheckCollisionFreeCuda(q.T, sc.plant) == 1][:n]
+    ms, A = _timed(lambda: csd.VisibilityGraph(nodes.T, sc.plant, 0.01), reps=1)
+    E = len(nodes) * (len(nodes) - 1) // 2
+    print(json.dumps({"case": "visibility_graph", "nodes": len(nodes), "edges": E, "ms": ms,
+                      "edges_per_s": E / ms * 1e3, "free_edges": int(A.nnz)}))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["check_points", "batch", "point_check", "edge_check", "eizo_single"])
+    ap.add_argument("case", choices=["check_points", "batch", "point_check", "edge_check", "eizo_single",
+                                     "visibility_graph"])
     ap.add_argument("--configs", type=int, default=1 << 20)
     ap.add_argument("--no-cull", action="store_true", help="check_points: link-level broad phase off (full sweep)")
     ap.add_argument("--slots", type=int, default=24)
     ap.add_argument("--edges", type=int, default=100000)
     ap.add_argument("--regions", type=int, default=20)
+    ap.add_argument("--nodes", type=int, default=1000)
     ap.add_argument("--iterations", type=int, default=12)
     ap.add_argument("--sample-variant", type=int, default=3)
     ap.add_argument("--check-item-cap", type=int, default=128)
@@ -198,6 +217,8 @@ def main() -> None:
         edge_check(a.edges)
     elif a.case == "eizo_single":
         eizo_single(a.regions)
+    elif a.case == "visibility_graph":
+        visibility_graph(a.nodes)
     else:
         batch(a.slots, a.iterations, a.sample_variant, a.check_item_cap)
 

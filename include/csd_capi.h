@@ -125,6 +125,16 @@ csd_status_t csd_check_edges(csd_plant_t plant, const float* starts, const float
                              float step_size, int32_t mode, uint8_t* free_out, int64_t* points_checked,
                              int32_t flags, void* stream);
 
+/* All-pairs visibility graph: VisibilityGraph, csdecomp/src/planning/cuda_visibility_graph.cu:175-375.
+ * nodes: [n][dim] configurations (n >= 2). adjacency receives one byte per
+ * pair i < j in upper-triangle row-major order (pair (i, j) at
+ * i n - i (i + 1) / 2 + j - i - 1): 1 if the edge is collision free under the
+ * reference's visibility-graph discretisation (CSD_EDGE_VG: both endpoints,
+ * ceil(dist / step) + 2 points), else 0. Edges are generated on the device
+ * from the node indices; each is checked by one warp with early exit. */
+csd_status_t csd_visibility_graph(csd_plant_t plant, const float* nodes, int32_t n, float step_size,
+                                  uint8_t* adjacency, int32_t flags, void* stream);
+
 /* One pair: pairCollisionFree, csdecomp/src/plant/collision_checker.cpp:91-203
  * (GPU contact rule of cuda_geometry_utilities.h:16-125). 4x4 matrices column-major. */
 csd_status_t csd_pair_collision_free(int32_t type_a, const float* dims_a, const float* X_L_B_a,

@@ -151,6 +151,36 @@ def test_edge_visibility_graph_golden(plants, golden):
     s, e = zip(*[(nodes[i], nodes[j]) for i in range(n - 1) for j in range(i + 1, n)])
     v = csd.CheckEdgesCollisionFreeCuda(np.array(s).T, np.array(e).T, gp.plant, case["step"], csd.CSD_EDGE_VG)
     assert list(v) == case["adjacency_upper"]
+    # the all-pairs entry point (VisibilityGraph) gives the same upper triangle
+    A = csd.VisibilityGraph(nodes.T, gp.plant, case["step"])
+    iu, ju = np.triu_indices(n, 1)
+    assert list(np.asarray(A[iu, ju]).ravel()) == case["adjacency_upper"]
+    assert A.shape == (n, n) and np.tril(A.toarray()).sum() == 0
+
+
+@pytest.mark.parametrize("n", [2, 3, 97, 700])
+def test_visibility_graph_matches_explicit_edges(n):
+    """Edges generated on the device from node pairs equal the same edges
+    passed explicitly (every pair i < j, visibility-graph discretisation)."""
+    sc = scenes.edge_check_scene(keepout=0.8)
+    q = sc.random_configs(4 * n, 11 + n)
+    nodes = q[csd.CheckCollisionFreeCuda(q.T, sc.plant) == 1][:n]
+    nodes = np.concatenate([nodes, q[:max(0, n - len(nodes))]])  # pad with any configurations
+    A = csd.VisibilityGraph(nodes.T, sc.plant, 0.05)
+    iu, ju = np.triu_indices(n, 1)
+    ref = csd.CheckEdgesCollisionFreeCuda(nodes[iu].T, nodes[ju].T, sc.plant, 0.05, csd.CSD_EDGE_VG)
+    np.testing.assert_array_equal(np.asarray(A[iu, ju]).ravel(), ref)
+    if n > 3:
+        assert 0 < ref.sum() < len(ref)
+
+
+def test_visibility_graph_rejects_bad_arguments():
+    sc = scenes.point_check_scene()
+    q = sc.random_configs(3, 1)
+    with pytest.raises(ValueError):
+        csd.VisibilityGraph(q[:1].T, sc.plant, 0.01)
+    with pytest.raises(ValueError):
+        csd.VisibilityGraph(q.T, sc.plant, 0.0)
 
 
 def test_zero_length_edge_reference_rule():
