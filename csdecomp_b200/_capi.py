@@ -7,7 +7,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from typing import Dict
+from typing import Dict, List, Tuple
 
 import numpy as np
 
@@ -80,15 +80,23 @@ class EizoIterC(ctypes.Structure):
     ]
 
 
+class EditRegionsOptionsC(ctypes.Structure):
+    _fields_ = [("configuration_margin", ctypes.c_float), ("bisection_steps", ctypes.c_uint32)]
+
+
 # every entry point declared in include/csd_capi.h
 EXPORTS = (
     "csd_last_error", "csd_version", "csd_plant_create", "csd_plant_destroy", "csd_plant_info", "csd_fk",
     "csd_check_points", "csd_check_edges", "csd_visibility_graph", "csd_pair_collision_free", "csd_uniform_sample_hpolyhedra",
-    "csd_inflator_create", "csd_inflator_inflate", "csd_inflator_destroy", "csd_eizo", "csd_eizo_noalloc", "csd_batch_create", "csd_batch_inflate", "csd_batch_configs_checked",
+    "csd_inflator_create", "csd_inflator_inflate", "csd_inflator_destroy", "csd_eizo", "csd_eizo_noalloc", "csd_edit_regions", "csd_batch_create", "csd_batch_inflate", "csd_batch_configs_checked",
     "csd_batch_set_profiling", "csd_batch_stage_ms", "csd_batch_iteration_profile", "csd_batch_sample_flops",
     "csd_batch_autotune", "csd_batch_tuning", "csd_batch_set_shapes", "csd_batch_set_surrogate",
     "csd_batch_set_surrogate_rounds",    "csd_batch_destroy",
     "csd_num_samples_unadaptive", "csd_fp32_fma_probe", "csd_plant_flops", "csd_plant_set_culling",
+    "csd_plant_set_voxel_grid",
+    "csd_urdf_create", "csd_urdf_destroy", "csd_urdf_register_package", "csd_urdf_parse_file",
+    "csd_urdf_parse_string", "csd_urdf_parse_directives", "csd_urdf_plant_desc", "csd_urdf_limits",
+    "csd_urdf_robot_geometry_ids", "csd_urdf_link_index", "csd_urdf_geometry_index",
     "csd_mlp_num_params", "csd_mlp_create", "csd_mlp_destroy", "csd_mlp_get_params", "csd_mlp_set_params",
     "csd_mlp_infer", "csd_mlp_gradients", "csd_mlp_train", "csd_mlp_gemm_test",
 )
@@ -160,6 +168,10 @@ class PlantHandle:
         """Link-level broad phase of the collision checks on (default) or off."""
         check(lib().csd_plant_set_culling(self.handle, int(bool(enable))))
 
+    def set_voxel_grid(self, enable: bool) -> None:
+        """Voxel hash grid of the voxel checks on (default) or off (every voxel tested)."""
+        check(lib().csd_plant_set_voxel_grid(self.handle, int(bool(enable))))
+
     def flops(self) -> dict:
         fk, pl, pa = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         check(lib().csd_plant_flops(self.handle, ctypes.byref(fk), ctypes.byref(pl), ctypes.byref(pa)))
@@ -179,3 +191,91 @@ class PlantHandle:
             except Exception:  # pragma: no cover - interpreter shutdown
                 pass
         self.handle = None
+
+
+class NativeURDFParser:
+    """URDFParser (urdf_parser.h:18-163) run by the library's C++ loader
+    (csd_urdf_*): the same tables as csdecomp_b200.plant.URDFParser, without
+    Python's XML and YAML modules. For C++ callers the C ABI is the interface;
+    this class exposes it to Python for testing and scripting."""
+
+    def __init__(self):
+        h = ctypes.c_void_p()
+        check(lib().csd_urdf_create(ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib is not None:
+            _lib.csd_urdf_destroy(h)
+            self._h = None
+
+    def register_package(self, name: str, path: str) -> bool:
+        ok = ctypes.c_int32(0)
+        check(lib().csd_urdf_register_package(self._h, name.encode(), path.encode(), ctypes.byref(ok)))
+        return bool(ok.value)
+
+    def parse_urdf(self, path: str) -> bool:
+        check(lib().csd_urdf_parse_file(self._h, path.encode()))
+        return True
+
+    def parse_urdf_string(self, text: str) -> bool:
+        check(lib().csd_urdf_parse_string(self._h, text.encode()))
+        return True
+
+    def parse_directives(self, path: str) -> bool:
+        check(lib().csd_urdf_parse_directives(self._h, path.encode()))
+        return True
+
+    def arrays(self) -> Tuple[Dict[str, np.ndarray], int, int]:
+        """(flat tables as MinimalPlant.arrays() gives them, dim, num_links)."""
+        d = PlantDesc()
+        check(lib().csd_urdf_plant_desc(self._h, ctypes.byref(d)))
+        J, G, P = d.num_joints, d.num_geometries, d.num_collision_pairs
+
+        def grab(p, n, ct, dt):
+            if n == 0:
+                return np.zeros(0, dt)
+            return np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ct)), shape=(n,)).astype(dt).copy()
+        i32, f32 = (ctypes.c_int32, np.int32), (ctypes.c_float, np.float32)
+        a = {
+            "joint_type": grab(d.joint_type, J, *i32), "joint_parent_link": grab(d.joint_parent_link, J, *i32),
+            "joint_child_link": grab(d.joint_child_link, J, *i32),
+            "joint_idx_to_config_idx": grab(d.joint_idx_to_config_idx, J, *i32),
+            "joint_traversal_sequence": grab(d.joint_traversal_sequence, J, *i32),
+            "joint_X_PL_J": grab(d.joint_X_PL_J, 16 * J, *f32), "joint_axis": grab(d.joint_axis, 3 * J, *f32),
+            "geom_type": grab(d.geom_type, G, *i32), "geom_link_index": grab(d.geom_link_index, G, *i32),
+            "geom_group": grab(d.geom_group, G, *i32), "geom_dimensions": grab(d.geom_dimensions, 3 * G, *f32),
+            "geom_X_L_B": grab(d.geom_X_L_B, 16 * G, *f32),
+            "collision_pairs_flat": grab(d.collision_pairs_flat, 2 * P, *i32),
+        }
+        return a, d.num_configuration_variables, d.num_links
+
+    def get_minimal_plant(self):
+        from .plant import MinimalPlant
+        a, dim, L = self.arrays()
+        return MinimalPlant.from_arrays(a, dim, L)
+
+    def robot_geometry_ids(self) -> List[int]:
+        p = ctypes.POINTER(ctypes.c_int32)()
+        n = ctypes.c_int32(0)
+        check(lib().csd_urdf_robot_geometry_ids(self._h, ctypes.byref(p), ctypes.byref(n)))
+        return [int(p[i]) for i in range(n.value)]
+
+    def position_limits(self) -> Tuple[np.ndarray, np.ndarray]:
+        d = PlantDesc()
+        check(lib().csd_urdf_plant_desc(self._h, ctypes.byref(d)))
+        lo = np.zeros(d.num_configuration_variables, np.float32)
+        hi = np.zeros(d.num_configuration_variables, np.float32)
+        check(lib().csd_urdf_limits(self._h, ptr(lo), ptr(hi)))
+        return lo, hi
+
+    def link_index(self, name: str) -> int:
+        i = ctypes.c_int32(-1)
+        check(lib().csd_urdf_link_index(self._h, name.encode(), ctypes.byref(i)))
+        return i.value
+
+    def geometry_index(self, name: str) -> int:
+        i = ctypes.c_int32(-1)
+        check(lib().csd_urdf_geometry_index(self._h, name.encode(), ctypes.byref(i)))
+        return i.value

@@ -469,6 +469,102 @@ def EizoCuda(line_start, line_end, voxels, voxel_radius: float, domain: HPolyhed
     return MinimalHPolyhedron(A_out[:nf.value].copy(), b_out[:nf.value].copy())
 
 
+class EditRegionsOptions:
+    """EditRegionsOptions (cuda_edit_regions.h:12-16)."""
+
+    def __init__(self, configuration_margin: float = 0.01, bisection_steps: int = 9, verbose: bool = False):
+        self.configuration_margin = configuration_margin
+        self.bisection_steps = bisection_steps
+        self.verbose = verbose
+
+    def _c(self) -> "C.EditRegionsOptionsC":
+        if int(self.bisection_steps) < 0:
+            raise ValueError("bisection_steps must be non-negative")
+        return C.EditRegionsOptionsC(float(self.configuration_margin), int(self.bisection_steps))
+
+
+def EditRegionsCuda(collisions, line_segment_idxs, line_start_points, line_end_points, regions, plant,
+                    robot_geometry_ids, voxels, voxel_radius: float, options: EditRegionsOptions):
+    """EditRegionsCuda (cuda_edit_regions.cu:44-301, binding cuda_bindings.h:140-179):
+    cuts the colliding configurations (columns of `collisions`, dim x n) out of
+    the regions while each region keeps its segment (columns of
+    line_start_points / line_end_points, dim x len(regions)). Collision i is
+    bisected towards its projection on segment line_segment_idxs[i]; faces are
+    placed nearest first, each only if its optimized collision is still inside
+    the region. Returns (edited regions, (projections, optimized collisions)),
+    the two dim x n matrices grouped by segment as the reference returns them."""
+    h = plant_handle(plant)
+    d = h.dim
+    regions = list(regions)
+    if not regions:
+        raise ValueError("Regions vector cannot be empty")
+    m = len(regions)
+    ls = np.asarray(line_start_points, np.float32)
+    le = np.asarray(line_end_points, np.float32)
+    if ls.ndim != 2 or le.ndim != 2 or ls.shape[1] != m or le.shape[1] != m:
+        raise ValueError("Number of line segments must match number of regions")
+    if ls.shape[0] != le.shape[0]:
+        raise ValueError("Line start and end points must have same dimension")
+    amb = regions[0].ambient_dimension()
+    col = np.asarray(collisions, np.float32)
+    if col.ndim != 2 or col.shape[0] != amb:
+        raise ValueError("collisions must live in the same space as the regions")
+    if ls.shape[0] != amb:
+        raise ValueError("the linesegments must live in the same dimension as the regions")
+    if amb != d or any(r.ambient_dimension() != d for r in regions):
+        raise C.CsdError(C.CSD_ERR_DIMENSION, f"regions have dimension {amb}, the plant {d}")
+    ids = np.ascontiguousarray(np.asarray(list(robot_geometry_ids), np.int32).reshape(-1))
+    if ids.size == 0:
+        raise ValueError("Robot geometry IDs cannot be empty")
+    if not voxel_radius > 0:
+        raise ValueError("Voxel radius must be positive")
+    v = _voxel_rows(voxels)
+    if v.shape[0] > MAX_NUM_VOXELS:
+        raise RuntimeError("Voxel buffer size insufficient")
+    n = col.shape[1]
+    seg = np.ascontiguousarray(np.asarray(list(line_segment_idxs), np.int64).reshape(-1))
+    if seg.size != n:
+        raise ValueError("one line segment index per collision is required")
+    if n and (seg.min() < 0 or seg.max() >= m):
+        raise IndexError("line segment index out of range")
+    if options.verbose:
+        print(f"[EditRegionsCuda] Num collisions to be optimized {n}")
+    if n == 0:
+        raise RuntimeError("[EditRegionsCuda] No collisions are contained in the regions, this is not supported.\n")
+    q = np.ascontiguousarray(col.T)
+    seg32 = np.ascontiguousarray(seg.astype(np.uint32))
+    A = np.ascontiguousarray(np.concatenate([np.asarray(r.A(), np.float32).reshape(-1, d) for r in regions]))
+    b = np.ascontiguousarray(np.concatenate([np.asarray(r.b(), np.float32).reshape(-1) for r in regions]))
+    off = np.zeros(m + 1, np.int32)
+    off[1:] = np.cumsum([r.b().size for r in regions])
+    cap = int(off[-1]) + n
+    A_out = np.zeros((cap, d), np.float32)
+    b_out = np.zeros(cap, np.float32)
+    nf = np.zeros(m, np.int32)
+    proj = np.zeros((n, d), np.float32)
+    opt = np.zeros((n, d), np.float32)
+    o = options._c()
+    C.check(C.lib().csd_edit_regions(h.handle, C.ptr(q), C.ptr(seg32), ctypes.c_int64(n),
+                                     C.ptr(np.ascontiguousarray(ls.T)), C.ptr(np.ascontiguousarray(le.T)), m,
+                                     C.ptr(A), C.ptr(b), C.ptr(off), C.ptr(v) if v.size else None, v.shape[0],
+                                     ctypes.c_float(voxel_radius), C.ptr(ids), ids.size, ctypes.byref(o),
+                                     C.ptr(A_out), C.ptr(b_out), C.ptr(nf), C.ptr(proj), C.ptr(opt)))
+    counts = np.bincount(seg, minlength=m)
+    coff = np.concatenate([[0], np.cumsum(counts)])
+    edited = []
+    for r in range(m):
+        if counts[r] == 0:
+            if options.verbose:
+                print(f"[EditRegionsCuda] region {r} remains unchanged")
+            edited.append(regions[r])
+            continue
+        row = int(off[r] + coff[r])
+        if options.verbose:
+            print(f"[EditRegionsCuda] region {r} added {int(nf[r]) - regions[r].b().size} faces")
+        edited.append(HPolyhedron(A_out[row:row + nf[r]], b_out[row:row + nf[r]]))
+    return edited, (np.ascontiguousarray(proj.T), np.ascontiguousarray(opt.T))
+
+
 class BatchedEdgeInflator:
     """Many EI-ZO inflations advancing together on the GPU (csd_batch_*): each
     slot has its own plant, segment and domain and yields exactly the region

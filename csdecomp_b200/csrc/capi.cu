@@ -106,6 +106,7 @@ csd_status_t csd_check_points(csd_plant_t p, const float* q, int64_t n, const fl
     vt.tile_mask = p->vox_tab.as<uint32_t>();
     vt.other = p->vox_tab.as<uint32_t>() + p->dp.num_tiles;
     vt.num_other = no;
+    if ((s = build_voxel_grid(p, voxel_grid_cell(p, tab, vr), &p->vox_grid_buf, &vt, st))) return s;
   }
   if (flags == CSD_PTR_DEVICE) {
     s = launch_check_points(p, q, n, vt, out, st);

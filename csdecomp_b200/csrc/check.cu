@@ -233,7 +233,7 @@ static csd_status_t launch_grid(const csd_plant_s* p, K kernel, bool sm, int64_t
 csd_status_t launch_check_points(const csd_plant_s* p, const float* q, int64_t n, const VoxelTables& vt,
                                  uint8_t* out, cudaStream_t st) {
   if (n <= 0) return CSD_OK;
-  VoxArgs va{vt.vox, vt.nv, vt.vr, vt.tile_mask, vt.other, vt.num_other};
+  const VoxArgs va = vox_args(vt);
   size_t smem = 0;
   int grid = 0;
   csd_status_t s;

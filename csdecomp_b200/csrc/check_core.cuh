@@ -36,7 +36,36 @@ struct VoxArgs {
   const uint32_t* tile_mask;
   const uint32_t* other;
   int num_other;
+  // voxel hash grid (voxgrid.cu); gstart == nullptr: every voxel is tested
+  const float4* gvox;   // voxels ordered by bucket
+  const int* gstart;    // [buckets + 1] first voxel of each bucket
+  int gmask;            // buckets - 1 (a power of two minus one)
+  float ginv_h;         // 1 / cell edge
 };
+
+static inline VoxArgs vox_args(const VoxelTables& vt) {
+  return VoxArgs{vt.vox, vt.nv, vt.vr, vt.tile_mask, vt.other, vt.num_other, vt.gvox, vt.gstart, vt.gmask, vt.ginv_h};
+}
+
+// ---- voxel hash grid: cell (floor(x/h), floor(y/h), floor(z/h)) computed as
+// floor(x * inv_h), which is monotone in x, so a voxel within R of a point
+// lies in a cell between the cells of the point -/+ R on every axis. Buckets
+// by the spatial hash of Teschner et al. (2003), "Optimized Spatial Hashing
+// for Collision Detection of Deformable Objects" (primes 73856093, 19349663,
+// 83492791); cells sharing a bucket only add candidates.
+static __host__ __device__ __forceinline__ int vox_cell(float x, float inv_h) {
+#ifdef __CUDA_ARCH__
+  return __float2int_rd(__fmul_rn(x, inv_h));
+#else
+  const float v = floorf(x * inv_h);
+  return v >= 2147483520.f ? 2147483520 : v <= -2147483520.f ? -2147483520 : (int)v;
+#endif
+}
+static __host__ __device__ __forceinline__ uint32_t vox_bucket(int ix, int iy, int iz, int mask) {
+  return ((uint32_t)ix * 73856093u ^ (uint32_t)iy * 19349663u ^ (uint32_t)iz * 83492791u) & (uint32_t)mask;
+}
+constexpr int kVoxGridMaxCells = 512;   // larger query boxes test every voxel
+constexpr int kVoxGridMinVoxels = 64;   // fewer voxels are tested without a grid
 
 // Per-warp shared memory (floats): slot transforms [slots][12], the warp's
 // configuration [kMaxDim], two spare configurations (edge endpoints)
@@ -601,8 +630,96 @@ static __device__ bool sweep_generic(const DevPlant& p, const float4* stat, cons
   return false;
 }
 
+// Voxels near one geometry through the hash grid: every voxel in the cells
+// covering the geometry's bounding sphere (bc, br) grown by the voxel radius
+// (x 1.001 + 1e-4 m, above any FP32 rounding of the pair tests) is tested
+// with the same pair test as the full sweep, so the verdict is the full
+// sweep's. SPH: the geometry is the sphere G (tested as in the tile sweep).
+template <bool SPH>
+static __device__ bool grid_geom_hit(const VoxArgs& va, int tg, const float* G, const float* bc, float br) {
+  const float R = __fmaf_rn(__fadd_rn(br, va.vr), 1.001f, 1e-4f);
+  int lo[3], hi[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    lo[i] = vox_cell(__fsub_rn(bc[i], R), va.ginv_h);
+    hi[i] = vox_cell(__fadd_rn(bc[i], R), va.ginv_h);
+  }
+  const long long cells = (long long)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+  const bool finite = isfinite(bc[0]) && isfinite(bc[1]) && isfinite(bc[2]) && isfinite(R);
+  if (!finite || cells > kVoxGridMaxCells) {  // (a NaN pose collides with every voxel in the full sweep)
+    for (int v = 0; v < va.nv; ++v) {
+      float S[4] = {__ldg(va.vox + 3 * v), __ldg(va.vox + 3 * v + 1), __ldg(va.vox + 3 * v + 2), va.vr};
+      if (SPH ? sph_sph_hit(G, S) : pair_hit(G_SPHERE, S, tg, G)) return true;
+    }
+    return false;
+  }
+  for (int ix = lo[0]; ix <= hi[0]; ++ix)
+    for (int iy = lo[1]; iy <= hi[1]; ++iy)
+      for (int iz = lo[2]; iz <= hi[2]; ++iz) {
+        const uint32_t b = vox_bucket(ix, iy, iz, va.gmask);
+        const int k1 = __ldg(va.gstart + b + 1);
+        for (int k = __ldg(va.gstart + b); k < k1; ++k) {
+          const float4 v = __ldg(va.gvox + k);
+          float S[4] = {v.x, v.y, v.z, va.vr};
+          if (SPH ? sph_sph_hit(G, S) : pair_hit(G_SPHERE, S, tg, G)) return true;
+        }
+      }
+  return false;
+}
+
+// Bounding sphere of a world-posed geometry (WG layout: sphere [c r],
+// capsule [a r | u hl], box [x -q0 | y -q1 | z -q2 | h]).
+static __device__ __forceinline__ float geom_bound(int tg, const float* G, float* c) {
+  if (tg == G_SPHERE || tg == G_CAPSULE) {
+    c[0] = G[0];
+    c[1] = G[1];
+    c[2] = G[2];
+    return tg == G_SPHERE ? G[3] : G[3] + G[7];
+  }
+#pragma unroll
+  for (int r = 0; r < 3; ++r) c[r] = -fmaf(G[8 + r], G[11], fmaf(G[4 + r], G[7], G[r] * G[3]));
+  return sqrtf(fmaf(G[14], G[14], fmaf(G[13], G[13], G[12] * G[12])));
+}
+
+static __device__ bool sweep_voxels_grid(const DevPlant& p, const float4* stat, const float* pose, const VoxArgs& va,
+                                         int lane) {
+  for (int t = 0; t < p.num_tiles; ++t) {
+    const uint32_t mask = va.tile_mask[t];
+    if (!mask) continue;
+    float c[4];
+    own_sphere(p, pose, t * kWarp + lane, c);
+    const bool hit = ((mask >> lane) & 1u) && grid_geom_hit<true>(va, G_SPHERE, c, c, c[3]);
+    if (__any_sync(kFull, hit)) return true;
+  }
+  for (int o0 = 0; o0 < va.num_other; o0 += kWarp) {
+    const int o = o0 + lane;
+    bool hit = false;
+    if (o < va.num_other) {
+      const uint32_t ref = va.other[o];
+      float G[16];
+      int tg;
+      if (ref & 0x80000000u) {
+        const int s = (int)(ref & 0x7fffffffu);
+        tg = __ldg(p.static_type + s);
+        load4f(stat + 4 * s, tg == G_SPHERE ? 1 : tg == G_CAPSULE ? 2 : 4, G);
+      } else {
+        tg = __ldg(&p.moving[ref].type);
+        const int nw = tg == G_SPHERE ? 4 : tg == G_CAPSULE ? 8 : 16;
+        const float* src = pose + pose_offset(p, (int)ref);
+        for (int i = 0; i < nw; ++i) G[i] = src[i];
+      }
+      float bc[3];
+      const float br = geom_bound(tg, G, bc);
+      hit = grid_geom_hit<false>(va, tg, G, bc, br);
+    }
+    if (__any_sync(kFull, hit)) return true;
+  }
+  return false;
+}
+
 static __device__ bool sweep_voxels(const DevPlant& p, const float4* stat, const float* pose, const VoxArgs& va,
                                     int lane) {
+  if (va.gstart) return sweep_voxels_grid(p, stat, pose, va, lane);
   for (int t = 0; t < p.num_tiles; ++t) {
     const uint32_t mask = va.tile_mask[t];
     if (!mask) continue;

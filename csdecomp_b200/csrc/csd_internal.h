@@ -84,8 +84,9 @@ struct csd_plant_s {
   csd::HostPlant host;
   void* blob = nullptr;  // device tables
   bool cull_eligible = false;  // <= 32 slots and <= 1024 statics
+  bool vox_grid = true;        // voxel checks through the hash grid (csd_plant_set_voxel_grid)
   // scratch for host-pointer calls and per-call voxel tables
-  csd::DevBuf in_buf, in_buf2, out_buf, out_buf2, vox_buf, vox_tab, counter;
+  csd::DevBuf in_buf, in_buf2, out_buf, out_buf2, vox_buf, vox_tab, vox_grid_buf, counter;
   ~csd_plant_s();
 };
 
@@ -99,10 +100,23 @@ struct VoxelTables {
   const uint32_t* tile_mask = nullptr;  // [num_tiles] lanes of each sphere tile checked against voxels
   const uint32_t* other = nullptr;      // geometry refs (bit31 = static) checked lane-over-voxels
   int num_other = 0;
+  // hash grid over the voxels (voxgrid.cu); gstart == nullptr: no grid
+  const float4* gvox = nullptr;
+  const int* gstart = nullptr;
+  int gmask = 0;
+  float ginv_h = 0.f;
 };
 
 csd_status_t build_voxel_tables(csd_plant_s* p, const int32_t* robot_ids, int nr, std::vector<uint32_t>* tab,
                                 int* num_other);
+// Cell edge of the voxel grid for these tables (tab from build_voxel_tables):
+// twice the median radius of the robot spheres checked against voxels plus
+// the voxel radius.
+float voxel_grid_cell(const csd_plant_s* p, const std::vector<uint32_t>& tab, float vr);
+// Builds the hash grid of the device voxels vt->vox (vt->nv of them) into buf
+// on stream st and fills vt's grid fields, when the plant's grid switch is on
+// and there are at least kVoxGridMinVoxels voxels; otherwise leaves them null.
+csd_status_t build_voxel_grid(const csd_plant_s* p, float cell, DevBuf* buf, VoxelTables* vt, cudaStream_t st);
 
 // kernels (check.cu)
 csd_status_t launch_check_points(const csd_plant_s* p, const float* q, int64_t n, const VoxelTables& vt,

@@ -84,7 +84,7 @@ struct csd_inflator_s {
   std::vector<float> domain_A, domain_b;
   std::vector<uint32_t> vtab_host;
   int num_other = 0;
-  csd::DevBuf A, At, b, nf, samples, flags, cols, proj, dist, seg, vox, vtab, cnt;
+  csd::DevBuf A, At, b, nf, samples, flags, cols, proj, dist, seg, vox, vtab, vgrid, cnt;
   csd::EizoCounters* host_cnt = nullptr;  // pinned
   int* host_nf = nullptr;                 // pinned
   ~csd_inflator_s() {
@@ -229,6 +229,7 @@ csd_status_t csd_inflator_inflate(csd_inflator_t h, const float* ls, const float
   if (nv) CSD_CUDA_TRY(cudaMemcpyAsync(h->vox.ptr, voxels, (size_t)nv * 12, cudaMemcpyHostToDevice, st));
   const float* ls_d = h->seg.as<float>();
   const float* le_d = ls_d + d;
+  csd_status_t s;
   VoxelTables vt;
   if (nv > 0 && !h->vtab_host.empty()) {
     vt.vox = h->vox.as<float>();
@@ -237,10 +238,10 @@ csd_status_t csd_inflator_inflate(csd_inflator_t h, const float* ls, const float
     vt.tile_mask = h->vtab.as<uint32_t>();
     vt.other = h->vtab.as<uint32_t>() + p->dp.num_tiles;
     vt.num_other = h->num_other;
+    if ((s = build_voxel_grid(p, voxel_grid_cell(p, h->vtab_host, vr), &h->vgrid, &vt, st))) return s;
   }
-  VoxArgs va{vt.vox, vt.nv, vt.vr, vt.tile_mask, vt.other, vt.num_other};
+  const VoxArgs va = vox_args(vt);
   EizoCounters* cnt = h->cnt.as<EizoCounters>();
-  csd_status_t s;
   int nit = 0;
   int last_with_faces = -1;
   auto t_prev = std::chrono::high_resolution_clock::now();
@@ -488,7 +489,7 @@ extern "C" csd_status_t csd_eizo_noalloc(csd_plant_t plant, const float* ls, con
     vt.other = vtab + T;
     vt.num_other = num_other;
   }
-  VoxArgs va{vt.vox, vt.nv, vt.vr, vt.tile_mask, vt.other, vt.num_other};
+  const VoxArgs va = vox_args(vt);
   EizoCounters hc{};
   int nit = 0, last_with_faces = -1;
   for (uint32_t it = 0; it < o->max_iterations; ++it) {

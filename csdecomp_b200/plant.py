@@ -53,15 +53,34 @@ def _f32(x) -> np.float32:
     return np.float32(x)
 
 
+def _mat3(a, b):
+    """3x3 product in FP64, each entry summed k = 0, 1, 2 (the native loader's order)."""
+    out = [[0.0] * 3 for _ in range(3)]
+    for i in range(3):
+        for j in range(3):
+            s = 0.0
+            for k in range(3):
+                s += a[i][k] * b[k][j]
+            out[i][j] = s
+    return out
+
+
 def rpy_to_matrix(r: float, p: float, y: float) -> np.ndarray:
-    """Rz(y) * Ry(p) * Rx(r) (urdf_parser.cpp:370-375), evaluated in FP64, stored FP32."""
+    """(Rz(y) * Ry(p)) * Rx(r) (urdf_parser.cpp:370-375), evaluated in FP64, stored FP32."""
     cr, sr = math.cos(r), math.sin(r)
     cp, sp = math.cos(p), math.sin(p)
     cy, sy = math.cos(y), math.sin(y)
-    rx = np.array([[1, 0, 0], [0, cr, -sr], [0, sr, cr]])
-    ry = np.array([[cp, 0, sp], [0, 1, 0], [-sp, 0, cp]])
-    rz = np.array([[cy, -sy, 0], [sy, cy, 0], [0, 0, 1]])
-    return (rz @ ry @ rx).astype(np.float32)
+    rx = [[1.0, 0.0, 0.0], [0.0, cr, -sr], [0.0, sr, cr]]
+    ry = [[cp, 0.0, sp], [0.0, 1.0, 0.0], [-sp, 0.0, cp]]
+    rz = [[cy, -sy, 0.0], [sy, cy, 0.0], [0.0, 0.0, 1.0]]
+    return np.array(_mat3(_mat3(rz, ry), rx), np.float64).astype(np.float32)
+
+
+def unit_axis(a) -> np.ndarray:
+    """a / |a| in FP32 with |a|^2 summed x, y, z (Eigen's normalized() on a Vector3f)."""
+    x, y, z = (np.float32(v) for v in a)
+    n = np.float32(np.sqrt(np.float32(np.float32(np.float32(x * x) + np.float32(y * y)) + np.float32(z * z))))
+    return np.array([x / n, y / n, z / n], np.float32)
 
 
 def make_transform(R: np.ndarray, t: Sequence[float]) -> np.ndarray:
@@ -504,6 +523,10 @@ class URDFParser:
             self._parse_joint(joint_el)
         if not any(j.parent_link == 0 for j in tree.joints):
             raise RuntimeError("[CSDECOMP:URDFPARSER] The provided urdf is not connected to the 'world' link")
+        for link in tree.links[1:]:  # urdf_parser.cpp:136-154
+            if link.parent_joint < 0:
+                raise RuntimeError(f"[CSDECOMP:URDFPARSER] The link {link.name} has no parent joint; every model "
+                                   "must be connected to the world frame.")
         tree.finalize()
         self.finalize_scene()
         return True
@@ -538,8 +561,7 @@ class URDFParser:
             ax = el.find("axis")
             if ax is None:
                 raise RuntimeError("revolute or prismatic joint without axis")
-            a = np.array(_floats(ax.get("xyz"), 3), np.float32)
-            axis = (a / np.float32(np.sqrt(np.float32(np.dot(a, a))))).astype(np.float32)
+            axis = unit_axis(_floats(ax.get("xyz"), 3))
         parent, child = el.find("parent"), el.find("child")
         if parent is None or child is None:
             raise RuntimeError("Joint is missing parent or child element")

@@ -23,6 +23,14 @@
   python -m csdecomp_b200.profile_cases visibility_graph [--nodes n]
       VisibilityGraph over n free configurations of the config-3 scene, 0.01 rad
       step (n (n - 1) / 2 edges checked on the device)
+  python -m csdecomp_b200.profile_cases voxel_check [--configs N] [--voxels V]
+      checkCollisionFreeVoxelsCuda at scale: the config-2 arm (80 spheres + 4
+      capsules, 200 world primitives) against V voxels of radius 0.02 m
+      (uniform in a 3 x 3 x 1.5 m box around the arm, none within 0.3 m of its
+      base), N uniform configurations; with and without the voxel hash grid
+  python -m csdecomp_b200.profile_cases edit_regions [--regions R] [--collisions C]
+      EditRegionsCuda on the config-3 scene: R box regions around seed edges,
+      C colliding configurations drawn inside each, 9 bisection steps
 
 Each prints the device time of what it ran (CUDA events, after one warm-up).
 """
@@ -195,16 +203,91 @@ def visibility_graph(n: int) -> None:
                       "edges_per_s": E / ms * 1e3, "free_edges": int(A.nnz)}))
 
 
+def edit_regions(regions: int, per_region: int) -> None:
+    import csdecomp_b200 as csd
+    from csdecomp_b200 import scenes
+    sc = scenes.edge_check_scene(keepout=0.8)
+    edges = scenes.seed_edges(sc, regions, 3100, lambda q: csd.CheckCollisionFreeCuda(q.T, sc.plant),
+                              lambda x, y: csd.CheckEdgesCollisionFreeCuda(x.T, y.T, sc.plant), length=(0.1, 0.5))
+    rng = np.random.default_rng(5)
+    lo, hi = sc.lower(), sc.upper()
+    doms, cols, segs = [], [], []
+    for r, (q0, q1) in enumerate(edges):
+        blo = np.maximum(lo, np.minimum(q0, q1) - 0.4).astype(np.float32)
+        bhi = np.minimum(hi, np.maximum(q0, q1) + 0.4).astype(np.float32)
+        P = csd.HPolyhedron()
+        P.MakeBox(blo, bhi)
+        doms.append(P)
+        got = np.zeros((0, sc.dim), np.float32)
+        while got.shape[0] < per_region:
+            q = (blo + (bhi - blo) * rng.random((4 * per_region, sc.dim))).astype(np.float32)
+            got = np.concatenate([got, q[csd.CheckCollisionFreeCuda(q.T, sc.plant) == 0]])
+        cols.append(got[:per_region])
+        segs.append(np.full(per_region, r))
+    col = np.concatenate(cols).T
+    seg = np.concatenate(segs)
+    ls = np.stack([e[0] for e in edges], 1).astype(np.float32)
+    le = np.stack([e[1] for e in edges], 1).astype(np.float32)
+    opts = csd.EditRegionsOptions()
+    rids = sc.inspector.robot_geometry_ids
+    ms, out = _timed(lambda: csd.EditRegionsCuda(col, seg, ls, le, doms, sc.plant, rids, csd.Voxels(), 0.01, opts))
+    added = sum(e.b().size - d.b().size for e, d in zip(out[0], doms))
+    n = col.shape[1]
+    print(json.dumps({"case": "edit_regions", "regions": len(edges), "collisions": n, "ms": ms,
+                      "collisions_per_s": n / ms * 1e3, "checks_per_s": n * opts.bisection_steps / ms * 1e3,
+                      "faces_added": int(added)}))
+
+
+def voxel_scene(voxels: int, seed: int = 17):
+    """The voxel-at-scale workload: (scene, voxels [V][3], radius, robot ids)."""
+    from csdecomp_b200 import scenes
+    sc = scenes.edge_check_scene(keepout=0.8)
+    rng = np.random.default_rng(seed)
+    v = np.zeros((0, 3), np.float32)
+    while v.shape[0] < voxels:
+        c = rng.uniform([-1.5, -1.5, 0.0], [1.5, 1.5, 1.5], (2 * voxels, 3)).astype(np.float32)
+        v = np.concatenate([v, c[np.linalg.norm(c, axis=1) > 0.3]])
+    return sc, np.ascontiguousarray(v[:voxels]), 0.02, sc.inspector.robot_geometry_ids
+
+
+def voxel_check(n: int, voxels: int) -> None:
+    import torch
+    import csdecomp_b200 as csd
+    from csdecomp_b200 import _capi as C
+    sc, vox, vr, rids = voxel_scene(voxels)
+    h = csd.plant_handle(sc.plant)
+    q = torch.from_numpy(np.ascontiguousarray(sc.random_configs(n, 5))).cuda()
+    vd = torch.from_numpy(vox).cuda()
+    ids = torch.tensor(list(rids), dtype=torch.int32).cuda()
+    out = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream()
+
+    def run():
+        C.check(C.lib().csd_check_points(h.handle, C.ptr(q.data_ptr()), ctypes.c_int64(n), C.ptr(vd.data_ptr()),
+                                         voxels, ctypes.c_float(vr), C.ptr(ids.data_ptr()), len(rids),
+                                         C.ptr(out.data_ptr()), C.CSD_PTR_DEVICE, ctypes.c_void_p(st.cuda_stream)))
+    res = {}
+    for grid in (True, False):
+        h.set_voxel_grid(grid)
+        ms, _ = _timed(run)
+        res["grid" if grid else "every_voxel"] = {"ms": ms, "configs_per_s": n / ms * 1e3,
+                                                   "free_fraction": float(out.float().mean().item())}
+    h.set_voxel_grid(True)
+    print(json.dumps({"case": "voxel_check", "configs": n, "voxels": voxels, "voxel_radius": vr, **res}))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["check_points", "batch", "point_check", "edge_check", "eizo_single",
-                                     "visibility_graph"])
+                                     "visibility_graph", "edit_regions", "voxel_check"])
     ap.add_argument("--configs", type=int, default=1 << 20)
     ap.add_argument("--no-cull", action="store_true", help="check_points: link-level broad phase off (full sweep)")
     ap.add_argument("--slots", type=int, default=24)
     ap.add_argument("--edges", type=int, default=100000)
     ap.add_argument("--regions", type=int, default=20)
     ap.add_argument("--nodes", type=int, default=1000)
+    ap.add_argument("--collisions", type=int, default=512, help="edit_regions: collisions per region")
+    ap.add_argument("--voxels", type=int, default=10000, help="voxel_check: voxels")
     ap.add_argument("--iterations", type=int, default=12)
     ap.add_argument("--sample-variant", type=int, default=3)
     ap.add_argument("--check-item-cap", type=int, default=128)
@@ -219,6 +302,10 @@ def main() -> None:
         eizo_single(a.regions)
     elif a.case == "visibility_graph":
         visibility_graph(a.nodes)
+    elif a.case == "edit_regions":
+        edit_regions(a.regions, a.collisions)
+    elif a.case == "voxel_check":
+        voxel_check(a.configs, a.voxels)
     else:
         batch(a.slots, a.iterations, a.sample_variant, a.check_item_cap)
 

@@ -2,7 +2,8 @@
  * csd_capi.h -- C ABI of csdecomp_b200, the B200 (sm_100a) implementation of
  * CSDecomp's hot path: batched forward kinematics, primitive-pair collision
  * checking over a MinimalPlant, batched edge checks, hit-and-run sampling in
- * an H-polytope and EI-ZO edge inflation.
+ * an H-polytope, EI-ZO edge inflation, the visibility graph and region
+ * editing.
  *
  * Every entry point names the reference interface it replaces (paths are
  * relative to the wernerpe/csdecomp source tree). Conventions:
@@ -93,6 +94,34 @@ typedef struct csd_inflator_s* csd_inflator_t;
 
 const char* csd_last_error(void);
 int32_t csd_version(void);
+
+/* Native model loader: URDFParser, csdecomp/src/plant/urdf_parser.h:18-163
+ * (parseURDF :33, parseURDFString :49, registerPackage :56, parseDirectives
+ * :78, getMinimalPlant :86, getSceneInspector().robot_geometry_ids, the
+ * kinematic tree's position limits). A handle holds one model. Parse errors
+ * (the reference's std::runtime_error, and a root element other than
+ * <robot>, for which the reference returns false) give CSD_ERR_INVALID with
+ * the message in csd_last_error(). No device is used. */
+typedef struct csd_urdf_s* csd_urdf_t;
+csd_status_t csd_urdf_create(csd_urdf_t* out);
+csd_status_t csd_urdf_destroy(csd_urdf_t h);
+/* registered (optional) = 0 when name or path is empty or path does not exist. */
+csd_status_t csd_urdf_register_package(csd_urdf_t h, const char* name, const char* path, int32_t* registered);
+csd_status_t csd_urdf_parse_file(csd_urdf_t h, const char* path);
+csd_status_t csd_urdf_parse_string(csd_urdf_t h, const char* urdf_text);
+/* Model directives (add_model, add_weld, add_frame; package:// paths). */
+csd_status_t csd_urdf_parse_directives(csd_urdf_t h, const char* path);
+/* The parsed MinimalPlant; the pointers stay valid until csd_urdf_destroy and
+ * can be passed straight to csd_plant_create. */
+csd_status_t csd_urdf_plant_desc(csd_urdf_t h, csd_plant_desc_t* desc);
+/* lower/upper: num_configuration_variables floats each. */
+csd_status_t csd_urdf_limits(csd_urdf_t h, float* lower, float* upper);
+/* Geometries of the ROBOT group (pointer owned by the handle). */
+csd_status_t csd_urdf_robot_geometry_ids(csd_urdf_t h, const int32_t** ids, int32_t* n);
+csd_status_t csd_urdf_link_index(csd_urdf_t h, const char* name, int32_t* index);
+/* scene_collision_geometry_name_to_geometry_index ("<collision name>::<k>" or
+ * "<link>::col_geom::<k>", k counting the link's collisions from 1). */
+csd_status_t csd_urdf_geometry_index(csd_urdf_t h, const char* name, int32_t* index);
 
 /* Uploads a plant once (device-resident, reusable across calls). Replaces the
  * per-call CudaPtr<const MinimalPlant> upload of checkCollisionFreeCuda,
@@ -304,6 +333,38 @@ csd_status_t csd_eizo_noalloc(csd_plant_t plant, const float* line_start, const 
                               float* A_out, float* b_out, int32_t* num_faces, csd_eizo_iteration_info_t* info,
                               int32_t info_capacity, int32_t* num_iterations, void* stream);
 
+/* EditRegionsOptions, csdecomp/src/planning/cuda_edit_regions.h:12-16
+ * (defaults 0.01, 9; verbose printing is left to the caller). */
+typedef struct {
+  float configuration_margin;
+  uint32_t bisection_steps;
+} csd_edit_regions_options_t;
+
+/* Region editing: EditRegionsCuda, csdecomp/src/planning/cuda_edit_regions.cu:44-301
+ * (pybind cuda_bindings.h:140-179). Collision i ([n][dim]) belongs to segment
+ * line_segment_idxs[i] < m; segment r runs from line_starts[r] to
+ * line_ends[r] ([m][dim]) and lies in region r, rows
+ * [face_offsets[r], face_offsets[r+1]) of A ([F][dim] row-major) and b. Each
+ * collision is bisected towards its projection on its segment
+ * (bisection_steps fused FK + checks, voxels as in csd_check_points); per
+ * region a face is placed for each optimized collision, nearest first, that
+ * lies strictly inside the region edited so far, relaxed so the segment stays
+ * inside. A_out/b_out hold face_offsets[m] + n rows: region r is written at
+ * row face_offsets[r] + (collisions of segments < r), num_faces[r] rows (the
+ * original faces first); other rows are unspecified. projections and
+ * optimized_collisions ([n][dim]) come back grouped by segment, in the given
+ * order within a segment, as the reference returns them. Errors: endpoints
+ * outside their region (CSD_ERR_NOT_CONTAINED), n = 0, a segment index out of
+ * range, no robot geometry ids or voxel_radius <= 0 (CSD_ERR_INVALID), more
+ * than 10000 voxels (CSD_ERR_CAPACITY). Host arrays; synchronous. */
+csd_status_t csd_edit_regions(csd_plant_t plant, const float* collisions, const uint32_t* line_segment_idxs,
+                              int64_t n, const float* line_starts, const float* line_ends, int32_t m,
+                              const float* A, const float* b, const int32_t* face_offsets, const float* voxels,
+                              int32_t num_voxels, float voxel_radius, const int32_t* robot_geometry_ids,
+                              int32_t num_robot_geometries, const csd_edit_regions_options_t* options,
+                              float* A_out, float* b_out, int32_t* num_faces, float* projections,
+                              float* optimized_collisions);
+
 /* numSamplesUnadaptive, csdecomp/src/planning/cuda_set_builder_utils.h:198-203. */
 uint32_t csd_num_samples_unadaptive(float epsilon, float delta, float tau);
 
@@ -319,6 +380,14 @@ csd_status_t csd_fp32_fma_probe(int64_t iters, double* flops, double* seconds);
  * csd_plant_flops counts). Takes effect for later calls and for batches
  * created afterwards. */
 csd_status_t csd_plant_set_culling(csd_plant_t plant, int32_t enable);
+/* Voxel hash grid of the voxel checks (csd_check_points with voxels, csd_eizo
+ * and csd_inflator_inflate with voxels, csd_edit_regions; the reference tests
+ * every robot geometry against every voxel, cuda_collision_checker.cu:374-435):
+ * per call the voxels are bucketed on the device by a spatial hash of their
+ * cells, and each robot geometry tests only the voxels in the cells its
+ * bounding sphere touches. Used for 64 voxels or more; verdicts are
+ * unchanged. On by default; enable = 0 tests every voxel. */
+csd_status_t csd_plant_set_voxel_grid(csd_plant_t plant, int32_t enable);
 
 /* Algorithmic FP32 work of checking one configuration of this plant without
  * early exit: forward kinematics, geometry placement and all pair tests

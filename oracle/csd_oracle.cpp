@@ -1031,4 +1031,133 @@ int orc_eizo(const orc_plant_t* p, const float* ls, const float* le, const float
   return 0;
 }
 
+// EditRegionsCuda, cuda_edit_regions.cu:44-301. Collisions are grouped by
+// segment in a stable counting order (:85-107); each is projected onto its
+// segment (cuda_set_builder_utils.cu:25-67, the projection kernel called at
+// :177), bisected towards the projection (:196-225) and measured against it
+// (:227-230). Per region the candidates are visited in ascending distance
+// (:239-241, std::sort there; equal distances here keep their group order)
+// and a face is added for each one that lies strictly inside the region as
+// edited so far (:253-259), with the segment relaxation of :262-272.
+// Region r's faces are written at row face_offsets[r] + (collisions of the
+// segments before r); projections and optimized collisions come out in the
+// grouped order. Dot products are accumulated in coordinate order with
+// fused multiply-adds. A non-NULL checker replaces the oracle's own point
+// check (GPU contact rule). Returns 0, -1 for a dimension above 16, -2 for a
+// segment index out of range, -3 if the point check fails.
+int orc_edit_regions(const orc_plant_t* p, const float* collisions, const uint32_t* seg, int64_t n,
+                     const float* starts, const float* ends, int32_t m, const float* A, const float* b,
+                     const int32_t* face_offsets, const float* voxels, int32_t nv, float vr,
+                     const int32_t* rids, int32_t nr, float margin, uint32_t steps, float* A_out,
+                     float* b_out, int32_t* num_faces, float* proj_out, float* opt_out,
+                     orc_checker_fn checker, void* ctx, int nthreads) {
+  const int d = p->num_configuration_variables;
+  if (d > 16) return -1;
+  set_threads(nthreads);
+  for (int64_t i = 0; i < n; ++i)
+    if (seg[i] >= (uint32_t)m) return -2;
+  // stable grouping by segment
+  std::vector<int64_t> coff(m + 1, 0);
+  for (int64_t i = 0; i < n; ++i) ++coff[seg[i] + 1];
+  for (int r = 0; r < m; ++r) coff[r + 1] += coff[r];
+  std::vector<int64_t> fill(coff.begin(), coff.end() - 1);
+  std::vector<float> cols((size_t)n * d), proj((size_t)n * d), lo, hi, mid((size_t)n * d);
+  std::vector<uint32_t> gseg(n);
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t j = fill[seg[i]]++;
+    std::memcpy(&cols[(size_t)j * d], collisions + (size_t)i * d, sizeof(float) * d);
+    gseg[j] = seg[i];
+  }
+  for (int64_t i = 0; i < n; ++i) {
+    const float* ls = starts + (size_t)gseg[i] * d;
+    const float* le = ends + (size_t)gseg[i] * d;
+    const float* c = &cols[(size_t)i * d];
+    float seg2 = 0.f, a = 0.f;
+    for (int k = 0; k < d; ++k) {
+      seg2 = std::fmaf(le[k] - ls[k], le[k] - ls[k], seg2);
+      a = std::fmaf(c[k] - ls[k], le[k] - ls[k], a);
+    }
+    float t = std::fmin(std::fmax(a / seg2, 0.0f), 1.0f);
+    for (int k = 0; k < d; ++k) proj[(size_t)i * d + k] = std::fmaf(t, le[k], (1.0f - t) * ls[k]);
+  }
+  lo = proj;
+  hi = cols;
+  std::vector<uint8_t> flags(n);
+  for (uint32_t s = 0; s < steps; ++s) {
+    for (size_t j = 0; j < (size_t)n * d; ++j) mid[j] = 0.5f * (lo[j] + hi[j]);
+    const int rc = checker ? checker(mid.data(), n, flags.data(), ctx)
+                           : orc_check_points(p, mid.data(), n, ORC_RULE_GPU, voxels, nv, vr, rids, nr,
+                                              flags.data(), nthreads);
+    if (rc) return -3;
+    for (int64_t i = 0; i < n; ++i) {
+      float* dst = flags[i] ? lo.data() : hi.data();
+      std::memcpy(dst + (size_t)i * d, &mid[(size_t)i * d], sizeof(float) * d);
+      if (!flags[i]) std::memcpy(&cols[(size_t)i * d], &mid[(size_t)i * d], sizeof(float) * d);
+    }
+  }
+  std::vector<float> dist(n);
+  for (int64_t i = 0; i < n; ++i) {
+    float s2 = 0.f;
+    for (int k = 0; k < d; ++k) {
+      float x = cols[(size_t)i * d + k] - proj[(size_t)i * d + k];
+      s2 = std::fmaf(x, x, s2);
+    }
+    dist[i] = std::sqrt(s2);
+  }
+  std::memcpy(proj_out, proj.data(), sizeof(float) * n * d);
+  std::memcpy(opt_out, cols.data(), sizeof(float) * n * d);
+  for (int r = 0; r < m; ++r) {
+    const int64_t F0 = face_offsets[r + 1] - face_offsets[r];
+    const int64_t row0 = face_offsets[r] + coff[r];
+    float* Ao = A_out + (size_t)row0 * d;
+    float* bo = b_out + row0;
+    std::memcpy(Ao, A + (size_t)face_offsets[r] * d, sizeof(float) * F0 * d);
+    std::memcpy(bo, b + face_offsets[r], sizeof(float) * F0);
+    int64_t F = F0;
+    std::vector<int64_t> order;
+    for (int64_t i = coff[r]; i < coff[r + 1]; ++i)
+      if (dist[i] < FLT_MAX) order.push_back(i);
+    std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) { return dist[x] < dist[y]; });
+    const float* ls = starts + (size_t)r * d;
+    const float* le = ends + (size_t)r * d;
+    for (int64_t i : order) {
+      const float* c = &cols[(size_t)i * d];
+      bool inside = true;
+      for (int64_t f = 0; f < F && inside; ++f) {
+        float v = 0.f;
+        for (int k = 0; k < d; ++k) v = std::fmaf(Ao[(size_t)f * d + k], c[k], v);
+        if (!(v - bo[f] < 0.f)) inside = false;
+      }
+      if (!inside) continue;
+      const float* pr = &proj[(size_t)i * d];
+      float a[16];
+      float n2 = 0.f;
+      for (int k = 0; k < d; ++k) {
+        a[k] = c[k] - pr[k];
+        n2 = std::fmaf(a[k], a[k], n2);
+      }
+      if (n2 > 0.f) {
+        float nrm = std::sqrt(n2);
+        for (int k = 0; k < d; ++k) a[k] = a[k] / nrm;
+      }
+      float bb = 0.f, v1 = 0.f, v2 = 0.f;
+      for (int k = 0; k < d; ++k) {
+        bb = std::fmaf(a[k], c[k], bb);
+        v1 = std::fmaf(a[k], ls[k], v1);
+        v2 = std::fmaf(a[k], le[k], v2);
+      }
+      bb = bb - margin;
+      v1 = v1 - bb;
+      v2 = v2 - bb;
+      float relax = std::max(v1, v2);
+      if (relax > 0) bb = (float)((double)bb + ((double)relax + 2e-6));
+      for (int k = 0; k < d; ++k) Ao[(size_t)F * d + k] = a[k];
+      bo[F] = bb;
+      ++F;
+    }
+    num_faces[r] = (int32_t)F;
+  }
+  return 0;
+}
+
 }  // extern "C"

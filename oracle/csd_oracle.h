@@ -15,6 +15,7 @@
  *   hit-and-run             csdecomp/src/geometry/cuda_hit_and_run_sampling.cu:18-119
  *   EI-ZO loop              csdecomp/src/planning/cuda_edge_inflation_zero_order.cu:94-339
  *                           csdecomp/src/planning/cuda_set_builder_utils.cu:25-455
+ *   region editing          csdecomp/src/planning/cuda_edit_regions.cu:44-301
  *
  * Capsules have no reference semantics (the reference throws on them); the
  * oracle defines them in FP64 as sphere-swept segments along the local z axis.
@@ -147,6 +148,22 @@ int orc_eizo(const orc_plant_t* p, const float* line_start, const float* line_en
 
 /* numSamplesUnadaptive, csdecomp/src/planning/cuda_set_builder_utils.h:198-203 */
 uint32_t orc_num_samples_unadaptive(float epsilon, float delta, float tau);
+
+/* EditRegionsCuda, csdecomp/src/planning/cuda_edit_regions.cu:44-301.
+ * collisions [n][d] with their segment indices; starts/ends [m][d]; region r
+ * is rows [face_offsets[r], face_offsets[r+1]) of A (row-major) and b. Region
+ * r comes back at row face_offsets[r] + (collisions of segments < r) of
+ * A_out/b_out with num_faces[r] rows; proj_out/opt_out are [n][d] in the
+ * grouped (segment-stable) order. checker (may be NULL) replaces the
+ * oracle's own point check. Returns 0, -1 dim > 16, -2 segment index out of
+ * range, -3 point check failed. */
+int orc_edit_regions(const orc_plant_t* p, const float* collisions, const uint32_t* seg, int64_t n,
+                     const float* starts, const float* ends, int32_t m, const float* A, const float* b,
+                     const int32_t* face_offsets, const float* voxels, int32_t nv, float vr,
+                     const int32_t* robot_geom_ids, int32_t num_robot_geoms, float margin,
+                     uint32_t bisection_steps, float* A_out, float* b_out, int32_t* num_faces,
+                     float* proj_out, float* opt_out, orc_checker_fn checker, void* checker_ctx,
+                     int nthreads);
 
 int orc_max_threads(void);
 

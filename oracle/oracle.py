@@ -291,3 +291,66 @@ def eizo(plant, line_start, line_end, A_domain, b_domain, options, robot_geometr
         raise RuntimeError(f"oracle eizo failed ({rc})")
     recs = [dict((k, getattr(iters[i], k)) for k, _ in OrcEizoIter._fields_) for i in range(nit.value)]
     return A[:nf.value].copy(), b[:nf.value].copy(), recs
+
+
+def _checker_cb(checker, d):
+    if checker is None:
+        return None
+
+    def _cb(qp, n, outp, ctx):
+        try:
+            qa = np.ctypeslib.as_array(ctypes.cast(qp, ctypes.POINTER(ctypes.c_float)), shape=(n * d,))
+            res = np.asarray(checker(qa.reshape(n, d).copy()), np.uint8)
+            oa = np.ctypeslib.as_array(ctypes.cast(outp, ctypes.POINTER(ctypes.c_uint8)), shape=(n,))
+            oa[:] = res
+            return 0
+        except Exception:  # pragma: no cover - surfaced as an error code
+            return 1
+    return CHECKER_FN(_cb)
+
+
+def edit_regions(plant, collisions, line_segment_idxs, starts, ends, regions, robot_geometry_ids=(), voxels=None,
+                 voxel_radius: float = 0.0, configuration_margin: float = 0.01, bisection_steps: int = 9,
+                 checker=None, nthreads: int = 0):
+    """CPU EditRegionsCuda (cuda_edit_regions.cu:44-301). collisions [n][d]
+    with one segment index each; starts/ends [m][d]; regions a list of (A, b).
+    ``checker(q[n,d]) -> uint8[n]`` replaces the oracle's own point check when
+    given. Returns ([(A, b)] per region, projections [n][d], optimized [n][d]),
+    the last two in the grouped (segment-stable) order the reference returns."""
+    pv = PlantView(plant)
+    d = pv.dim
+    c = np.ascontiguousarray(np.asarray(collisions, np.float32).reshape(-1, d))
+    n = c.shape[0]
+    seg = np.ascontiguousarray(np.asarray(line_segment_idxs, np.uint32).reshape(-1))
+    ls = np.ascontiguousarray(np.asarray(starts, np.float32).reshape(-1, d))
+    le = np.ascontiguousarray(np.asarray(ends, np.float32).reshape(-1, d))
+    m = ls.shape[0]
+    A = np.ascontiguousarray(np.concatenate([np.asarray(a, np.float32).reshape(-1, d) for a, _ in regions]))
+    b = np.ascontiguousarray(np.concatenate([np.asarray(bb, np.float32).reshape(-1) for _, bb in regions]))
+    off = np.zeros(m + 1, np.int32)
+    off[1:] = np.cumsum([np.asarray(bb).size for _, bb in regions])
+    cap = int(off[-1]) + n
+    A_out = np.zeros((max(cap, 1), d), np.float32)
+    b_out = np.zeros(max(cap, 1), np.float32)
+    nf = np.zeros(m, np.int32)
+    proj = np.zeros((max(n, 1), d), np.float32)
+    opt = np.zeros((max(n, 1), d), np.float32)
+    if voxels is not None and len(voxels):
+        v = np.ascontiguousarray(np.asarray(voxels, np.float32).reshape(-1, 3))
+    else:
+        v = None
+    r = np.ascontiguousarray(np.asarray(robot_geometry_ids, np.int32).reshape(-1))
+    rc = lib().orc_edit_regions(pv.ref, _ptr(c), _ptr(seg), ctypes.c_int64(n), _ptr(ls), _ptr(le), m, _ptr(A),
+                                _ptr(b), _ptr(off), _ptr(v), 0 if v is None else v.shape[0],
+                                ctypes.c_float(voxel_radius), _ptr(r), r.size, ctypes.c_float(configuration_margin),
+                                ctypes.c_uint32(bisection_steps), _ptr(A_out), _ptr(b_out), _ptr(nf), _ptr(proj),
+                                _ptr(opt), _checker_cb(checker, d), None, nthreads)
+    if rc:
+        raise RuntimeError(f"oracle edit_regions failed ({rc})")
+    counts = np.bincount(seg, minlength=m) if n else np.zeros(m, np.int64)
+    coff = np.concatenate([[0], np.cumsum(counts)])
+    out = []
+    for i in range(m):
+        row = int(off[i] + coff[i])
+        out.append((A_out[row:row + nf[i]].copy(), b_out[row:row + nf[i]].copy()))
+    return out, proj[:n].copy(), opt[:n].copy()

@@ -156,7 +156,21 @@ def main(ref: str) -> None:
         ],
         "eizo_throws": {"src": "csdecomp/src/planning/tests/edge_inflation_zero_order_test.cpp:175-196",
                         "num_particles_too_many": 1000000, "domain_faces": 4000},
+        # the test's inline URDF is the one of edge_inflation_zero_order_test.cpp (checked below)
+        "edit_regions_2d": {"src": "csdecomp/src/planning/tests/cuda_edit_regions_test.cpp:79-227",
+                            "plant": "boxes_in_corners", "configuration_margin": 0.01, "bisection_steps": 9,
+                            "voxels": [[-0.55, 2.02, 0.0], [-1.50, 1.80, 0.0], [1.90, 1.90, 0.0]],
+                            "voxel_radius": 0.05,
+                            "starts": [[-1.90, 0.00], [0.00, 0.00], [0.00, 1.80]],
+                            "ends": [[0.00, 0.00], [0.00, 1.80], [1.90, 1.80]],
+                            "collisions": [[-0.9, 1.0], [0.6, 0.5], [1.1, -1.0], [1.9, 1.9]],
+                            "repeats": 3,
+                            "unbisected_steps": 1, "unbisected_col": 1, "unbisected_tol": 1e-6},
     }
+    if raw_urdf_from_test(os.path.join(ref, "csdecomp", "src", "planning", "tests", "cuda_edit_regions_test.cpp")) != \
+            raw_urdf_from_test(os.path.join(ref, "csdecomp", "src", "planning", "tests",
+                                            "edge_inflation_zero_order_test.cpp")):
+        raise RuntimeError("cuda_edit_regions_test.cpp no longer uses the boxes_in_corners URDF")
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(golden, f, indent=1)
     print("wrote", os.path.join(HERE, "plants.npz"), "and golden.json")
