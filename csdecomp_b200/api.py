@@ -571,7 +571,9 @@ class BatchedEdgeInflator:
     CudaEdgeInflator.inflateEdge would for the same inputs (no voxels)."""
 
     SAMPLE_VARIANTS = ("1 face/trip, 2 blocks/SM", "2 faces/trip, 2 blocks/SM", "1 face/trip, 3 blocks/SM",
-                       "2 faces/trip, 3 blocks/SM", "4 faces/trip, 2 blocks/SM", "4 faces/trip, 3 blocks/SM")
+                       "2 faces/trip, 3 blocks/SM", "4 faces/trip, 2 blocks/SM", "4 faces/trip, 3 blocks/SM",
+                       "1 packed face pair/trip, 2 blocks/SM", "2 packed face pairs/trip, 2 blocks/SM",
+                       "1 packed face pair/trip, 3 blocks/SM", "2 packed face pairs/trip, 3 blocks/SM")
     CHECK_ITEM_CAPS = (32, 128, 512)
 
     def __init__(self, plants: Sequence[MinimalPlant], options: EizoOptions, max_slots: int,
@@ -614,7 +616,7 @@ class BatchedEdgeInflator:
 
     def tuning(self) -> dict:
         sv, cap, nv = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
-        ms = np.zeros(16, np.float32)
+        ms = np.zeros(64, np.float32)
         C.check(C.lib().csd_batch_tuning(self._handle, ctypes.byref(sv), ctypes.byref(cap), C.ptr(ms),
                                          ctypes.byref(nv)))
         ns = len(self.SAMPLE_VARIANTS)

@@ -118,7 +118,7 @@ static __device__ __forceinline__ int item_size(int64_t total, int cap, int nw) 
 // takes a contiguous run of items, stages each new slot's region (At, b) in
 // shared memory and runs its chains G lanes per chain (G from the total
 // chain count: 8 when the batch is full, up to 32 in the tail).
-template <int U, int MINB>
+template <int U, int MINB, bool PK = false>
 __global__ void __launch_bounds__(256, MINB) batch_sample_kernel(BatchArgs a) {
   extern __shared__ __align__(16) float smf[];  // the face loop reads float2/float4 vectors
   const int N = a.n_tab[a.it->k];
@@ -151,9 +151,9 @@ __global__ void __launch_bounds__(256, MINB) batch_sample_kernel(BatchArgs a) {
       staged = slot;
     }
     if (dim <= 8)
-      sample_range<8, U>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, G, smf, fits);
+      sample_range<8, U, PK>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, G, smf, fits);
     else
-      sample_range<16, U>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, G, smf, fits);
+      sample_range<16, U, PK>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, G, smf, fits);
   }
 }
 
@@ -573,8 +573,8 @@ __global__ void __launch_bounds__(1024) batch_compact_sorted_kernel(BatchArgs a)
   }
 }
 
-// Sampler variants the autotuner chooses from: U faces per lane and trip,
-// MINB resident blocks per SM (register cap).
+// Sampler variants the autotuner chooses from: U faces (packed: U face
+// pairs) per lane and trip, MINB resident blocks per SM (register cap).
 using SampleFn = void (*)(BatchArgs);
 struct SampleVariant {
   SampleFn fn;
@@ -587,6 +587,10 @@ static const SampleVariant kSampleVariants[] = {
     {batch_sample_kernel<2, 3>, 2, 3},
     {batch_sample_kernel<4, 2>, 4, 2},
     {batch_sample_kernel<4, 3>, 4, 3},
+    {batch_sample_kernel<1, 2, true>, 1, 2},
+    {batch_sample_kernel<2, 2, true>, 2, 2},
+    {batch_sample_kernel<1, 3, true>, 1, 3},
+    {batch_sample_kernel<2, 3, true>, 2, 3},
 };
 constexpr int kNumSampleVariants = (int)(sizeof(kSampleVariants) / sizeof(kSampleVariants[0]));
 // Largest check work item (configurations) the autotuner chooses from.
@@ -1147,7 +1151,7 @@ csd_status_t csd_batch_set_surrogate_rounds(csd_batch_t h, int32_t rounds, int32
 csd_status_t csd_batch_set_shapes(csd_batch_t h, int32_t sample_variant, int32_t check_item_cap) {
   CSD_CHECK(h && sample_variant >= 0 && sample_variant < kNumSampleVariants && check_item_cap >= 8 &&
                 check_item_cap % 8 == 0,
-            CSD_ERR_INVALID, "bad shapes: sampler variant in [0, 6), check item cap a positive multiple of 8");
+            CSD_ERR_INVALID, "bad shapes: sampler variant out of range, or check item cap not a positive multiple of 8");
   h->sample_variant = sample_variant;
   h->cfg_max = check_item_cap;
   return CSD_OK;

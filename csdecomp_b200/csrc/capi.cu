@@ -89,6 +89,12 @@ csd_status_t csd_check_points(csd_plant_t p, const float* q, int64_t n, const fl
   VoxelTables vt;
   csd_status_t s;
   if (nv > 0 && nr > 0) {
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, robot_ids) == cudaSuccess && pa.type == cudaMemoryTypeDevice) {
+      set_error("robot_geometry_ids must be host memory (they are read on the host)");
+      return CSD_ERR_INVALID;
+    }
+    cudaGetLastError();  // an unregistered host pointer is not an error here
     std::vector<uint32_t> tab;
     int no = 0;
     if ((s = build_voxel_tables(p, robot_ids, nr, &tab, &no))) return s;

@@ -152,6 +152,150 @@ __device__ __forceinline__ bool run_chain_group(const float* __restrict__ At, in
   return ok;
 }
 
+// ---- packed FP32 pairs (sm_100 f32x2): each half is an IEEE round-to-nearest
+// operation, so a packed result is bit for bit the two scalar results.
+__device__ __forceinline__ uint64_t f2_pack(float lo, float hi) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(uint64_t v, float* lo, float* hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(*lo), "=f"(*hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t f2_mul(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t f2_sub(uint64_t a, uint64_t b) {
+  uint64_t d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
+// run_chain_group over a staged polytope (row stride ST, even; 8-byte aligned
+// rows) with faces taken in adjacent pairs (f, f + 1), f even: one 64-bit
+// shared-memory load brings coordinate k of both faces, and one packed FMA
+// per dot product advances both. The configuration and the direction are
+// kept duplicated in both halves ((x_k, x_k), (d_k, d_k)) so they pair with
+// any face pair. Per face the operations and their order are those of
+// run_chain_group (product, FMAs in coordinate order, b - A x, division), and
+// the theta bounds are order-independent reductions, so the chain ends bit
+// for bit where run_chain ends. U pairs per lane and trip.
+template <int MAXD, int G, int ST, int U>
+__device__ __forceinline__ bool run_chain_group_x2(const float* __restrict__ At, const float* __restrict__ bp, int F,
+                                                   int dim, int mixing, uint32_t k0, uint32_t k1, uint32_t chain,
+                                                   uint32_t stream, float* x, int gl) {
+  static_assert(ST > 0 && ST % 2 == 0, "packed faces need an even staged stride");
+  constexpr int R = (MAXD / 2 + 1 + G - 1) / G;
+  const int npairs = (dim + 1) >> 1;
+  uint64_t xx[MAXD];
+#pragma unroll
+  for (int k = 0; k < MAXD; ++k) xx[k] = f2_pack(x[k], x[k]);
+  bool ok = true;
+  for (int step = 0; step < mixing; ++step) {
+    float c0[R], c1[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      c0[r] = 0.f;
+      c1[r] = 0.f;
+      const int job = gl + r * G;
+      if (job <= npairs) {
+        const int word = 2 * job;
+        uint32_t w[4];
+        philox4x32_10((uint32_t)step, chain, stream, (uint32_t)(word >> 2), k0, k1, w);
+        const uint32_t wa = (word & 2) ? w[2] : w[0];
+        const uint32_t wb = (word & 2) ? w[3] : w[1];
+        if (job < npairs) {
+          float u = u01_open0(wa);
+          float v = u01_open1(wb);
+          float rad = __fsqrt_rn(__fmul_rn(-2.0f, log_unit(u)));
+          float sn, cs;
+          sincos_2pi(v, &sn, &cs);
+          c0[r] = __fmul_rn(rad, cs);
+          c1[r] = __fmul_rn(rad, sn);
+        } else {
+          c0[r] = u01_open0(wa);
+        }
+      }
+    }
+    uint64_t dd[MAXD];
+#pragma unroll
+    for (int k = 0; k < MAXD; ++k) {
+      const int p = k >> 1;
+      const float dk = __shfl_sync(0xffffffffu, (k & 1) ? c1[p / G] : c0[p / G], p % G, G);
+      dd[k] = f2_pack(dk, dk);
+    }
+    float utv = c0[0];
+#pragma unroll
+    for (int r = 1; r < R; ++r)
+      if (npairs / G == r) utv = c0[r];
+    const float ut = __shfl_sync(0xffffffffu, utv, npairs % G, G);
+    float tmax = FLT_MAX, tmin = -FLT_MAX;
+    for (int f0 = 2 * gl; f0 < F; f0 += 2 * G * U) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int f = f0 + 2 * G * u;
+        if (U == 1 || f < F) {
+          const float* col = At + f;
+          uint64_t a = *reinterpret_cast<const uint64_t*>(col);
+          uint64_t ax = f2_mul(a, xx[0]);
+          uint64_t ad = f2_mul(a, dd[0]);
+#pragma unroll
+          for (int k = 1; k < MAXD; ++k) {
+            if (k < dim) {
+              a = *reinterpret_cast<const uint64_t*>(col + k * ST);
+              ax = f2_fma(a, xx[k], ax);
+              ad = f2_fma(a, dd[k], ad);
+            }
+          }
+          const uint64_t lb2 = f2_sub(*reinterpret_cast<const uint64_t*>(bp + f), ax);
+          float lb0, lb1, ad0, ad1;
+          f2_unpack(lb2, &lb0, &lb1);
+          f2_unpack(ad, &ad0, &ad1);
+          if (ad0 < 0.0f)
+            tmin = fmaxf(tmin, __fdiv_rn(lb0, ad0));
+          else if (ad0 > 0.0f)
+            tmax = fminf(tmax, __fdiv_rn(lb0, ad0));
+          if (f + 1 < F) {  // the pair's second face (row entries past F are never used)
+            if (ad1 < 0.0f)
+              tmin = fmaxf(tmin, __fdiv_rn(lb1, ad1));
+            else if (ad1 > 0.0f)
+              tmax = fminf(tmax, __fdiv_rn(lb1, ad1));
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int o = G / 2; o; o >>= 1) {
+      tmin = fmaxf(tmin, __shfl_xor_sync(0xffffffffu, tmin, o, G));
+      tmax = fminf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o, G));
+    }
+    if (isinf(tmax) || isinf(tmin) || tmax < tmin) ok = false;
+    if (ok) {
+      double th = __dadd_rn(__dmul_rn((double)ut, __dsub_rn(__dmul_rn(0.999999, (double)tmax), (double)tmin)),
+                            (double)tmin);
+      const float theta = __double2float_rn(th);
+      const uint64_t tt = f2_pack(theta, theta);
+#pragma unroll
+      for (int k = 0; k < MAXD; ++k)
+        if (k < dim) xx[k] = f2_fma(tt, dd[k], xx[k]);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < MAXD; ++k) {
+    float lo, hi;
+    f2_unpack(xx[k], &lo, &hi);
+    x[k] = lo;
+  }
+  return ok;
+}
+
 // Writes coordinates gl, gl + G, ... of a group-replicated vector.
 template <int MAXD, int G>
 __device__ __forceinline__ void group_store(const float* x, int dim, int gl, float* __restrict__ dst, bool ok,
@@ -187,7 +331,7 @@ __device__ __forceinline__ void stage_polytope(const float* __restrict__ At, int
 // Chains [first, last) of one polytope by the whole block, G lanes per
 // chain; the trip count is uniform across the block (groups past `last`
 // repeat the last chain and store nothing). A failed chain stores `start`.
-template <int MAXD, int G, int ST, int U>
+template <int MAXD, int G, int ST, int U, bool PK = false>
 __device__ __forceinline__ void sample_chains(const float* __restrict__ At, int ldt, const float* __restrict__ b,
                                               int F, int dim, const float* __restrict__ start, int first, int last,
                                               int mixing, uint32_t k0, uint32_t k1, uint32_t stream,
@@ -201,7 +345,11 @@ __device__ __forceinline__ void sample_chains(const float* __restrict__ At, int 
     float x[MAXD];
 #pragma unroll
     for (int k = 0; k < MAXD; ++k) x[k] = k < dim ? start[k] : 0.f;
-    const bool ok = run_chain_group<MAXD, G, ST, U>(At, ldt, b, F, dim, mixing, k0, k1, (uint32_t)cc, stream, x, gl);
+    bool ok;
+    if constexpr (PK && ST > 0)
+      ok = run_chain_group_x2<MAXD, G, ST, U>(At, b, F, dim, mixing, k0, k1, (uint32_t)cc, stream, x, gl);
+    else
+      ok = run_chain_group<MAXD, G, ST, U>(At, ldt, b, F, dim, mixing, k0, k1, (uint32_t)cc, stream, x, gl);
     if (chain < last) group_store<MAXD, G>(x, dim, gl, out + (int64_t)chain * dim, ok, start);
   }
 }
@@ -214,8 +362,9 @@ __host__ __device__ __forceinline__ int group_width(int64_t total, int64_t grid_
 }
 
 // One polytope's chains [first, last) with the polytope staged in `sm` when
-// it fits (sm_ready: already staged), else read from global memory.
-template <int MAXD, int U>
+// it fits (sm_ready: already staged), else read from global memory. PK: the
+// staged path takes faces in packed pairs (U pairs per trip).
+template <int MAXD, int U, bool PK = false>
 __device__ __forceinline__ void sample_range(const float* __restrict__ At, int ldt, const float* __restrict__ b,
                                              int F, int dim, const float* __restrict__ start, int first, int last,
                                              int mixing, uint32_t k0, uint32_t k1, uint32_t stream,
@@ -225,11 +374,11 @@ __device__ __forceinline__ void sample_range(const float* __restrict__ At, int l
     const float* sAt = sm;
     const float* sb = sm + MAXD * ST;
     if (G == 8)
-      sample_chains<MAXD, 8, ST, U>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
+      sample_chains<MAXD, 8, ST, U, PK>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
     else if (G == 16)
-      sample_chains<MAXD, 16, ST, U>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
+      sample_chains<MAXD, 16, ST, U, PK>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
     else
-      sample_chains<MAXD, 32, ST, U>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
+      sample_chains<MAXD, 32, ST, U, PK>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
   } else {
     if (G == 8)
       sample_chains<MAXD, 8, 0, U>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out);

@@ -26,8 +26,9 @@
   python -m csdecomp_b200.profile_cases voxel_check [--configs N] [--voxels V]
       checkCollisionFreeVoxelsCuda at scale: the config-2 arm (80 spheres + 4
       capsules, 200 world primitives) against V voxels of radius 0.02 m
-      (uniform in a 3 x 3 x 1.5 m box around the arm, none within 0.3 m of its
-      base), N uniform configurations; with and without the voxel hash grid
+      (uniform in a 3 x 3 x 1.5 m box around the arm, none within 0.9 m of its
+      base, so that verdicts are mixed), N uniform configurations; with and
+      without the voxel hash grid
   python -m csdecomp_b200.profile_cases edit_regions [--regions R] [--collisions C]
       EditRegionsCuda on the config-3 scene: R box regions around seed edges,
       C colliding configurations drawn inside each, 9 bisection steps
@@ -213,17 +214,20 @@ def edit_regions(regions: int, per_region: int) -> None:
     lo, hi = sc.lower(), sc.upper()
     doms, cols, segs = [], [], []
     for r, (q0, q1) in enumerate(edges):
-        blo = np.maximum(lo, np.minimum(q0, q1) - 0.4).astype(np.float32)
-        bhi = np.minimum(hi, np.maximum(q0, q1) + 0.4).astype(np.float32)
+        blo = np.maximum(lo, np.minimum(q0, q1) - 1.2).astype(np.float32)
+        bhi = np.minimum(hi, np.maximum(q0, q1) + 1.2).astype(np.float32)
         P = csd.HPolyhedron()
         P.MakeBox(blo, bhi)
         doms.append(P)
         got = np.zeros((0, sc.dim), np.float32)
-        while got.shape[0] < per_region:
-            q = (blo + (bhi - blo) * rng.random((4 * per_region, sc.dim))).astype(np.float32)
+        for _ in range(8):  # bounded: a box may hold few collisions
+            q = (blo + (bhi - blo) * rng.random((16 * per_region, sc.dim))).astype(np.float32)
             got = np.concatenate([got, q[csd.CheckCollisionFreeCuda(q.T, sc.plant) == 0]])
-        cols.append(got[:per_region])
-        segs.append(np.full(per_region, r))
+            if got.shape[0] >= per_region:
+                break
+        got = got[:per_region]
+        cols.append(got)
+        segs.append(np.full(got.shape[0], r))
     col = np.concatenate(cols).T
     seg = np.concatenate(segs)
     ls = np.stack([e[0] for e in edges], 1).astype(np.float32)
@@ -246,7 +250,7 @@ def voxel_scene(voxels: int, seed: int = 17):
     v = np.zeros((0, 3), np.float32)
     while v.shape[0] < voxels:
         c = rng.uniform([-1.5, -1.5, 0.0], [1.5, 1.5, 1.5], (2 * voxels, 3)).astype(np.float32)
-        v = np.concatenate([v, c[np.linalg.norm(c, axis=1) > 0.3]])
+        v = np.concatenate([v, c[np.linalg.norm(c, axis=1) > 0.9]])
     return sc, np.ascontiguousarray(v[:voxels]), 0.02, sc.inspector.robot_geometry_ids
 
 
@@ -258,13 +262,13 @@ def voxel_check(n: int, voxels: int) -> None:
     h = csd.plant_handle(sc.plant)
     q = torch.from_numpy(np.ascontiguousarray(sc.random_configs(n, 5))).cuda()
     vd = torch.from_numpy(vox).cuda()
-    ids = torch.tensor(list(rids), dtype=torch.int32).cuda()
+    ids = np.ascontiguousarray(np.asarray(list(rids), np.int32))  # robot ids are host memory
     out = torch.zeros(n, dtype=torch.uint8, device="cuda")
     st = torch.cuda.current_stream()
 
     def run():
         C.check(C.lib().csd_check_points(h.handle, C.ptr(q.data_ptr()), ctypes.c_int64(n), C.ptr(vd.data_ptr()),
-                                         voxels, ctypes.c_float(vr), C.ptr(ids.data_ptr()), len(rids),
+                                         voxels, ctypes.c_float(vr), C.ptr(ids), len(rids),
                                          C.ptr(out.data_ptr()), C.CSD_PTR_DEVICE, ctypes.c_void_p(st.cuda_stream)))
     res = {}
     for grid in (True, False):

@@ -140,7 +140,8 @@ csd_status_t csd_fk(csd_plant_t plant, const float* q, int64_t n, float* transfo
  * and with voxels (num_voxels > 0) checkCollisionFreeVoxelsCuda, :374-435
  * (device-pointer forms: executeCollisionFreeKernel :182-209,
  * executeCollisionFreeVoxelsKernel :256-307). voxels: [V][3] world positions of
- * voxel spheres of radius voxel_radius, checked against robot_geometry_ids. */
+ * voxel spheres of radius voxel_radius, checked against robot_geometry_ids
+ * (always host memory, whatever `flags` says; a device pointer is refused). */
 csd_status_t csd_check_points(csd_plant_t plant, const float* q, int64_t n, const float* voxels,
                               int32_t num_voxels, float voxel_radius, const int32_t* robot_geometry_ids,
                               int32_t num_robot_geometries, uint8_t* free_out, int32_t flags, void* stream);
@@ -272,11 +273,13 @@ csd_status_t csd_batch_set_profiling(csd_batch_t h, int32_t enable);
 csd_status_t csd_batch_stage_ms(csd_batch_t h, float* stage_ms /* [8] */);
 /* Autotuner: during the first `iterations` iterations of the next
  * csd_batch_inflate, every sampler variant (faces per lane and trip x
- * resident blocks per SM: [1x2, 2x2, 1x3, 2x3, 4x2, 4x3]) and every check work-item
- * cap ([32, 128, 512] configurations) is timed on that iteration's own
- * inputs; the fastest of each is kept for the graph and later calls.
- * csd_batch_tuning reports the choice and the summed time of each variant
- * (variant_ms: 6 sampler entries, then 3 check entries). */
+ * resident blocks per SM: [1x2, 2x2, 1x3, 2x3, 4x2, 4x3], then packed face
+ * pairs (two faces per 64-bit load and per f32x2 FMA) per lane and trip x
+ * blocks per SM: [1x2, 2x2, 1x3, 2x3]) and every check work-item cap ([32,
+ * 128, 512] configurations) is timed on that iteration's own inputs; the
+ * fastest of each is kept for the graph and later calls. All variants give
+ * identical samples. csd_batch_tuning reports the choice and the summed time
+ * of each variant (variant_ms: 10 sampler entries, then 3 check entries). */
 csd_status_t csd_batch_autotune(csd_batch_t h, int32_t iterations);
 /* Surrogate-guided checking (mlp: one net per plant of the batch, same
  * dimensions; NULL turns it off). Each iteration then scores every sample

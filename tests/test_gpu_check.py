@@ -153,6 +153,24 @@ def test_voxel_grid_matches_every_voxel(plants, case):
     band_parity(plant, q[:1500], vox, vr, rids)
 
 
+def test_device_robot_ids_refused(plants):
+    """csd_check_points reads robot_geometry_ids on the host: a device pointer
+    there is refused with CSD_ERR_INVALID, not dereferenced."""
+    import ctypes
+    import torch
+    from csdecomp_b200 import _capi as C
+    gp = plants["movable_block"]
+    h = csd.plant_handle(gp.plant)
+    q = torch.zeros((4, gp.dim), dtype=torch.float32, device="cuda")
+    vox = torch.zeros((100, 3), dtype=torch.float32, device="cuda")
+    ids = torch.tensor(gp.robot_geometry_ids, dtype=torch.int32, device="cuda")
+    out = torch.zeros(4, dtype=torch.uint8, device="cuda")
+    rc = C.lib().csd_check_points(h.handle, C.ptr(q.data_ptr()), ctypes.c_int64(4), C.ptr(vox.data_ptr()), 100,
+                                  ctypes.c_float(0.01), C.ptr(ids.data_ptr()), ids.numel(), C.ptr(out.data_ptr()),
+                                  C.CSD_PTR_DEVICE, None)
+    assert rc == C.CSD_ERR_INVALID
+
+
 def test_empty_batch():
     sc = scenes.point_check_scene()
     assert csd.CheckCollisionFreeCuda(np.zeros((7, 0), np.float32), sc.plant).shape == (0,)
