@@ -591,6 +591,8 @@ static const SampleVariant kSampleVariants[] = {
     {batch_sample_kernel<2, 2, true>, 2, 2},
     {batch_sample_kernel<1, 3, true>, 1, 3},
     {batch_sample_kernel<2, 3, true>, 2, 3},
+    {batch_sample_kernel<1, 4>, 1, 4},
+    {batch_sample_kernel<2, 4>, 2, 4},
 };
 constexpr int kNumSampleVariants = (int)(sizeof(kSampleVariants) / sizeof(kSampleVariants[0]));
 // Largest check work item (configurations) the autotuner chooses from.

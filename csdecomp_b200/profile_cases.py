@@ -5,7 +5,7 @@
       configurations of the 7-DOF arm (80 spheres + 4 capsules) in 200 world
       primitives (with --no-cull every pair is evaluated: the full sweep)
   python -m csdecomp_b200.profile_cases batch [--slots S] [--iterations I]
-      [--sample-variant V] [--check-item-cap C]
+      [--sample-variant V] [--check-item-cap C] [--per-iteration]
       S inflations of the batched EI-ZO workload (first S scenes), at most I
       iterations, launched stage by stage (profiling mode) with the given
       sampler variant and check work-item cap (defaults: the shapes the
@@ -73,7 +73,7 @@ def check_points(n: int, cull: bool = True) -> None:
                       "flop_per_config": h.flops()["total"], "launch_ms": ms[-1]}))
 
 
-def batch(slots: int, iterations: int, sample_variant: int, check_item_cap: int) -> None:
+def batch(slots: int, iterations: int, sample_variant: int, check_item_cap: int, per_iteration: bool = False) -> None:
     import csdecomp_b200 as csd
     from csdecomp_b200 import scenes
     eizo = dict(num_particles=2000, mixing_steps=50, bisection_steps=9, max_hyperplanes_per_iteration=10,
@@ -99,8 +99,12 @@ def batch(slots: int, iterations: int, sample_variant: int, check_item_cap: int)
     b.set_shapes(sample_variant, check_item_cap)
     b.set_profiling(True)
     b.inflate(list(range(len(scs))), [e[0] for e in edges], [e[1] for e in edges], doms)
-    print(json.dumps({"case": "batch", "slots": len(scs), "stage_ms": b.stage_ms(),
-                      "iterations": b.last_iterations.tolist()}))
+    out = {"case": "batch", "slots": len(scs), "stage_ms": b.stage_ms(), "iterations": b.last_iterations.tolist()}
+    if per_iteration:
+        ms, act = b.iteration_profile()
+        out["per_iteration"] = {"active": act.tolist(), "total_ms": ms.sum(1).round(3).tolist(),
+                                "stages": list(b.STAGES), "stage_ms": ms.round(3).tolist()}
+    print(json.dumps(out))
 
 
 def _timed(fn, reps: int = 3):
@@ -295,6 +299,7 @@ def main() -> None:
     ap.add_argument("--iterations", type=int, default=12)
     ap.add_argument("--sample-variant", type=int, default=3)
     ap.add_argument("--check-item-cap", type=int, default=128)
+    ap.add_argument("--per-iteration", action="store_true", help="batch: stage times and active slots per iteration")
     a = ap.parse_args()
     if a.case == "check_points":
         check_points(a.configs, not a.no_cull)
@@ -311,7 +316,7 @@ def main() -> None:
     elif a.case == "voxel_check":
         voxel_check(a.configs, a.voxels)
     else:
-        batch(a.slots, a.iterations, a.sample_variant, a.check_item_cap)
+        batch(a.slots, a.iterations, a.sample_variant, a.check_item_cap, a.per_iteration)
 
 
 if __name__ == "__main__":

@@ -275,11 +275,12 @@ csd_status_t csd_batch_stage_ms(csd_batch_t h, float* stage_ms /* [8] */);
  * csd_batch_inflate, every sampler variant (faces per lane and trip x
  * resident blocks per SM: [1x2, 2x2, 1x3, 2x3, 4x2, 4x3], then packed face
  * pairs (two faces per 64-bit load and per f32x2 FMA) per lane and trip x
- * blocks per SM: [1x2, 2x2, 1x3, 2x3]) and every check work-item cap ([32,
- * 128, 512] configurations) is timed on that iteration's own inputs; the
- * fastest of each is kept for the graph and later calls. All variants give
- * identical samples. csd_batch_tuning reports the choice and the summed time
- * of each variant (variant_ms: 10 sampler entries, then 3 check entries). */
+ * blocks per SM: [1x2, 2x2, 1x3, 2x3], then unpacked [1x4, 2x4]) and every
+ * check work-item cap ([32, 128, 512] configurations) is timed on that
+ * iteration's own inputs; the fastest of each is kept for the graph and later
+ * calls. All variants give identical samples. csd_batch_tuning reports the
+ * choice and the summed time of each variant (variant_ms: 12 sampler entries,
+ * then 3 check entries). */
 csd_status_t csd_batch_autotune(csd_batch_t h, int32_t iterations);
 /* Surrogate-guided checking (mlp: one net per plant of the batch, same
  * dimensions; NULL turns it off). Each iteration then scores every sample
