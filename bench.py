@@ -371,7 +371,8 @@ def main():
     sampler_roofline = {"bound": "fp32", "achieved": s_flop / (s_ms * 1e-3) / 1e12, "peak": None, "unit": "TFLOP/s",
                         "frac": None, "traffic": None,
                         "kernel": "batch_sample_kernel (hit-and-run, G lanes per chain, faces staged in shared memory; "
-                                  "autotuned variant " + tuned_plain["sample_variant"] + ")",
+                                  "autotuned variant " + tuned_plain["sample_variant"] + "; regions beyond its "
+                                  "staging: " + tuned_plain["large_region_variant"] + ")",
                         "flop_per_unit": "4 d F per chain and mixing step (two length-d dot products per face, "
                                          "FMA = 2), summed over the slots and iterations of the step",
                         "flop_per_step": s_flop, "kernel_ms_per_step": s_ms,
@@ -425,7 +426,9 @@ def main():
                                          "note": "trained once before the timed steps; every verdict is the exact "
                                                  "checker's, admissibility uses the unchanged first-M test"},
                            "autotuned": {"batched": tuned_plain["sample_variant"] + f", check cap {tuned_plain['check_item_cap']}",
-                                         "surrogate": tuned_surr["sample_variant"]}},
+                                         "batched_large_regions": tuned_plain["large_region_variant"],
+                                         "surrogate": tuned_surr["sample_variant"],
+                                         "surrogate_large_regions": tuned_surr["large_region_variant"]}},
                 "configs_per_s": configs_all / dev_s,
                 "configs_checked_per_step": configs_all / args.steps / world,
                 "batched_gpu": {"value": batched_value, "unit": "regions/s", "configs_per_s": b_cfg / b_dev,

@@ -621,7 +621,11 @@ class BatchedEdgeInflator:
         C.check(C.lib().csd_batch_tuning(self._handle, ctypes.byref(sv), ctypes.byref(cap), C.ptr(ms),
                                          ctypes.byref(nv)))
         ns = len(self.SAMPLE_VARIANTS)
+        t, lg, lr = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        C.check(C.lib().csd_batch_sample_variants(self._handle, ctypes.byref(t), ctypes.byref(lg), ctypes.byref(lr)))
         return {"sample_variant": self.SAMPLE_VARIANTS[sv.value], "check_item_cap": cap.value,
+                "large_region_variant": self.SAMPLE_VARIANTS[lg.value],
+                "last_run_variant": self.SAMPLE_VARIANTS[lr.value],
                 "sample_ms": dict(zip(self.SAMPLE_VARIANTS, ms[:ns].tolist())),
                 "check_ms": dict(zip(self.CHECK_ITEM_CAPS, ms[ns:nv.value].tolist()))}
 

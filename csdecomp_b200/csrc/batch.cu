@@ -59,6 +59,9 @@ struct BatchIter {    // device-side iteration state
   int active;         // slots still running, counted by the faces kernel
   int last_active;    // the count of the iteration that just finished
   int num_act;        // length of the active-slot list of iteration k
+  int max_nf8;        // most faces of an active slot with dim <= 8
+  int max_nf16;       // most faces of an active slot with dim > 8
+  int pad[2];
 };
 
 struct BatchArgs {
@@ -140,20 +143,23 @@ __global__ void __launch_bounds__(256, MINB) batch_sample_kernel(BatchArgs a) {
     const float* b = a.fpool + S.b_off;
     const float* ls = a.fpool + S.seg_off;
     float* out = a.fpool + S.smp_off;
-    const bool fits = F <= (dim <= 8 ? kStageFaces8 : kStageFaces16);
+    using SC = StageCfg<MINB>;
+    const bool fits = F <= (dim <= 8 ? SC::f8 : SC::f16);
     if (fits && staged != slot) {
       __syncthreads();  // the previous slot's chains are done with the buffer
       if (dim <= 8)
-        stage_polytope<8, kStageFaces8>(At, a.capacity, b, F, dim, smf);
+        stage_polytope<8, SC::f8>(At, a.capacity, b, F, dim, smf);
       else
-        stage_polytope<16, kStageFaces16>(At, a.capacity, b, F, dim, smf);
+        stage_polytope<16, SC::f16>(At, a.capacity, b, F, dim, smf);
       __syncthreads();
       staged = slot;
     }
     if (dim <= 8)
-      sample_range<8, U, PK>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, G, smf, fits);
+      sample_range<8, U, PK, SC::f8, SC::f16>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u,
+                                              out, G, smf, fits);
     else
-      sample_range<16, U, PK>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, G, smf, fits);
+      sample_range<16, U, PK, SC::f8, SC::f16>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u,
+                                               out, G, smf, fits);
   }
 }
 
@@ -307,13 +313,18 @@ __global__ void __launch_bounds__(1024) batch_faces_kernel(BatchArgs a) {
 // One block: advances k and rebuilds the active-slot list (ascending).
 __global__ void __launch_bounds__(1024) batch_step_kernel(BatchArgs a) {
   __shared__ int warp_n[32];
-  __shared__ int base;
+  __shared__ int base, mf8, mf16;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-  if (tid == 0) base = 0;
+  if (tid == 0) {
+    base = 0;
+    mf8 = 0;
+    mf16 = 0;
+  }
   __syncthreads();
   for (int s0 = 0; s0 < a.num_slots; s0 += blockDim.x) {
     const int s = s0 + tid;
     const bool act = s < a.num_slots && !a.slots[s].done;
+    if (act) atomicMax(a.slots[s].dim <= 8 ? &mf8 : &mf16, a.slots[s].nf);
     const unsigned m = __ballot_sync(0xffffffffu, act);
     if (lane == 0) warp_n[warp] = __popc(m);
     __syncthreads();
@@ -331,6 +342,8 @@ __global__ void __launch_bounds__(1024) batch_step_kernel(BatchArgs a) {
     it->active = 0;
     it->k += 1;
     it->num_act = base;
+    it->max_nf8 = mf8;
+    it->max_nf16 = mf16;
   }
 }
 
@@ -579,21 +592,18 @@ using SampleFn = void (*)(BatchArgs);
 struct SampleVariant {
   SampleFn fn;
   int u, minb;
+  size_t smem;   // staging buffer (StageCfg<minb>::bytes)
+  int f8, f16;   // faces staged for dim <= 8 / <= 16
 };
+#define CSD_SAMPLE_VARIANT(U, MINB, PK) \
+  { batch_sample_kernel<U, MINB, PK>, U, MINB, StageCfg<MINB>::bytes, StageCfg<MINB>::f8, StageCfg<MINB>::f16 }
 static const SampleVariant kSampleVariants[] = {
-    {batch_sample_kernel<1, 2>, 1, 2},
-    {batch_sample_kernel<2, 2>, 2, 2},
-    {batch_sample_kernel<1, 3>, 1, 3},
-    {batch_sample_kernel<2, 3>, 2, 3},
-    {batch_sample_kernel<4, 2>, 4, 2},
-    {batch_sample_kernel<4, 3>, 4, 3},
-    {batch_sample_kernel<1, 2, true>, 1, 2},
-    {batch_sample_kernel<2, 2, true>, 2, 2},
-    {batch_sample_kernel<1, 3, true>, 1, 3},
-    {batch_sample_kernel<2, 3, true>, 2, 3},
-    {batch_sample_kernel<1, 4>, 1, 4},
-    {batch_sample_kernel<2, 4>, 2, 4},
+    CSD_SAMPLE_VARIANT(1, 2, false), CSD_SAMPLE_VARIANT(2, 2, false), CSD_SAMPLE_VARIANT(1, 3, false),
+    CSD_SAMPLE_VARIANT(2, 3, false), CSD_SAMPLE_VARIANT(4, 2, false), CSD_SAMPLE_VARIANT(4, 3, false),
+    CSD_SAMPLE_VARIANT(1, 2, true),  CSD_SAMPLE_VARIANT(2, 2, true),  CSD_SAMPLE_VARIANT(1, 3, true),
+    CSD_SAMPLE_VARIANT(2, 3, true),  CSD_SAMPLE_VARIANT(1, 4, false), CSD_SAMPLE_VARIANT(2, 4, false),
 };
+#undef CSD_SAMPLE_VARIANT
 constexpr int kNumSampleVariants = (int)(sizeof(kSampleVariants) / sizeof(kSampleVariants[0]));
 // Largest check work item (configurations) the autotuner chooses from.
 constexpr int kCheckItemCaps[] = {32, 128, 512};
@@ -614,7 +624,10 @@ struct csd_batch_s {
   size_t check_smem = 0;
   int check_grid = 0, bisect_grid = 0;
   int cfg_max = 128, part_max = 64;
-  int sample_variant = 0;
+  int sample_variant = 0;     // tuned (or set) variant
+  int large_variant = 1;      // variant once a slot's faces exceed the tuned variant's staging
+  int run_variant = 0;        // variant of the current iterations
+  bool switch_large = true;   // false after csd_batch_set_shapes: run exactly the set variant
   int sample_grid[csd::kNumSampleVariants] = {};
   int tune_iters = 0;                               // iterations of the next inflate to tune on
   double tune_ms[csd::kNumSampleVariants + csd::kNumCheckVariants] = {};
@@ -660,7 +673,8 @@ void launch_iteration(csd_batch_s* h, int num_slots, const BatchArgs& a, cudaStr
                       bool skip_sample = false) {
   if (ev) cudaEventRecord(ev[0], s);
   if (!skip_sample)
-    kSampleVariants[h->sample_variant].fn<<<h->sample_grid[h->sample_variant], 256, kStageBytes, s>>>(a);
+    kSampleVariants[h->run_variant].fn<<<h->sample_grid[h->run_variant], 256, kSampleVariants[h->run_variant].smem,
+                                         s>>>(a);
   if (ev) cudaEventRecord(ev[1], s);
   if (a.mlp_wb) {
     batch_score_kernel<<<dim3((h->n_max + 127) / 128, num_slots), mlp::kThreads, mlp::kFwdSmem, s>>>(a);
@@ -700,7 +714,7 @@ void launch_iteration(csd_batch_s* h, int num_slots, const BatchArgs& a, cudaStr
 }
 
 csd_status_t build_graph(csd_batch_s* h, int num_slots, const BatchArgs& a) {
-  if (h->graph && h->graph_slots == num_slots && h->graph_cfg == a.cfg_max && h->graph_variant == h->sample_variant &&
+  if (h->graph && h->graph_slots == num_slots && h->graph_cfg == a.cfg_max && h->graph_variant == h->run_variant &&
       h->graph_mlp == a.mlp_wb)
     return CSD_OK;
   if (h->graph) {
@@ -724,7 +738,7 @@ csd_status_t build_graph(csd_batch_s* h, int num_slots, const BatchArgs& a) {
   }
   h->graph_slots = num_slots;
   h->graph_cfg = a.cfg_max;
-  h->graph_variant = h->sample_variant;
+  h->graph_variant = h->run_variant;
   h->graph_mlp = a.mlp_wb;
   return CSD_OK;
 }
@@ -795,9 +809,10 @@ csd_status_t csd_batch_create(const csd_plant_t* plants, int32_t num_plants, int
   h->bisect_grid = g2;
   for (int v = 0; v < kNumSampleVariants; ++v) {
     CSD_CUDA_TRY(cudaFuncSetAttribute(kSampleVariants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kStageBytes));
+                                      (int)kSampleVariants[v].smem));
     int per_sm = 0;
-    CSD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kSampleVariants[v].fn, 256, kStageBytes));
+    CSD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kSampleVariants[v].fn, 256,
+                                                             kSampleVariants[v].smem));
     h->sample_grid[v] = device_sm_count() * std::max(1, per_sm);
   }
   // buffers
@@ -960,6 +975,7 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
   CSD_CUDA_TRY(cudaMemsetAsync(h->status.ptr, 0, 16, st));
   batch_transpose_kernel<<<n, 256, 0, st>>>(a);
   CSD_CUDA_TRY(cudaGetLastError());
+  h->run_variant = h->sample_variant;
   csd_status_t s = build_graph(h, n, a);
   if (s) return s;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -986,7 +1002,7 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
       int j = 0;
       for (int v = 0; v < kNumSampleVariants; ++v, ++j) {
         cudaEventRecord(tev[2 * j], st);
-        kSampleVariants[v].fn<<<h->sample_grid[v], 256, kStageBytes, st>>>(a);
+        kSampleVariants[v].fn<<<h->sample_grid[v], 256, kSampleVariants[v].smem, st>>>(a);
         cudaEventRecord(tev[2 * j + 1], st);
       }
       for (int c = 0; c < kNumCheckVariants && !a.mlp_wb; ++c, ++j) {
@@ -1016,6 +1032,12 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
         for (int c = 1; c < kNumCheckVariants; ++c)
           if (h->tune_ms[kNumSampleVariants + c] < h->tune_ms[kNumSampleVariants + bc]) bc = c;
         h->sample_variant = bs;
+        h->run_variant = bs;
+        // for slots whose faces outgrow bs's staging: the fastest variant with more staging room
+        int bl = -1;
+        for (int v = 0; v < kNumSampleVariants; ++v)
+          if (kSampleVariants[v].f16 > kSampleVariants[bs].f16 && (bl < 0 || h->tune_ms[v] < h->tune_ms[bl])) bl = v;
+        h->large_variant = bl >= 0 ? bl : bs;
         if (!a.mlp_wb) h->cfg_max = kCheckItemCaps[bc];
         a.cfg_max = h->cfg_max;
         h->graph_slots = -1;  // recapture with the chosen shapes
@@ -1045,6 +1067,15 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
     CSD_CUDA_TRY(cudaStreamSynchronize(st));
     active_now = h->host_iter->last_active;
     if (active_now == 0) break;
+    // a slot's region outgrew the staging buffer of the running variant: continue with the
+    // large-staging variant (identical samples; the graph is captured again once)
+    if (h->switch_large && h->tune_iters == 0 && h->run_variant != h->large_variant) {
+      const SampleVariant& rv = kSampleVariants[h->run_variant];
+      if (h->host_iter->max_nf8 > rv.f8 || h->host_iter->max_nf16 > rv.f16) {
+        h->run_variant = h->large_variant;
+        if ((s = build_graph(h, n, a))) return s;
+      }
+    }
   }
   if (device_ms) {
     CSD_CUDA_TRY(cudaEventRecord(ev1, st));
@@ -1155,7 +1186,17 @@ csd_status_t csd_batch_set_shapes(csd_batch_t h, int32_t sample_variant, int32_t
                 check_item_cap % 8 == 0,
             CSD_ERR_INVALID, "bad shapes: sampler variant out of range, or check item cap not a positive multiple of 8");
   h->sample_variant = sample_variant;
+  h->run_variant = sample_variant;
+  h->switch_large = false;
   h->cfg_max = check_item_cap;
+  return CSD_OK;
+}
+
+csd_status_t csd_batch_sample_variants(csd_batch_t h, int32_t* tuned, int32_t* large, int32_t* last_run) {
+  CSD_CHECK(h, CSD_ERR_INVALID, "null batch");
+  if (tuned) *tuned = h->sample_variant;
+  if (large) *large = h->switch_large ? h->large_variant : h->sample_variant;
+  if (last_run) *last_run = h->run_variant;
   return CSD_OK;
 }
 

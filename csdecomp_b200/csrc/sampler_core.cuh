@@ -318,6 +318,18 @@ constexpr int kStageFaces16 = 1024;  // faces staged for dim <= 16
 constexpr size_t kStageBytes = 9 * kStageFaces8 * sizeof(float);
 static_assert(9 * kStageFaces8 >= 17 * kStageFaces16, "staging buffer");
 
+// Staging capacity of a kernel with MINB resident blocks per SM: the largest
+// buffer that MINB blocks fit in the SM's 227 KB (2 blocks: 3072 / 1536
+// faces, 3 blocks: 2048 / 1024, 4 blocks: 1536 / 768).
+template <int MINB>
+struct StageCfg {
+  static constexpr int f8 = MINB <= 2 ? 3072 : MINB == 3 ? 2048 : 1536;
+  static constexpr int f16 = f8 / 2;
+  static constexpr size_t bytes = 9 * (size_t)f8 * sizeof(float);
+  static_assert(9 * f8 >= 17 * f16, "staging buffer");
+  static_assert(MINB * bytes <= 227 * 1024, "MINB staging buffers fit one SM");
+};
+
 template <int MAXD, int ST>
 __device__ __forceinline__ void stage_polytope(const float* __restrict__ At, int ldt, const float* __restrict__ b,
                                                int F, int dim, float* sm) {
@@ -364,12 +376,12 @@ __host__ __device__ __forceinline__ int group_width(int64_t total, int64_t grid_
 // One polytope's chains [first, last) with the polytope staged in `sm` when
 // it fits (sm_ready: already staged), else read from global memory. PK: the
 // staged path takes faces in packed pairs (U pairs per trip).
-template <int MAXD, int U, bool PK = false>
+template <int MAXD, int U, bool PK = false, int ST8 = kStageFaces8, int ST16 = kStageFaces16>
 __device__ __forceinline__ void sample_range(const float* __restrict__ At, int ldt, const float* __restrict__ b,
                                              int F, int dim, const float* __restrict__ start, int first, int last,
                                              int mixing, uint32_t k0, uint32_t k1, uint32_t stream,
                                              float* __restrict__ out, int G, float* sm, bool staged) {
-  constexpr int ST = MAXD <= 8 ? kStageFaces8 : kStageFaces16;
+  constexpr int ST = MAXD <= 8 ? ST8 : ST16;
   if (staged) {
     const float* sAt = sm;
     const float* sb = sm + MAXD * ST;

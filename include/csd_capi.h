@@ -298,8 +298,17 @@ csd_status_t csd_batch_set_surrogate(csd_batch_t h, csd_mlp_t mlp, float stop_pr
  * (defaults: 3 rounds, first round 1024 samples). */
 csd_status_t csd_batch_set_surrogate_rounds(csd_batch_t h, int32_t rounds, int32_t first_round);
 /* Sets the shapes directly (e.g. a tuning result kept from an earlier run):
- * sampler variant index as above, check work-item cap a multiple of 8. */
+ * sampler variant index as above, check work-item cap a multiple of 8. The
+ * set variant then runs for every iteration. */
 csd_status_t csd_batch_set_shapes(csd_batch_t h, int32_t sample_variant, int32_t check_item_cap);
+/* Each sampler variant stages a slot's region in shared memory up to a face
+ * count set by its blocks per SM (2: 3072 faces for dim <= 8, 1536 above;
+ * 3: 2048 / 1024; 4: 1536 / 768); larger regions are read from L2. After
+ * tuning, once an active slot outgrows the tuned variant's staging, the
+ * iterations continue with the fastest variant that stages more (the graph is
+ * captured once more). tuned / large / last_run: the tuned variant, the one
+ * used for large regions, the one the last iteration ran. */
+csd_status_t csd_batch_sample_variants(csd_batch_t h, int32_t* tuned, int32_t* large, int32_t* last_run);
 csd_status_t csd_batch_tuning(csd_batch_t h, int32_t* sample_variant, int32_t* check_item_cap, float* variant_ms,
                               int32_t* num_variants);
 /* Profiling mode, last csd_batch_inflate: per iteration the eight stage times
