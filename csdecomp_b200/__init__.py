@@ -9,7 +9,7 @@ from .plant import (CollisionGeometry, CollisionGroup, Joint, JointType, Kinemat
                     MinimalPlant, SceneInspector, ShapePrimitive, URDFParser)
 from .api import (MAX_DIM, BatchedEdgeInflator, MAX_NUM_FACES, MAX_NUM_VOXELS, CheckCollisionFree, CheckCollisionFreeCuda,
                   CheckCollisionFreeVoxels, CheckCollisionFreeVoxelsCuda, CheckEdgeCollisionFree,
-                  CheckEdgesCollisionFreeCuda, ComputeForwardKinematicsCuda, CudaEdgeInflator, EditRegionsCuda,
+                  CheckEdgesCollisionFreeCuda, CheckEdgesCollisionFreeRankedCuda, ComputeForwardKinematicsCuda, CudaEdgeInflator, EditRegionsCuda,
                   EditRegionsOptions, EizoCuda, EizoInfo,
                   EizoIterationInfo, EizoOptions, HPolyhedron, MinimalHPolyhedron, PairCollisionFree, Voxels,
                   UniformSampleInHPolyhedraCuda, VisibilityGraph, computeLinkFrameToWorldTransformsMinimal,

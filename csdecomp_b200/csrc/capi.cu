@@ -161,6 +161,76 @@ csd_status_t csd_check_edges(csd_plant_t p, const float* starts, const float* en
   return CSD_OK;
 }
 
+csd_status_t csd_check_edges_ranked(csd_plant_t p, csd_mlp_t mlp, int32_t net, const float* starts, const float* ends,
+                                    int64_t n, float step, int32_t mode, int32_t top, uint8_t* out, int64_t* pts,
+                                    int32_t flags, void* stream) {
+  CSD_CHECK(p && mlp && n >= 0 && (n == 0 || (starts && ends && out)), CSD_ERR_INVALID, "null argument");
+  CSD_CHECK(mode >= CSD_EDGE_L2_REF && mode <= CSD_EDGE_VG, CSD_ERR_INVALID, "bad edge discretisation mode");
+  CSD_CHECK(step > 0.f && std::isfinite(step), CSD_ERR_INVALID, "step size must be positive");
+  CSD_CHECK(top >= 0 && top <= 32, CSD_ERR_INVALID, "top must be in [0, 32]");
+  const MlpView mv = mlp_view(mlp);
+  const int d = p->dp.dim;
+  CSD_CHECK(net >= 0 && net < mv.nets, CSD_ERR_INVALID, "bad net index");
+  CSD_CHECK(mv.dims[net] == d, CSD_ERR_DIMENSION, "the net's input dimension differs from the plant's");
+  CSD_CHECK(mv.device == p->device, CSD_ERR_INVALID, "the surrogate and the plant live on different devices");
+  DeviceGuard g(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  csd_status_t s;
+  if (n == 0) return CSD_OK;
+  if ((s = p->counter.reserve(64))) return s;
+  const float* sd = starts;
+  const float* ed = ends;
+  uint8_t* od = out;
+  int64_t* pd = pts;
+  const size_t qb = (size_t)n * d * sizeof(float);
+  if (flags != CSD_PTR_DEVICE) {
+    if ((s = p->in_buf.reserve(qb + 16)) || (s = p->in_buf2.reserve(qb + 16)) || (s = p->out_buf.reserve((size_t)n + 16)) ||
+        (s = p->out_buf2.reserve((size_t)n * sizeof(int64_t) + 16)))
+      return s;
+    CSD_CUDA_TRY(cudaMemcpyAsync(p->in_buf.ptr, starts, qb, cudaMemcpyHostToDevice, st));
+    CSD_CUDA_TRY(cudaMemcpyAsync(p->in_buf2.ptr, ends, qb, cudaMemcpyHostToDevice, st));
+    sd = p->in_buf.as<float>();
+    ed = p->in_buf2.as<float>();
+    od = p->out_buf.as<uint8_t>();
+    pd = pts ? p->out_buf2.as<int64_t>() : nullptr;
+  }
+  // points per edge, their offsets, and chunks of at most kChunk scored points
+  constexpr int64_t kChunk = int64_t(1) << 22;
+  DevBuf cnt, offd, xb, lg;
+  if ((s = cnt.reserve((size_t)n * 8 + 16)) || (s = offd.reserve((size_t)(n + 1) * 8 + 16))) return s;
+  if ((s = launch_edge_count(sd, ed, n, d, step, (int)mode, cnt.as<int64_t>(), st))) return s;
+  std::vector<int64_t> off(n + 1, 0);
+  CSD_CUDA_TRY(cudaMemcpyAsync(off.data() + 1, cnt.ptr, (size_t)n * 8, cudaMemcpyDeviceToHost, st));
+  CSD_CUDA_TRY(cudaStreamSynchronize(st));
+  for (int64_t i = 0; i < n; ++i) off[i + 1] += off[i];
+  CSD_CUDA_TRY(cudaMemcpyAsync(offd.ptr, off.data(), (size_t)(n + 1) * 8, cudaMemcpyHostToDevice, st));
+  const int64_t most = std::min<int64_t>(off[n], kChunk);
+  if (top > 0 && most > 0) {
+    if ((s = xb.reserve((size_t)most * d * 4 + 16)) || (s = lg.reserve((size_t)most * 4 + 16))) return s;
+  }
+  for (int64_t c0 = 0; c0 < n;) {
+    int64_t c1 = c0 + 1;
+    while (c1 < n && off[c1 + 1] - off[c0] <= kChunk) ++c1;
+    const int64_t P = off[c1] - off[c0];
+    const bool ranked = top > 0 && P <= kChunk;  // an edge longer than a chunk is checked unranked
+    if (ranked) {
+      if ((s = launch_edge_materialize(sd, ed, c0, c1, offd.as<int64_t>(), d, (int)mode, xb.as<float>(), st))) return s;
+      const int32_t rows = (int32_t)P;
+      if ((s = csd_mlp_infer(mlp, 1, &net, &rows, xb.as<float>(), lg.as<float>(), CSD_PTR_DEVICE, st))) return s;
+    }
+    if ((s = launch_check_edges_ranked(p, sd, ed, c0, c1, offd.as<int64_t>(), ranked ? lg.as<float>() : nullptr, top,
+                                       (int)mode, od, pd, p->counter.as<unsigned int>(), st)))
+      return s;
+    c0 = c1;
+  }
+  if (flags != CSD_PTR_DEVICE) {
+    CSD_CUDA_TRY(cudaMemcpyAsync(out, od, (size_t)n, cudaMemcpyDeviceToHost, st));
+    if (pts) CSD_CUDA_TRY(cudaMemcpyAsync(pts, pd, (size_t)n * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+  }
+  CSD_CUDA_TRY(cudaStreamSynchronize(st));
+  return CSD_OK;
+}
+
 csd_status_t csd_visibility_graph(csd_plant_t p, const float* nodes, int32_t n, float step, uint8_t* adjacency,
                                   int32_t flags, void* stream) {
   CSD_CHECK(p && n >= 2 && nodes && adjacency, CSD_ERR_INVALID, "a visibility graph needs at least two nodes");

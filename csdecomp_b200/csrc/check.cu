@@ -176,6 +176,127 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) check_edges_kernel(Dev
   }
 }
 
+// ------------------------------------------------- surrogate-ranked edge checks
+// Points per edge (thread per edge).
+__global__ void edge_count_kernel(const float* __restrict__ s, const float* __restrict__ e, int64_t n, int d,
+                                  float step, int mode, int64_t* __restrict__ counts) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    counts[i] = edge_points(s + i * d, e + i * d, d, step, mode);
+}
+
+// The points of edges [e0, e1) as rows of x (edge i's points from row
+// off[i] - off[e0]); warp per edge, lane per point.
+__global__ void edge_materialize_kernel(const float* __restrict__ s, const float* __restrict__ e, int64_t e0,
+                                        int64_t e1, const int64_t* __restrict__ off, int d, int mode,
+                                        float* __restrict__ x) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = e0 + blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < e1; i += nw) {
+    const int64_t np = off[i + 1] - off[i];
+    float* xi = x + (off[i] - off[e0]) * d;
+    for (int64_t k = lane; k < np; k += 32)
+      for (int c = 0; c < d; ++c) xi[k * d + c] = edge_coord(s[i * d + c], e[i * d + c], np, mode, k);
+  }
+}
+
+// Warp per edge of [e0, e1): if logits are given, the point with the highest
+// logit in each residue class k mod 32 is a candidate, the candidates are
+// checked in decreasing logit (at most `top`), then every other point
+// coarse-to-fine as check_edges_kernel visits them. The verdict is the AND
+// over all points either way; only the order (and so the early exit) depends
+// on the logits.
+template <bool SM>
+__global__ void __launch_bounds__(32 * kWarpsPerBlock, 3)
+    check_edges_ranked_kernel(DevPlant p, const float* __restrict__ starts, const float* __restrict__ ends, int64_t e0,
+                              int64_t e1, const int64_t* __restrict__ off, const float* __restrict__ logits, int top,
+                              int mode, uint8_t* __restrict__ out, int64_t* __restrict__ pts,
+                              unsigned long long* counter) {
+  extern __shared__ float4 smem4[];
+  __shared__ uint64_t bar;
+  const WarpCtx<SM> w = warp_setup<SM>(p, smem4, &bar);
+  if (!w.ok) return;
+  const int lane = threadIdx.x & 31;
+  const int d = p.dim;
+  VoxArgs none{};
+  while (true) {
+    unsigned long long c = 0;
+    if (lane == 0) c = atomicAdd(counter, 1ull);
+    c = __shfl_sync(kFull, c, 0);
+    const int64_t e = e0 + (int64_t)c;
+    if (e >= e1) break;
+    const int64_t np = off[e + 1] - off[e];
+    const float a1 = lane < d ? starts[e * d + lane] : 0.f, a2 = lane < d ? ends[e * d + lane] : 0.f;
+    bool collided = false;
+    int64_t checked = 0;
+    // candidates: best logit of each residue class, sorted descending across the warp
+    float bv = -FLT_MAX;
+    int64_t bk = -1;
+    if (logits) {
+      const float* lg = logits + (off[e] - off[e0]);
+      for (int64_t k = lane; k < np; k += 32) {
+        const float v = lg[k];
+        if (v > bv || bk < 0) {
+          bv = v;
+          bk = k;
+        }
+      }
+    }
+    // bitonic sort of (bv, bk) over the 32 lanes: lane r ends with the r-th
+    // candidate by decreasing logit (lower index on ties; empty classes last)
+    auto before = [](float va, int64_t ka, float vb, int64_t kb) {
+      return ka >= 0 && (kb < 0 || va > vb || (va == vb && ka < kb));
+    };
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        const float ov = __shfl_xor_sync(kFull, bv, stride);
+        const int64_t ok = __shfl_xor_sync(kFull, bk, stride);
+        const bool descending = (lane & size) == 0;
+        const bool lower = (lane & stride) == 0;
+        const bool take = (lower == descending) ? before(ov, ok, bv, bk) : before(bv, bk, ov, ok);
+        if (take) {
+          bv = ov;
+          bk = ok;
+        }
+      }
+    }
+    int ncand = logits ? min(top, np < 32 ? (int)np : 32) : 0;
+    const int64_t G = (np + 31) / 32;
+    // one visiting loop (one inlined check): candidates r < ncand first, then coarse-to-fine
+    int r = 0;
+    int64_t v = 0;
+    while (!collided) {
+      int64_t k;
+      if (r < ncand) {
+        k = __shfl_sync(kFull, bk, r);
+        ++r;
+        if (k < 0) {  // fewer candidates than `top`: the rest are empty classes
+          ncand = r - 1;
+          continue;
+        }
+      } else {
+        if (v >= 32 * G) break;
+        k = (v % 32) * G + v / 32;
+        ++v;
+        if (k >= np) continue;
+        if (__any_sync(kFull, lane < ncand && bk == k)) continue;  // checked as a candidate
+      }
+      const float x = edge_coord(a1, a2, np, mode, k);
+      __syncwarp();
+      if (lane < d) w.qs[lane] = x;
+      __syncwarp();
+      fk_warp(p, w.qs, w.X, lane);
+      ++checked;
+      collided = check_config(p, w.stat, w.aabb, w.X, w.pose, lane, none);
+    }
+    if (lane == 0) {
+      out[e] = collided ? 0 : 1;
+      if (pts) pts[e] = checked;
+    }
+  }
+}
+
 // ---------------------------------------------------------------- FK output
 // Warp per configuration; lane l writes reference link l's 4x4 (column-major).
 __global__ void __launch_bounds__(32 * kWarpsPerBlock) fk_kernel(DevPlant p, const float* __restrict__ q, int64_t n,
@@ -255,6 +376,46 @@ csd_status_t launch_fk(const csd_plant_s* p, const float* q, int64_t n, float* t
   csd_status_t s = launch_grid(p, fk_kernel, false, n, &smem, &grid);
   if (s) return s;
   fk_kernel<<<grid, 32 * kWarpsPerBlock, smem, st>>>(p->dp, q, n, tf);
+  CSD_CUDA_TRY(cudaGetLastError());
+  return CSD_OK;
+}
+
+csd_status_t launch_edge_count(const float* s, const float* e, int64_t n, int d, float step, int mode,
+                               int64_t* counts, cudaStream_t st) {
+  if (n <= 0) return CSD_OK;
+  const int grid = (int)std::min<int64_t>((n + 255) / 256, 8 * device_sm_count());
+  edge_count_kernel<<<grid, 256, 0, st>>>(s, e, n, d, step, mode, counts);
+  CSD_CUDA_TRY(cudaGetLastError());
+  return CSD_OK;
+}
+
+csd_status_t launch_edge_materialize(const float* s, const float* e, int64_t e0, int64_t e1, const int64_t* off, int d,
+                                     int mode, float* x, cudaStream_t st) {
+  if (e1 <= e0) return CSD_OK;
+  const int grid = (int)std::min<int64_t>((e1 - e0 + 7) / 8, 8 * device_sm_count());
+  edge_materialize_kernel<<<grid, 256, 0, st>>>(s, e, e0, e1, off, d, mode, x);
+  CSD_CUDA_TRY(cudaGetLastError());
+  return CSD_OK;
+}
+
+csd_status_t launch_check_edges_ranked(const csd_plant_s* p, const float* s0, const float* e0p, int64_t e0, int64_t e1,
+                                       const int64_t* off, const float* logits, int top, int mode, uint8_t* out,
+                                       int64_t* pts, unsigned int* counter, cudaStream_t st) {
+  if (e1 <= e0) return CSD_OK;
+  size_t smem = 0;
+  int grid = 0;
+  csd_status_t s;
+  CSD_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
+  unsigned long long* ctr = reinterpret_cast<unsigned long long*>(counter);
+  if (statics_in_smem(p)) {
+    if ((s = launch_grid(p, check_edges_ranked_kernel<true>, true, e1 - e0, &smem, &grid))) return s;
+    check_edges_ranked_kernel<true><<<grid, 32 * kWarpsPerBlock, smem, st>>>(p->dp, s0, e0p, e0, e1, off, logits, top,
+                                                                              mode, out, pts, ctr);
+  } else {
+    if ((s = launch_grid(p, check_edges_ranked_kernel<false>, false, e1 - e0, &smem, &grid))) return s;
+    check_edges_ranked_kernel<false><<<grid, 32 * kWarpsPerBlock, smem, st>>>(p->dp, s0, e0p, e0, e1, off, logits,
+                                                                               top, mode, out, pts, ctr);
+  }
   CSD_CUDA_TRY(cudaGetLastError());
   return CSD_OK;
 }

@@ -124,6 +124,14 @@ csd_status_t launch_check_points(const csd_plant_s* p, const float* q, int64_t n
 csd_status_t launch_fk(const csd_plant_s* p, const float* q, int64_t n, float* tf, cudaStream_t st);
 csd_status_t launch_check_edges(const csd_plant_s* p, const float* s, const float* e, int64_t n, float step,
                                 int mode, uint8_t* out, int64_t* pts, unsigned int* counter, cudaStream_t st, int64_t nodes = 0);
+// surrogate-ranked edge checks (check.cu)
+csd_status_t launch_edge_count(const float* s, const float* e, int64_t n, int d, float step, int mode,
+                               int64_t* counts, cudaStream_t st);
+csd_status_t launch_edge_materialize(const float* s, const float* e, int64_t e0, int64_t e1, const int64_t* off, int d,
+                                     int mode, float* x, cudaStream_t st);
+csd_status_t launch_check_edges_ranked(const csd_plant_s* p, const float* s0, const float* e0p, int64_t e0, int64_t e1,
+                                       const int64_t* off, const float* logits, int top, int mode, uint8_t* out,
+                                       int64_t* pts, unsigned int* counter, cudaStream_t st);
 // sampler.cu
 csd_status_t launch_hit_and_run(const float* A, const float* b, const int32_t* face_off, int num_poly, int dim,
                                 const float* starts, int samples_per_poly, int mixing, uint64_t seed,

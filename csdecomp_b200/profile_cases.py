@@ -29,6 +29,10 @@
       (uniform in a 3 x 3 x 1.5 m box around the arm, none within 0.9 m of its
       base, so that verdicts are mixed), N uniform configurations; with and
       without the voxel hash grid
+  python -m csdecomp_b200.profile_cases edge_check_ranked [--edges E]
+      config-2 arm with a 0.8 m keep-out (mixed verdicts): E edges from free
+      starts, lengths U[0.05, 1.0] rad; unranked checks against checks ranked
+      by a surrogate trained on 65,536 labelled configurations of the scene
   python -m csdecomp_b200.profile_cases edit_regions [--regions R] [--collisions C]
       EditRegionsCuda on the config-3 scene: R box regions around seed edges,
       C colliding configurations drawn inside each, 9 bisection steps
@@ -284,10 +288,38 @@ def voxel_check(n: int, voxels: int) -> None:
     print(json.dumps({"case": "voxel_check", "configs": n, "voxels": voxels, "voxel_radius": vr, **res}))
 
 
+def edge_check_ranked(n: int) -> None:
+    import csdecomp_b200 as csd
+    from csdecomp_b200 import scenes
+    from csdecomp_b200.surrogate import CollisionSurrogate, training_set
+    sc = scenes.edge_check_scene(keepout=0.8)
+    seeds = scenes.seed_edges(sc, 64, 77, lambda q: csd.CheckCollisionFreeCuda(q.T, sc.plant),
+                              lambda a, b: csd.CheckEdgesCollisionFreeCuda(a.T, b.T, sc.plant))
+    bank = CollisionSurrogate([sc.dim], seed=1)
+    x, y = training_set(sc, seeds, 65536, seed=2)
+    bank.train([x], [y], batch=512, epochs=6, lr=2e-3)
+    rng = np.random.default_rng(9)
+    q = sc.random_configs(8 * n, 10)
+    q0 = q[csd.CheckCollisionFreeCuda(q.T, sc.plant) == 1][:n]
+    d = rng.normal(size=q0.shape)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    q1 = np.clip(q0 + rng.uniform(0.05, 1.0, (len(q0), 1)) * d, sc.lower(), sc.upper()).astype(np.float32)
+    ms_u, (fu, pu) = _timed(lambda: csd.CheckEdgesCollisionFreeCuda(q0.T, q1.T, sc.plant, 0.01,
+                                                                  return_points_checked=True))
+    ms_r, (fr, pr) = _timed(lambda: csd.CheckEdgesCollisionFreeRankedCuda(q0.T, q1.T, sc.plant, bank, 0, 0.01, top=8,
+                                                                        return_points_checked=True))
+    col = fu == 0
+    print(json.dumps({"case": "edge_check_ranked", "edges": int(len(q0)), "free_fraction": float(fu.mean()),
+                      "identical": bool((fu == fr).all()),
+                      "unranked": {"ms": ms_u, "points": int(pu.sum()), "points_per_colliding_edge": float(pu[col].mean())},
+                      "ranked": {"ms": ms_r, "points": int(pr.sum()), "points_per_colliding_edge": float(pr[col].mean())},
+                      "training_colliding_fraction": float(y.mean())}))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["check_points", "batch", "point_check", "edge_check", "eizo_single",
-                                     "visibility_graph", "edit_regions", "voxel_check"])
+                                     "visibility_graph", "edit_regions", "voxel_check", "edge_check_ranked"])
     ap.add_argument("--configs", type=int, default=1 << 20)
     ap.add_argument("--no-cull", action="store_true", help="check_points: link-level broad phase off (full sweep)")
     ap.add_argument("--slots", type=int, default=24)
@@ -315,6 +347,8 @@ def main() -> None:
         edit_regions(a.regions, a.collisions)
     elif a.case == "voxel_check":
         voxel_check(a.configs, a.voxels)
+    elif a.case == "edge_check_ranked":
+        edge_check_ranked(a.edges)
     else:
         batch(a.slots, a.iterations, a.sample_variant, a.check_item_cap, a.per_iteration)
 

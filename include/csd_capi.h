@@ -155,6 +155,21 @@ csd_status_t csd_check_edges(csd_plant_t plant, const float* starts, const float
                              float step_size, int32_t mode, uint8_t* free_out, int64_t* points_checked,
                              int32_t flags, void* stream);
 
+/* Surrogate-ranked edge checks (no counterpart in the reference): as
+ * csd_check_edges, but each edge's points are first scored by net `net` of
+ * the surrogate bank `mlp` (csd_mlp_*, input dimension = the plant's); per
+ * residue class k mod 32 the highest-scored point is a candidate, up to `top`
+ * (<= 32) candidates are checked in decreasing score, then every other point
+ * in the coarse-to-fine order of csd_check_edges. Verdicts are exact (a free
+ * edge has every point checked); the ranking only moves a colliding edge's
+ * first hit earlier. Points are scored in chunks of up to 2^22; an edge with
+ * more points is checked unranked. starts/ends/free_out/points_checked follow
+ * `flags`. */
+typedef struct csd_mlp_s* csd_mlp_t;  /* the surrogate bank (csd_mlp_* below) */
+csd_status_t csd_check_edges_ranked(csd_plant_t plant, csd_mlp_t mlp, int32_t net, const float* starts,
+                                    const float* ends, int64_t n, float step_size, int32_t mode, int32_t top,
+                                    uint8_t* free_out, int64_t* points_checked, int32_t flags, void* stream);
+
 /* All-pairs visibility graph: VisibilityGraph, csdecomp/src/planning/cuda_visibility_graph.cu:175-375.
  * nodes: [n][dim] configurations (n >= 2). adjacency receives one byte per
  * pair i < j in upper-triangle row-major order (pair (i, j) at
@@ -245,7 +260,7 @@ csd_status_t csd_eizo(csd_plant_t plant, const float* line_start, const float* l
  * per stage, replayed as a CUDA graph. Each slot computes exactly what
  * csd_inflator_inflate computes for the same inputs. No voxels. */
 typedef struct csd_batch_s* csd_batch_t;
-typedef struct csd_mlp_s* csd_mlp_t;  /* the surrogate bank, declared with csd_mlp_* below */
+/* csd_mlp_t (the surrogate bank, functions csd_mlp_* below) is declared above csd_check_edges_ranked. */
 csd_status_t csd_batch_create(const csd_plant_t* plants, int32_t num_plants, int32_t max_slots,
                               const csd_eizo_options_t* options, int32_t face_capacity, csd_batch_t* out);
 /* n slots: slot i uses plants[slot_plant[i]] (dim d_i); starts/ends hold the

@@ -91,3 +91,60 @@ def test_surrogate_must_match_the_plants():
         b.set_surrogate(CollisionSurrogate([S7.dim]), 0.1)
     with pytest.raises(RuntimeError):
         b.set_surrogate(CollisionSurrogate([S14.dim, S7.dim]), 0.1)
+
+
+def edge_set(sc, n, seed):
+    """Edges from free starts, mixed verdicts: lengths U[0.05, 1.0] rad."""
+    rng = np.random.default_rng(seed)
+    q = sc.random_configs(8 * n, seed)
+    q0 = q[csd.CheckCollisionFreeCuda(q.T, sc.plant) == 1][:n]
+    d = rng.normal(size=q0.shape)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    q1 = np.clip(q0 + rng.uniform(0.05, 1.0, (len(q0), 1)) * d, sc.lower(), sc.upper()).astype(np.float32)
+    return q0, q1
+
+
+@pytest.mark.parametrize("mode", [csd.CSD_EDGE_L2_REF, csd.CSD_EDGE_LINF, csd.CSD_EDGE_VG])
+def test_ranked_edges_exact(mode):
+    """Ranking only reorders: verdicts equal the unranked check for an
+    untrained net, a trained one and every candidate count."""
+    bank, _, _ = trained_bank(epochs=2)
+    raw = CollisionSurrogate([S7.dim, S14.dim], seed=3)
+    for net, sc in enumerate((S7, S14)):
+        q0, q1 = edge_set(sc, 400, 11 + net)
+        ref, ref_pts = csd.CheckEdgesCollisionFreeCuda(q0.T, q1.T, sc.plant, 0.01, mode, return_points_checked=True)
+        assert 0 < ref.mean() < 1
+        for b in (bank, raw):
+            for top in (0, 1, 8, 32):
+                got, pts = csd.CheckEdgesCollisionFreeRankedCuda(q0.T, q1.T, sc.plant, b, net, 0.01, mode, top,
+                                                                 return_points_checked=True)
+                np.testing.assert_array_equal(got, ref)
+                # free edges: every point is checked exactly once
+                np.testing.assert_array_equal(pts[ref == 1], ref_pts[ref == 1])
+                if top == 0:
+                    np.testing.assert_array_equal(pts, ref_pts)
+
+
+def test_ranked_edges_exit_earlier():
+    """A trained net moves colliding edges' first hit earlier."""
+    bank, _, _ = trained_bank()
+    for net, sc in enumerate((S7, S14)):
+        q0, q1 = edge_set(sc, 600, 31 + net)
+        ref, ref_pts = csd.CheckEdgesCollisionFreeCuda(q0.T, q1.T, sc.plant, 0.01, return_points_checked=True)
+        got, pts = csd.CheckEdgesCollisionFreeRankedCuda(q0.T, q1.T, sc.plant, bank, net, 0.01, top=8,
+                                                         return_points_checked=True)
+        np.testing.assert_array_equal(got, ref)
+        col = ref == 0
+        assert col.sum() > 50
+        assert pts[col].mean() < ref_pts[col].mean(), (pts[col].mean(), ref_pts[col].mean())
+
+
+def test_ranked_edges_bad_arguments():
+    bank, _, _ = trained_bank(epochs=1)
+    q0, q1 = edge_set(S7, 8, 5)
+    with pytest.raises(csd.CsdError):
+        csd.CheckEdgesCollisionFreeRankedCuda(q0.T, q1.T, S7.plant, bank, 1)  # the 14-D net on the 7-D plant
+    with pytest.raises(ValueError):
+        csd.CheckEdgesCollisionFreeRankedCuda(q0.T, q1.T, S7.plant, bank, 0, top=33)
+    with pytest.raises(ValueError):
+        csd.CheckEdgesCollisionFreeRankedCuda(q0.T, q1.T, S7.plant, bank, 5)
