@@ -5,8 +5,8 @@ MinimalPlant, batched edge checks, hit-and-run sampling in H-polytopes and
 EI-ZO edge inflation and region editing, behind the reference's Python names (see api.py) and
 the C ABI of include/csd_capi.h.
 """
-from .plant import (CollisionGeometry, CollisionGroup, Joint, JointType, KinematicTree, Link, MinimalKinematicTree,
-                    MinimalPlant, SceneInspector, ShapePrimitive, URDFParser)
+from .plant import (CollisionGeometry, CollisionGroup, Joint, JointType, KinematicTree, Link, MinimalJoint,
+                    MinimalKinematicTree, MinimalLink, MinimalPlant, Plant, SceneInspector, ShapePrimitive, URDFParser)
 from .api import (MAX_DIM, BatchedEdgeInflator, MAX_NUM_FACES, MAX_NUM_VOXELS, CheckCollisionFree, CheckCollisionFreeCuda,
                   CheckCollisionFreeVoxels, CheckCollisionFreeVoxelsCuda, CheckEdgeCollisionFree,
                   CheckEdgesCollisionFreeCuda, CheckEdgesCollisionFreeRankedCuda, ComputeForwardKinematicsCuda, CudaEdgeInflator, EditRegionsCuda,

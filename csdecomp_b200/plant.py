@@ -214,8 +214,30 @@ class KinematicTree:
 
 
 @dataclass
+class MinimalJoint:
+    """minimal_kinematic_tree.h:18-26."""
+    type: int = JointType.FIXED
+    X_PL_J: np.ndarray = field(default_factory=lambda: np.eye(4, dtype=np.float32))
+    index: int = 0
+    parent_link: int = -1
+    child_link: int = -1
+    axis: np.ndarray = field(default_factory=lambda: np.zeros(3, np.float32))
+
+
+@dataclass
+class MinimalLink:
+    """minimal_kinematic_tree.h:31-37 (the child joint array holds exactly the
+    link's child joints; the reference pads it to MAX_CHILD_JOINT_COUNT)."""
+    index: int = 0
+    parent_joint_index: int = -1
+    child_joint_index_array: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    num_child_joints: int = 0
+
+
+@dataclass
 class MinimalKinematicTree:
-    """Table form of minimal_kinematic_tree.h:42-53 (no fixed capacities)."""
+    """Table form of minimal_kinematic_tree.h:42-53 (no fixed capacities);
+    ``joints`` and ``links`` give the reference's per-element structs."""
 
     joint_type: np.ndarray
     joint_X_PL_J: np.ndarray  # [J,4,4]
@@ -227,6 +249,20 @@ class MinimalKinematicTree:
     num_configuration_variables: int
     num_joints: int
     num_links: int
+
+    @property
+    def joints(self) -> List[MinimalJoint]:
+        return [MinimalJoint(int(self.joint_type[j]), self.joint_X_PL_J[j].copy(), j, int(self.joint_parent_link[j]),
+                             int(self.joint_child_link[j]), self.joint_axis[j].copy()) for j in range(self.num_joints)]
+
+    @property
+    def links(self) -> List[MinimalLink]:
+        out = []
+        for l in range(self.num_links):
+            parent = np.nonzero(self.joint_child_link == l)[0]
+            children = np.nonzero(self.joint_parent_link == l)[0].astype(np.int32)
+            out.append(MinimalLink(l, int(parent[0]) if len(parent) else -1, children, int(len(children))))
+        return out
 
     @staticmethod
     def from_tree(t: KinematicTree) -> "MinimalKinematicTree":
@@ -344,6 +380,68 @@ class MinimalPlant:
                 collision_pairs_flat=np.ascontiguousarray(self.collision_pairs_flat, np.int32),
             )
         return self._arrays
+
+
+class Plant:
+    """Plant (minimal_plant.h:42-145): a kinematic tree, its scene inspector and
+    the scene's collision geometries, with the reference's accessors.
+    numJoints() returns the number of joints (the reference returns the number
+    of links there, minimal_plant.h:50)."""
+
+    def __init__(self, kin_tree: KinematicTree, inspector: SceneInspector,
+                 scene_collision_geometries: List[CollisionGeometry]):
+        self._tree = kin_tree
+        self._inspector = inspector
+        self._geoms = list(scene_collision_geometries)
+
+    def numLinks(self) -> int:
+        return self._tree.numLinks()
+
+    def numJoints(self) -> int:
+        return self._tree.numJoints()
+
+    def getPositionLowerLimits(self) -> np.ndarray:
+        return self._tree.getPositionLowerLimits()
+
+    def getPositionUpperLimits(self) -> np.ndarray:
+        return self._tree.getPositionUpperLimits()
+
+    def numConfigurationVariables(self) -> int:
+        return self._tree.numConfigurationVariables()
+
+    def getMinimalPlant(self) -> "MinimalPlant":
+        if not self._tree.is_finalized:
+            self._tree.finalize()
+        return MinimalPlant(self._tree.get_minimal_kinematic_tree(), self._geoms,
+                            self._inspector.get_collision_pair_matrix())
+
+    def getKinematicTree(self) -> KinematicTree:
+        return self._tree
+
+    def getSceneInspector(self) -> SceneInspector:
+        return self._inspector
+
+    def getRobotGeometryIds(self) -> List[int]:
+        return self._inspector.robot_geometry_ids
+
+    def getSceneCollisionGeometries(self) -> List[CollisionGeometry]:
+        return self._geoms
+
+    def getCollisionPairMatrix(self) -> np.ndarray:
+        return self._inspector.get_collision_pair_matrix()
+
+    def getSceneCollisionGeometryNames(self) -> List[str]:
+        names = self._inspector.scene_collision_geometry_name_to_geometry_index
+        keys = [""] * len(names)
+        for name, idx in names.items():
+            keys[idx] = name
+        return keys
+
+    def getSceneCollisionGeometryIndexByName(self, name: str) -> int:
+        idx = self._inspector.scene_collision_geometry_name_to_geometry_index.get(name)
+        if idx is None:
+            raise IndexError("Geometry name not found: " + name)
+        return idx
 
 
 # --------------------------------------------------------------------------- scene rules

@@ -1,5 +1,6 @@
 """Plant loader: the reference parser's grouping, traversal and pair rules."""
 import numpy as np
+import pytest
 
 from csdecomp_b200 import scenes
 from csdecomp_b200.plant import CollisionGroup, URDFParser
@@ -46,3 +47,40 @@ def test_edge_scene_keepout():
     assert s.plant.num_scene_geometries == 284
     caps = [g for g in s.plant.scene_collision_geometries if g.type == 3]
     assert len(caps) == 4
+
+
+def test_plant_wrapper(plants):
+    """Plant (minimal_plant.h:42-145) over the parser's outputs gives the
+    parser's MinimalPlant and the reference's accessors."""
+    import os
+    from csdecomp_b200.plant import Plant, URDFParser
+    d = os.path.join(os.path.dirname(__file__), "golden", "loader")
+    p = URDFParser()
+    p.register_package("loader_assets", d)
+    p.parse_directives(os.path.join(d, "cell.yml"))
+    pl = Plant(p.get_kinematic_tree(), p.get_scene_inspector(), p.get_scene_collision_geometries())
+    a = p.get_minimal_plant().arrays()
+    b = pl.getMinimalPlant().arrays()
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    assert pl.numLinks() == 10 and pl.numJoints() == 9 and pl.numConfigurationVariables() == 3
+    assert pl.getRobotGeometryIds() == p.get_scene_inspector().robot_geometry_ids
+    names = pl.getSceneCollisionGeometryNames()
+    assert len(names) == len(p.get_scene_collision_geometries())
+    for i, n in enumerate(names):
+        assert pl.getSceneCollisionGeometryIndexByName(n) == i
+    with pytest.raises(IndexError):
+        pl.getSceneCollisionGeometryIndexByName("no such geometry")
+    np.testing.assert_array_equal(pl.getCollisionPairMatrix(), p.get_scene_inspector().get_collision_pair_matrix())
+
+
+def test_minimal_tree_structs(plants):
+    """MinimalJoint / MinimalLink views agree with the tables."""
+    kt = plants["kinova_on_table"].plant.kin_tree
+    joints, links = kt.joints, kt.links
+    assert len(joints) == kt.num_joints and len(links) == kt.num_links
+    for j in joints:
+        assert links[j.child_link].parent_joint_index == j.index
+        assert j.index in links[j.parent_link].child_joint_index_array
+    assert links[0].parent_joint_index == -1
+    assert sum(l.num_child_joints for l in links) == kt.num_joints
