@@ -126,7 +126,7 @@ class KinematicTree:
         self.joints: List[Joint] = []
         self.link_name_to_index: Dict[str, int] = {}
         self.joint_name_to_index: Dict[str, int] = {}
-        self.is_finalized = False
+        self._finalized = False
         self.joint_idx_to_config_idx: List[int] = []
         self.joint_traversal_sequence: List[int] = []
         self.num_configuration_variables = 0
@@ -137,7 +137,7 @@ class KinematicTree:
     def add_link(self, link: Link) -> int:
         if link.name in self.link_name_to_index:
             raise RuntimeError(f"Duplicate link name detected in URDF. Name : {link.name}")
-        if self.is_finalized:
+        if self._finalized:
             raise RuntimeError("Cannot add link to finalized tree.")
         idx = len(self.links)
         self.links.append(link)
@@ -148,7 +148,7 @@ class KinematicTree:
     def add_joint(self, joint: Joint) -> int:
         if joint.name in self.joint_name_to_index:
             raise RuntimeError("Duplicate joint name detected in URDF.")
-        if self.is_finalized:
+        if self._finalized:
             raise RuntimeError("Cannot add joint to finalized tree.")
         if joint.parent_link == -1 or joint.child_link == -1:
             raise RuntimeError("Parent or child link not found for joint: " + joint.name)
@@ -168,7 +168,7 @@ class KinematicTree:
 
     # kinematic_tree.cpp:82-146
     def finalize(self) -> None:
-        self.is_finalized = True
+        self._finalized = True
         self.num_configuration_variables = 0
         self.joint_idx_to_config_idx = []
         for j in self.joints:
@@ -187,6 +187,54 @@ class KinematicTree:
         self.joint_traversal_sequence = seq
         self.position_lower_limits = [j.position_lower_limit for j in self.joints if j.type != JointType.FIXED]
         self.position_upper_limits = [j.position_upper_limit for j in self.joints if j.type != JointType.FIXED]
+
+    def is_finalized(self) -> bool:
+        return self._finalized
+
+    isFinalized = is_finalized
+
+    # kinematic_tree.cpp:69-80, 148-165
+    def get_link_name(self, index: int) -> str:
+        for name, i in self.link_name_to_index.items():
+            if i == index:
+                return name
+        raise RuntimeError("link index not found")
+
+    def get_link(self, index: int) -> Link:
+        if not 0 <= index < len(self.links):
+            raise IndexError("link index out of range")
+        return self.links[index]
+
+    def get_joint_index(self, name: str) -> int:
+        return self.joint_name_to_index.get(name, -1)
+
+    def get_joint(self, index: int) -> Joint:
+        if not 0 <= index < len(self.joints):
+            raise IndexError("joint index out of range")
+        return self.joints[index]
+
+    def get_links(self) -> List[Link]:
+        return self.links
+
+    def get_joints(self) -> List[Joint]:
+        return self.joints
+
+    def get_leaf_link_indices(self) -> List[int]:
+        return [i for i, l in enumerate(self.links) if not l.child_joints]
+
+    def compute_link_frame_to_world_transforms(self, joint_values) -> List[np.ndarray]:
+        """computeLinkFrameToWorldTransforms (kinematic_tree.cpp:195-240): one
+        4 x 4 link-to-world transform per link, evaluated on the GPU."""
+        if not self._finalized:
+            raise RuntimeError("KinematicTree is not finalized")
+        q = np.asarray(joint_values, np.float32).reshape(-1)
+        if q.size != self.num_configuration_variables:
+            raise ValueError(f"Incorrect number of configuration varialbes added, there are "
+                             f"{self.num_configuration_variables} active joints and {q.size} configuration "
+                             f"values were provided")
+        from .api import ComputeForwardKinematicsCuda
+        tf = ComputeForwardKinematicsCuda(q.reshape(-1, 1), self.get_minimal_kinematic_tree())[0]
+        return [tf[l].copy() for l in range(tf.shape[0])]
 
     def numLinks(self) -> int:
         return len(self.links)
@@ -266,7 +314,7 @@ class MinimalKinematicTree:
 
     @staticmethod
     def from_tree(t: KinematicTree) -> "MinimalKinematicTree":
-        if not t.is_finalized:
+        if not t._finalized:
             raise RuntimeError("KinematicTree is not finalized")
         J = len(t.joints)
         return MinimalKinematicTree(
@@ -410,7 +458,7 @@ class Plant:
         return self._tree.numConfigurationVariables()
 
     def getMinimalPlant(self) -> "MinimalPlant":
-        if not self._tree.is_finalized:
+        if not self._tree._finalized:
             self._tree.finalize()
         return MinimalPlant(self._tree.get_minimal_kinematic_tree(), self._geoms,
                             self._inspector.get_collision_pair_matrix())
@@ -516,7 +564,7 @@ def compute_collision_pairs(tree: KinematicTree, geoms: List[CollisionGeometry])
 def build_plant(tree: KinematicTree, geoms: List[CollisionGeometry],
                 names: Optional[Dict[str, int]] = None) -> Tuple[MinimalPlant, SceneInspector]:
     """finalize_scene + getMinimalPlant for a finalized tree (urdf_parser.cpp:167-206, 485-616)."""
-    if not tree.is_finalized:
+    if not tree._finalized:
         tree.finalize()
     _group_geometries(tree, geoms)
     insp = SceneInspector()
@@ -741,6 +789,22 @@ class URDFParser:
         if self._plant is None:
             raise RuntimeError("No URDF has been parsed yet")
         return self._plant
+
+    # urdf_parser.h:116-131, urdf_parser.cpp:477-483
+    def override_kinematic_tree(self, kinematic_tree: KinematicTree) -> None:
+        self.kinematic_tree = kinematic_tree
+
+    def override_scene_collision_geometries(self, geometries: List[CollisionGeometry]) -> None:
+        self.scene_collision_geometries = list(geometries)
+
+    def build_plant(self) -> "Plant":
+        if not self.kinematic_tree.is_finalized():
+            raise RuntimeError("No URDF has been parsed yet, cannot build plant!")
+        return Plant(self.kinematic_tree, self.inspector, self.scene_collision_geometries)
+
+    overrideKinematicTree = override_kinematic_tree
+    overrideSceneCollisionGeometries = override_scene_collision_geometries
+    buildPlant = build_plant
 
     getMinimalPlant = get_minimal_plant
 

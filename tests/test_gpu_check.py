@@ -304,3 +304,22 @@ def test_broad_phase_leaves_every_verdict_unchanged(arms):
     e_off = csd.CheckEdgesCollisionFreeCuda(a.T, b.T, sc.plant)
     h.set_culling(True)
     np.testing.assert_array_equal(e_on, e_off)
+
+
+def test_tree_link_transforms():
+    """KinematicTree.compute_link_frame_to_world_transforms (GPU FK) equals the
+    batched FK and the oracle's FP64 FK."""
+    import os
+    from csdecomp_b200.plant import URDFParser
+    d = os.path.join(os.path.dirname(__file__), "golden", "loader")
+    p = URDFParser()
+    p.register_package("loader_assets", d)
+    p.parse_directives(os.path.join(d, "cell.yml"))
+    kt = p.get_kinematic_tree()
+    q = np.array([0.3, -0.7, 0.02], np.float32)
+    tfs = kt.compute_link_frame_to_world_transforms(q)
+    assert len(tfs) == kt.numLinks()
+    batched = csd.ComputeForwardKinematicsCuda(q.reshape(-1, 1), p.get_minimal_plant())[0]
+    np.testing.assert_array_equal(np.stack(tfs), batched)
+    ref = O.fk(p.get_minimal_plant(), q.reshape(1, -1), fp64=True).reshape(-1, 4, 4).transpose(0, 2, 1)
+    np.testing.assert_allclose(np.stack(tfs), ref, atol=1e-5)

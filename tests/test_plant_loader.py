@@ -84,3 +84,29 @@ def test_minimal_tree_structs(plants):
         assert j.index in links[j.parent_link].child_joint_index_array
     assert links[0].parent_joint_index == -1
     assert sum(l.num_child_joints for l in links) == kt.num_joints
+
+
+def test_tree_accessors(plants):
+    """KinematicTree and URDFParser accessors of plant_bindings.h:14-63."""
+    import os
+    d = os.path.join(os.path.dirname(__file__), "golden", "loader")
+    p = URDFParser()
+    p.register_package("loader_assets", d)
+    p.parse_directives(os.path.join(d, "cell.yml"))
+    kt = p.get_kinematic_tree()
+    assert kt.is_finalized()
+    i = kt.get_link_index("arm::upper")
+    assert kt.get_link_name(i) == "arm::upper" and kt.get_link(i).name == "arm::upper"
+    j = kt.get_joint_index("arm::elbow")
+    assert j >= 0 and kt.get_joint(j).name == "arm::elbow" and kt.get_joint_index("nope") == -1
+    assert len(kt.get_links()) == 10 and len(kt.get_joints()) == 9
+    leaves = kt.get_leaf_link_indices()
+    assert all(not kt.get_link(l).child_joints for l in leaves)
+    assert kt.get_link_index("post::pole") in leaves
+    with pytest.raises(ValueError):
+        kt.compute_link_frame_to_world_transforms(np.zeros(2))
+    pl = p.build_plant()
+    np.testing.assert_array_equal(pl.getMinimalPlant().arrays()["geom_type"], p.get_minimal_plant().arrays()["geom_type"])
+    p2 = URDFParser()
+    with pytest.raises(RuntimeError):
+        p2.build_plant()
