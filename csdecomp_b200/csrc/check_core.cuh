@@ -257,7 +257,8 @@ static __device__ __forceinline__ Cull broad_phase(const DevPlant& p, const floa
     const float ox = __shfl_sync(kFull, cx, j), oy = __shfl_sync(kFull, cy, j), oz = __shfl_sync(kFull, cz, j);
     const float orr = __shfl_sync(kFull, cr, j);
     const float dx = cx - ox, dy = cy - oy, dz = cz - oz, t = cr + orr;
-    if (cr >= 0.f && orr >= 0.f && fmaf(dz, dz, fmaf(dy, dy, dx * dx)) <= t * t) lw |= 1u << j;
+    // !(d2 > t2): a NaN pose counts as near, so its pairs are tested (and collide) as in the full sweep
+    if (cr >= 0.f && orr >= 0.f && !(fmaf(dz, dz, fmaf(dy, dy, dx * dx)) > t * t)) lw |= 1u << j;
   }
   c.link = lw;
   uint32_t sw = 0;
@@ -270,7 +271,7 @@ static __device__ __forceinline__ Cull broad_phase(const DevPlant& p, const floa
       const float kx = __shfl_sync(kFull, cx, k), ky = __shfl_sync(kFull, cy, k), kz = __shfl_sync(kFull, cz, k);
       const float kr = __shfl_sync(kFull, cr, k);
       const float dx = kx - S.x, dy = ky - S.y, dz = kz - S.z, t = kr + S.w;
-      near |= kr >= 0.f && S.w >= 0.f && fmaf(dz, dz, fmaf(dy, dy, dx * dx)) <= t * t;
+      near |= kr >= 0.f && S.w >= 0.f && !(fmaf(dz, dz, fmaf(dy, dy, dx * dx)) > t * t);
     }
     const uint32_t bits = __ballot_sync(kFull, near);
     if (lane == g) sw = bits;

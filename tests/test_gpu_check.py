@@ -140,6 +140,7 @@ def test_voxel_grid_matches_every_voxel(plants, case):
         gp = plants["movable_block" if case == "movable_block_boxes" else "kinova_on_table"]
         plant, rids, dim = gp.plant, gp.robot_geometry_ids, gp.dim
         q = (gp.lower + (gp.upper - gp.lower) * rng.random((6000, gp.dim))).astype(np.float32)
+    q = np.concatenate([q, np.full((3, dim), np.nan, np.float32)])  # NaN poses collide in both forms
     mixed = 0
     for nv, vr in [(64, 0.05), (3000, 0.02), (20000, 0.01)]:
         near = rng.normal(0, 0.4, (nv // 2, 3))
@@ -148,9 +149,26 @@ def test_voxel_grid_matches_every_voxel(plants, case):
         on = voxel_verdicts(plant, q, vox, vr, rids, True)
         off = voxel_verdicts(plant, q, vox, vr, rids, False)
         np.testing.assert_array_equal(on, off)
-        mixed += 0 < on.mean() < 1
+        assert not on[-3:].any()
+        mixed += 0 < on[:-3].mean() < 1
     assert mixed >= 1
     band_parity(plant, q[:1500], vox, vr, rids)
+
+
+def test_nan_configurations_collide():
+    """A NaN configuration collides (every pair test of the reference's rule
+    fails on NaN), with the link-level broad phase on and off."""
+    sc = scenes.edge_check_scene(keepout=0.8)
+    h = csd.plant_handle(sc.plant)
+    q = sc.random_configs(64, 3)
+    q[::4, 2] = np.nan
+    for cull in (True, False):
+        h.set_culling(cull)
+        v = csd.CheckCollisionFreeCuda(q.T, sc.plant)
+        assert not v[::4].any(), cull
+    h.set_culling(True)
+    ref = O.check_points(sc.plant, q[::4], O.RULE_GPU)
+    assert not ref.any()
 
 
 def test_device_robot_ids_refused(plants):
