@@ -13,7 +13,7 @@
 //                            check of the midpoint with the link-level broad
 //                            phase, distance to the projection (the EI-ZO
 //                            bisection body, bisect_particle)
-//   2. edit_faces_kernel    one block per region: copies the region, drops the
+//   2. edit_faces_kernel    one warp per region: copies the region, drops the
 //                            candidates outside it, then repeatedly takes the
 //                            nearest live candidate (lower index on ties),
 //                            places its face with the segment relaxation of
@@ -54,63 +54,23 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, 3)
   }
 }
 
-// Argmin of dist[0, K) over the block: (value, index), lower index on ties.
-static __device__ __forceinline__ void block_argmin(const float* __restrict__ dist, int K, float* red_v, int* red_i,
-                                                    float* best_v, int* best_s) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-  float bv = FLT_MAX;
-  int bi = 0x7fffffff;
-  for (int i = tid; i < K; i += blockDim.x) {
-    const float v = dist[i];
-    if (v < bv) {  // ascending i: the first of equal values is kept
-      bv = v;
-      bi = i;
-    }
-  }
-  for (int o = 16; o; o >>= 1) {
-    const float ov = __shfl_down_sync(0xffffffffu, bv, o);
-    const int oi = __shfl_down_sync(0xffffffffu, bi, o);
-    if (ov < bv || (ov == bv && oi < bi)) {
-      bv = ov;
-      bi = oi;
-    }
-  }
-  if (lane == 0) {
-    red_v[warp] = bv;
-    red_i[warp] = bi;
-  }
-  __syncthreads();
-  if (tid == 0) {
-    float v = FLT_MAX;
-    int ix = 0x7fffffff;
-    for (int w = 0; w < nw; ++w)
-      if (red_v[w] < v || (red_v[w] == v && red_i[w] < ix)) {
-        v = red_v[w];
-        ix = red_i[w];
-      }
-    *best_v = v;
-    *best_s = ix;
-  }
-  __syncthreads();
-}
-
 // Region r: faces [face_off[r], face_off[r+1]) of A/b, candidates
 // [coll_off[r], coll_off[r+1]) of cols/proj/dist; written at row
-// face_off[r] + coll_off[r] of A_out/b_out. dist is consumed (FLT_MAX marks a
-// candidate that is placed or cut off).
+// face_off[r] + coll_off[r] of A_out/b_out. One warp per region (shuffles and
+// warp barriers only; kEditFaceThreads / 32 regions per block). dist is
+// consumed (FLT_MAX marks a candidate that is placed or cut off). Lane 0
+// computes each face with the coordinate-order arithmetic of the oracle.
 __global__ void __launch_bounds__(kEditFaceThreads)
     edit_faces_kernel(int m, int dim, float margin, const float* __restrict__ starts, const float* __restrict__ ends,
                       const float* __restrict__ A, const float* __restrict__ b, const int* __restrict__ face_off,
                       const int* __restrict__ coll_off, const float* __restrict__ cols,
                       const float* __restrict__ proj, float* __restrict__ dist, float* __restrict__ A_out,
                       float* __restrict__ b_out, int* __restrict__ num_faces) {
-  __shared__ float red_v[kEditFaceThreads / 32];
-  __shared__ int red_i[kEditFaceThreads / 32];
-  __shared__ float face[kMaxDim + 1];
-  __shared__ int best_s;
-  __shared__ float best_v;
-  const int tid = threadIdx.x;
-  for (int r = blockIdx.x; r < m; r += gridDim.x) {
+  __shared__ float face_s[kEditFaceThreads / 32][kMaxDim + 1];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  float* face = face_s[wib];
+  const int nwarps = gridDim.x * (kEditFaceThreads / 32);
+  for (int r = blockIdx.x * (kEditFaceThreads / 32) + wib; r < m; r += nwarps) {
     const int f0 = face_off[r], F0 = face_off[r + 1] - f0;
     const int c0 = coll_off[r], K = coll_off[r + 1] - c0;
     const int64_t row0 = (int64_t)f0 + c0;
@@ -118,13 +78,13 @@ __global__ void __launch_bounds__(kEditFaceThreads)
     float* bo = b_out + row0;
     const float* Ar = A + (int64_t)f0 * dim;
     const float* br = b + f0;
-    for (int i = tid; i < F0 * dim; i += blockDim.x) Ao[i] = Ar[i];
-    for (int i = tid; i < F0; i += blockDim.x) bo[i] = br[i];
+    for (int i = lane; i < F0 * dim; i += 32) Ao[i] = Ar[i];
+    for (int i = lane; i < F0; i += 32) bo[i] = br[i];
     const float* cr = cols + (int64_t)c0 * dim;
     const float* pr = proj + (int64_t)c0 * dim;
     float* dr = dist + c0;
     // candidates not strictly inside the original region are never placed
-    for (int i = tid; i < K; i += blockDim.x) {
+    for (int i = lane; i < K; i += 32) {
       const float* x = cr + (int64_t)i * dim;
       bool inside = dr[i] < FLT_MAX;
       for (int f = 0; f < F0 && inside; ++f) {
@@ -134,17 +94,35 @@ __global__ void __launch_bounds__(kEditFaceThreads)
       }
       if (!inside) dr[i] = FLT_MAX;
     }
-    __syncthreads();
+    __syncwarp();
     const float* ls = starts + (int64_t)r * dim;
     const float* le = ends + (int64_t)r * dim;
     int nf = F0;
     for (;;) {
-      block_argmin(dr, K, red_v, red_i, &best_v, &best_s);
-      if (!(best_v < FLT_MAX)) break;
-      if (tid == 0) {
-        const int s = best_s;
-        const float* c = cr + (int64_t)s * dim;
-        const float* q = pr + (int64_t)s * dim;
+      // nearest live candidate, lower index on ties
+      float bv = FLT_MAX;
+      int bi = 0x7fffffff;
+      for (int i = lane; i < K; i += 32) {
+        const float v = dr[i];
+        if (v < bv) {  // ascending i: the first of equal values is kept
+          bv = v;
+          bi = i;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o; o >>= 1) {
+        const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ov < bv || (ov == bv && oi < bi)) {
+          bv = ov;
+          bi = oi;
+        }
+      }
+      if (!(bv < FLT_MAX)) break;
+      if (lane == 0) {
+        const int sidx = bi;
+        const float* c = cr + (int64_t)sidx * dim;
+        const float* q = pr + (int64_t)sidx * dim;
         float a[kMaxDim];
         float n2 = 0.f;
         for (int k = 0; k < dim; ++k) {
@@ -173,11 +151,11 @@ __global__ void __launch_bounds__(kEditFaceThreads)
         }
         bo[nf] = bb;
         face[dim] = bb;
-        dr[s] = FLT_MAX;
+        dr[sidx] = FLT_MAX;
       }
-      __syncthreads();
+      __syncwarp();
       const float bb = face[dim];
-      for (int i = tid; i < K; i += blockDim.x) {
+      for (int i = lane; i < K; i += 32) {
         if (!(dr[i] < FLT_MAX)) continue;
         const float* x = cr + (int64_t)i * dim;
         float v = 0.f;
@@ -185,10 +163,10 @@ __global__ void __launch_bounds__(kEditFaceThreads)
         if (!(__fsub_rn(v, bb) < 0.f)) dr[i] = FLT_MAX;
       }
       ++nf;
-      __syncthreads();
+      __syncwarp();
     }
-    if (tid == 0) num_faces[r] = nf;
-    __syncthreads();
+    if (lane == 0) num_faces[r] = nf;
+    __syncwarp();
   }
 }
 
@@ -350,7 +328,7 @@ csd_status_t csd_edit_regions(csd_plant_t plant, const float* collisions, const 
   }
   CSD_CUDA_TRY(cudaGetLastError());
   // 2. faces, one block per region
-  const int fgrid = std::min(m, 8 * device_sm_count());
+  const int fgrid = std::min((m + kEditFaceThreads / 32 - 1) / (kEditFaceThreads / 32), 8 * device_sm_count());
   edit_faces_kernel<<<fgrid, kEditFaceThreads, 0, st>>>(m, d, options->configuration_margin, ls, le, Ad, bd, foff,
                                                         coffd, cols, proj, dist, Ao, bo, nfd);
   CSD_CUDA_TRY(cudaGetLastError());
