@@ -1092,6 +1092,8 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
     set_error("a tensor-core barrier wait timed out in the scoring stage");
     return CSD_ERR_CUDA;
   }
+  for (csd_plant_t pl : h->plants)
+    if ((s = plant_status(pl, st))) return s;
   h->host_slots.assign(slots.begin(), slots.end());
   size_t aoff = 0;
   for (int i = 0; i < n; ++i) {

@@ -4,7 +4,7 @@
 #include <cstring>
 #include <vector>
 
-#include "csd_internal.h"
+#include "check_core.cuh"
 
 namespace csd {
 csd_status_t launch_pair(int ta, const float* g_dev, int tb, uint8_t* out, cudaStream_t st);
@@ -29,6 +29,22 @@ csd_status_t build_voxel_tables(csd_plant_s* p, const int32_t* ids, int nr, std:
   }
   tab->insert(tab->end(), other.begin(), other.end());
   *num_other = (int)other.size();
+  return CSD_OK;
+}
+
+// Reads and clears the plant's status word once the stream's work is done:
+// nonzero when a block's bounded wait for the static-table staging gave up,
+// in which case that block returned without checking its configurations.
+csd_status_t plant_status(const csd_plant_s* p, cudaStream_t st) {
+  int v = 0;
+  CSD_CUDA_TRY(cudaMemcpyAsync(&v, p->dp.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CSD_CUDA_TRY(cudaStreamSynchronize(st));
+  if (v) {
+    CSD_CUDA_TRY(cudaMemsetAsync(p->dp.status, 0, sizeof(int), st));
+    CSD_CUDA_TRY(cudaStreamSynchronize(st));
+    set_error("a check kernel's bounded wait for the static-table staging gave up; the call's results are incomplete");
+    return CSD_ERR_CUDA;
+  }
   return CSD_OK;
 }
 
@@ -117,7 +133,7 @@ csd_status_t csd_check_points(csd_plant_t p, const float* q, int64_t n, const fl
   if (flags == CSD_PTR_DEVICE) {
     s = launch_check_points(p, q, n, vt, out, st);
     if (s) return s;
-    if (nv > 0 && nr > 0) CSD_CUDA_TRY(cudaStreamSynchronize(st));  // voxel tables are reused per call
+    if (nv > 0 && nr > 0) return plant_status(p, st);  // synchronises: voxel tables are reused per call
     return CSD_OK;
   }
   if ((s = p->in_buf.reserve((size_t)n * d * sizeof(float) + 16))) return s;
@@ -125,8 +141,29 @@ csd_status_t csd_check_points(csd_plant_t p, const float* q, int64_t n, const fl
   if (n * d) CSD_CUDA_TRY(cudaMemcpyAsync(p->in_buf.ptr, q, (size_t)n * d * sizeof(float), cudaMemcpyHostToDevice, st));
   if ((s = launch_check_points(p, p->in_buf.as<float>(), n, vt, p->out_buf.as<uint8_t>(), st))) return s;
   if (n) CSD_CUDA_TRY(cudaMemcpyAsync(out, p->out_buf.ptr, (size_t)n, cudaMemcpyDeviceToHost, st));
-  CSD_CUDA_TRY(cudaStreamSynchronize(st));
-  return CSD_OK;
+  return plant_status(p, st);
+}
+
+csd_status_t csd_plant_status(csd_plant_t p, int32_t* timed_out, void* stream) {
+  CSD_CHECK(p && timed_out, CSD_ERR_INVALID, "null argument");
+  DeviceGuard g(p->device);
+  const csd_status_t s = plant_status(p, (cudaStream_t)stream);
+  *timed_out = s == CSD_ERR_CUDA ? 1 : 0;
+  return s == CSD_ERR_CUDA ? CSD_OK : s;
+}
+
+csd_status_t csd_plant_wait_selftest(csd_plant_t p, int32_t polls, int32_t* reported) {
+  CSD_CHECK(p && reported && polls >= 1, CSD_ERR_INVALID, "bad arguments");
+  DeviceGuard g(p->device);
+  *reported = 0;
+  staging_wait_selftest_kernel<<<1, 128, 0, 0>>>(p->dp.status, (long long)polls);
+  CSD_CUDA_TRY(cudaGetLastError());
+  const csd_status_t s = plant_status(p, 0);
+  if (s == CSD_ERR_CUDA) {
+    *reported = 1;
+    return CSD_OK;
+  }
+  return s;
 }
 
 csd_status_t csd_check_edges(csd_plant_t p, const float* starts, const float* ends, int64_t n, float step, int32_t mode,
@@ -157,8 +194,7 @@ csd_status_t csd_check_edges(csd_plant_t p, const float* starts, const float* en
     CSD_CUDA_TRY(cudaMemcpyAsync(out, p->out_buf.ptr, (size_t)n, cudaMemcpyDeviceToHost, st));
     if (pts) CSD_CUDA_TRY(cudaMemcpyAsync(pts, p->out_buf2.ptr, (size_t)n * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   }
-  CSD_CUDA_TRY(cudaStreamSynchronize(st));
-  return CSD_OK;
+  return plant_status(p, st);
 }
 
 csd_status_t csd_check_edges_ranked(csd_plant_t p, csd_mlp_t mlp, int32_t net, const float* starts, const float* ends,
@@ -227,8 +263,7 @@ csd_status_t csd_check_edges_ranked(csd_plant_t p, csd_mlp_t mlp, int32_t net, c
     CSD_CUDA_TRY(cudaMemcpyAsync(out, od, (size_t)n, cudaMemcpyDeviceToHost, st));
     if (pts) CSD_CUDA_TRY(cudaMemcpyAsync(pts, pd, (size_t)n * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
   }
-  CSD_CUDA_TRY(cudaStreamSynchronize(st));
-  return CSD_OK;
+  return plant_status(p, st);
 }
 
 csd_status_t csd_visibility_graph(csd_plant_t p, const float* nodes, int32_t n, float step, uint8_t* adjacency,
@@ -251,8 +286,7 @@ csd_status_t csd_visibility_graph(csd_plant_t p, const float* nodes, int32_t n, 
                               p->out_buf.as<uint8_t>(), nullptr, p->counter.as<unsigned int>(), st, n)))
     return s;
   CSD_CUDA_TRY(cudaMemcpyAsync(adjacency, p->out_buf.ptr, (size_t)E, cudaMemcpyDeviceToHost, st));
-  CSD_CUDA_TRY(cudaStreamSynchronize(st));
-  return CSD_OK;
+  return plant_status(p, st);
 }
 
 csd_status_t csd_pair_collision_free(int32_t ta, const float* da, const float* XLBa, const float* XWLa, int32_t tb,

@@ -84,6 +84,18 @@ static __device__ __forceinline__ unsigned smem_addr(const void* p) {
 // invalidates the barrier so a later call can stage another plant. Returns
 // false (and sets p.status) if the wait does not complete within kSpinLimit
 // polls. Every thread of the block must call it.
+// Polls an mbarrier phase at most `limit` times; 1 when it completed.
+static __device__ __forceinline__ unsigned poll_mbarrier(uint64_t* bar, unsigned parity, long long limit) {
+  unsigned done = 0;
+  for (long long i = 0; i < limit && !done; ++i)
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+  return done;
+}
+
 static __device__ bool stage_statics(const DevPlant& p, float4* dst, uint64_t* bar) {
   const unsigned bytes = (unsigned)p.static_bytes;
   if (bytes == 0) return true;
@@ -104,28 +116,33 @@ static __device__ bool stage_statics(const DevPlant& p, float4* dst, uint64_t* b
     }
   }
   __syncthreads();
-  unsigned done = 0;
-  for (long long i = 0; i < kSpinLimit && !done; ++i) {
-    asm volatile(
-        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
-        : "=r"(done)
-        : "r"(smem_addr(bar))
-        : "memory");
-  }
-  if (!done) {
-    atomicExch(p.status, 1);
+  const unsigned done = poll_mbarrier(bar, 0, kSpinLimit);
+  // block-uniform outcome: every thread has seen the phase complete, or the block gives up together
+  if (!__syncthreads_and(done)) {
+    if (threadIdx.x == 0) atomicExch(p.status, 1);
     // wait (bounded) once more for the copy still in flight before the block leaves
-    for (long long i = 0; i < kSpinLimit && !done; ++i)
-      asm volatile(
-          "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
-          : "=r"(done)
-          : "r"(smem_addr(bar))
-          : "memory");
+    poll_mbarrier(bar, 0, kSpinLimit);
     return false;
   }
-  __syncthreads();  // every thread has seen the phase complete: the barrier can be reused
   if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
   return true;
+}
+
+// Self-test of the bounded wait and its reporting: an mbarrier expecting 16
+// bytes that no copy ever delivers, polled `limit` times; the block then gives
+// up exactly as stage_statics does and sets the plant's status word. No
+// asynchronous operation is in flight when the block leaves.
+static __global__ void staging_wait_selftest_kernel(int* status, long long limit) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar)), "r"(16u)
+                 : "memory");
+  }
+  __syncthreads();
+  const unsigned done = poll_mbarrier(&bar, 0, limit);
+  if (!__syncthreads_and(done) && threadIdx.x == 0) atomicExch(status, 1);
 }
 
 // ---------------------------------------------------------------------- FK

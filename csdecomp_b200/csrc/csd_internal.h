@@ -109,6 +109,9 @@ struct VoxelTables {
 
 csd_status_t build_voxel_tables(csd_plant_s* p, const int32_t* robot_ids, int nr, std::vector<uint32_t>* tab,
                                 int* num_other);
+// Synchronises st, then reads and clears the plant's status word (capi.cu):
+// CSD_ERR_CUDA when a block's bounded staging wait gave up since the last read.
+csd_status_t plant_status(const csd_plant_s* p, cudaStream_t st);
 // Cell edge of the voxel grid for these tables (tab from build_voxel_tables):
 // twice the median radius of the robot spheres checked against voxels plus
 // the voxel radius.

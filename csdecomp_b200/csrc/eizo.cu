@@ -313,7 +313,7 @@ csd_status_t csd_inflator_inflate(csd_inflator_t h, const float* ls, const float
   const int F = h->host_nf[0];
   CSD_CUDA_TRY(cudaMemcpyAsync(A_out, h->A.ptr, (size_t)F * d * 4, cudaMemcpyDeviceToHost, st));
   CSD_CUDA_TRY(cudaMemcpyAsync(b_out, h->b.ptr, (size_t)F * 4, cudaMemcpyDeviceToHost, st));
-  CSD_CUDA_TRY(cudaStreamSynchronize(st));
+  if ((s = plant_status(p, st))) return s;
   *num_faces = F;
   if (num_iters) *num_iters = nit;
   return CSD_OK;
@@ -551,7 +551,7 @@ extern "C" csd_status_t csd_eizo_noalloc(csd_plant_t plant, const float* ls, con
   }
   CSD_CUDA_TRY(cudaMemcpyAsync(A_out, A, (size_t)nf_host * d * 4, cudaMemcpyDeviceToHost, st));
   CSD_CUDA_TRY(cudaMemcpyAsync(b_out, b, (size_t)nf_host * 4, cudaMemcpyDeviceToHost, st));
-  CSD_CUDA_TRY(cudaStreamSynchronize(st));
+  if ((s = plant_status(plant, st))) return s;
   *num_faces = nf_host;
   if (num_iters) *num_iters = nit;
   return CSD_OK;

@@ -130,6 +130,20 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* desc, csd_plant_t* out);
 csd_status_t csd_plant_destroy(csd_plant_t plant);
 csd_status_t csd_plant_info(csd_plant_t plant, csd_plant_info_t* info);
 
+/* Bounded waits: each check kernel stages the plant's static tables into
+ * shared memory behind an mbarrier whose wait gives up after a bounded number
+ * of polls; the block then returns without checking its configurations and
+ * sets the plant's status word. Host-pointer calls (and csd_eizo,
+ * csd_inflator_inflate, csd_batch_inflate, csd_edit_regions) read and clear it
+ * before returning and fail with CSD_ERR_CUDA; device-pointer callers query
+ * it here after their stream's work (timed_out = 1: results since the last
+ * query are incomplete). Synchronises `stream`. */
+csd_status_t csd_plant_status(csd_plant_t plant, int32_t* timed_out, void* stream);
+/* Self-test of that path (no fault, no hang): one block polls `polls` times an
+ * mbarrier that nothing completes, gives up as the staging does and sets the
+ * status word; reported = 1 when the host read it back (and cleared it). */
+csd_status_t csd_plant_wait_selftest(csd_plant_t plant, int32_t polls, int32_t* reported);
+
 /* Forward kinematics: computeForwardKinematicsCuda,
  * csdecomp/src/plant/cuda_forward_kinematics.cu:92-129 (device-pointer form:
  * executeForwardKinematicsKernel, :79-90). transforms: [n][num_links][16]. */

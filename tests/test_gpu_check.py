@@ -341,3 +341,21 @@ def test_tree_link_transforms():
     np.testing.assert_array_equal(np.stack(tfs), batched)
     ref = O.fk(p.get_minimal_plant(), q.reshape(1, -1), fp64=True).reshape(-1, 4, 4).transpose(0, 2, 1)
     np.testing.assert_allclose(np.stack(tfs), ref, atol=1e-5)
+
+
+def test_staging_wait_gives_up_and_is_reported(plants):
+    """The bounded mbarrier wait gives up (nothing completes it), the block
+    sets the plant's status word, the host reads and clears it, and the
+    context stays usable."""
+    import ctypes
+    from csdecomp_b200 import _capi as C
+    gp = plants["movable_block"]
+    h = csd.plant_handle(gp.plant)
+    rep = ctypes.c_int32(0)
+    assert C.lib().csd_plant_wait_selftest(h.handle, 2000, ctypes.byref(rep)) == C.CSD_OK
+    assert rep.value == 1
+    t = ctypes.c_int32(1)
+    assert C.lib().csd_plant_status(h.handle, ctypes.byref(t), None) == C.CSD_OK and t.value == 0
+    rng = np.random.default_rng(4)
+    q = (gp.lower + (gp.upper - gp.lower) * rng.random((500, gp.dim))).astype(np.float32)
+    band_parity(gp.plant, q)
