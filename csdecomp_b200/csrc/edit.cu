@@ -327,7 +327,7 @@ csd_status_t csd_edit_regions(csd_plant_t plant, const float* collisions, const 
                                                                        cols, proj, dist);
   }
   CSD_CUDA_TRY(cudaGetLastError());
-  // 2. faces, one block per region
+  // 2. faces, one warp per region
   const int fgrid = std::min((m + kEditFaceThreads / 32 - 1) / (kEditFaceThreads / 32), 8 * device_sm_count());
   edit_faces_kernel<<<fgrid, kEditFaceThreads, 0, st>>>(m, d, options->configuration_margin, ls, le, Ad, bd, foff,
                                                         coffd, cols, proj, dist, Ao, bo, nfd);
