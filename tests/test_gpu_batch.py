@@ -88,3 +88,26 @@ def test_every_sampler_variant_gives_the_same_regions():
         for g, r in zip(got, ref):
             np.testing.assert_array_equal(g.A(), r.A(), err_msg=f"variant {v}")
             np.testing.assert_array_equal(g.b(), r.b(), err_msg=f"variant {v}")
+
+
+def test_autotuned_batch_reports_and_matches_fixed_shapes():
+    """An autotuned batch reports its choices (the tuned sampler variant, the
+    larger-staging variant kept for regions that outgrow it, the variant the
+    last iteration ran) and yields the regions of a batch with fixed shapes."""
+    s7 = scenes.arm_scene(31, num_spheres=40, num_capsules=2, num_world_boxes=30, num_world_spheres=30, keepout=0.8)
+    opt = csd.EizoOptions(num_particles=600, mixing_steps=20, max_iterations=40)
+    e7 = free_edges(s7, 3, 0.3, 5)
+    slots = [0, 0, 0]
+    tuned = csd.BatchedEdgeInflator([s7.plant], opt, max_slots=3, face_capacity=400, autotune_iterations=2)
+    got = tuned.inflate(slots, [e[0] for e in e7], [e[1] for e in e7], [box(s7)] * 3)
+    t = tuned.tuning()
+    names = csd.BatchedEdgeInflator.SAMPLE_VARIANTS
+    assert t["sample_variant"] in names and t["large_region_variant"] in names
+    assert t["last_run_variant"] in (t["sample_variant"], t["large_region_variant"])
+    assert len(t["sample_ms"]) == len(names) and all(v > 0 for v in t["sample_ms"].values())
+    fixed = csd.BatchedEdgeInflator([s7.plant], opt, max_slots=3, face_capacity=400, autotune_iterations=0)
+    fixed.set_shapes(0, 32)
+    ref = fixed.inflate(slots, [e[0] for e in e7], [e[1] for e in e7], [box(s7)] * 3)
+    for g, r in zip(got, ref):
+        np.testing.assert_array_equal(g.A(), r.A())
+        np.testing.assert_array_equal(g.b(), r.b())
