@@ -595,7 +595,9 @@ class BatchedEdgeInflator:
                        "2 faces/trip, 3 blocks/SM", "4 faces/trip, 2 blocks/SM", "4 faces/trip, 3 blocks/SM",
                        "1 packed face pair/trip, 2 blocks/SM", "2 packed face pairs/trip, 2 blocks/SM",
                        "1 packed face pair/trip, 3 blocks/SM", "2 packed face pairs/trip, 3 blocks/SM",
-                       "1 face/trip, 4 blocks/SM", "2 faces/trip, 4 blocks/SM")
+                       "1 face/trip, 4 blocks/SM", "2 faces/trip, 4 blocks/SM",
+                       "1 face row/trip, 3 blocks/SM", "2 face rows/trip, 3 blocks/SM",
+                       "1 face row/trip, 4 blocks/SM", "1 face row/trip, 2 blocks/SM")
     CHECK_ITEM_CAPS = (32, 128, 512)
 
     def __init__(self, plants: Sequence[MinimalPlant], options: EizoOptions, max_slots: int,

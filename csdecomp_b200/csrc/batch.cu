@@ -61,7 +61,8 @@ struct BatchIter {    // device-side iteration state
   int num_act;        // length of the active-slot list of iteration k
   int max_nf8;        // most faces of an active slot with dim <= 8
   int max_nf16;       // most faces of an active slot with dim > 8
-  int pad[2];
+  int sample_next;    // sampler work items claimed past the first one per block (zeroed before each launch)
+  int pad;
 };
 
 struct BatchArgs {
@@ -117,25 +118,29 @@ static __device__ __forceinline__ int item_size(int64_t total, int cap, int nw) 
 }
 
 // ------------------------------------------------------------------ kernels
-// Chains of the active slots in work items (slot, chunk of chains); a block
-// takes a contiguous run of items, stages each new slot's region (At, b) in
-// shared memory and runs its chains G lanes per chain (G from the total
-// chain count: 8 when the batch is full, up to 32 in the tail).
-template <int U, int MINB, bool PK = false>
+// Chains of the active slots in work items (slot, chunk of chains), handed
+// out as a queue: block b starts with item b and claims the next unclaimed
+// item (it->sample_next, zeroed before the launch) whenever it finishes one,
+// so blocks that drew chains of large regions (a slot's cost grows with its
+// faces and dimension) do not hold up the launch while others idle. A block
+// stages each new slot's region (At, b) in shared memory and runs its chains
+// G lanes per chain (G from the total chain count: 8 when the batch is full,
+// up to 32 in the tail). Each chain's draws and output row follow from its
+// index alone, so the order in which blocks take items changes no sample.
+template <int U, int MINB, int LAY = kLayStrided>
 __global__ void __launch_bounds__(256, MINB) batch_sample_kernel(BatchArgs a) {
   extern __shared__ __align__(16) float smf[];  // the face loop reads float2/float4 vectors
+  __shared__ int next_item;
   const int N = a.n_tab[a.it->k];
   const int64_t total = (int64_t)a.it->num_act * N;
   const int G = group_width(total, (int64_t)gridDim.x * (blockDim.x >> 5));
-  int64_t c = total / (4 * (int64_t)gridDim.x);
+  int64_t c = total / (16 * (int64_t)gridDim.x);
   c = c < 32 ? 32 : c > 1024 ? 1024 : c;
   const int chunk = (int)(c / 32) * 32;
   const int ips = (N + chunk - 1) / chunk;
-  const int64_t items = (int64_t)a.it->num_act * ips;
-  const int64_t per_block = (items + gridDim.x - 1) / gridDim.x;
-  const int64_t i0 = blockIdx.x * per_block, i1 = min(items, i0 + per_block);
+  const int items = a.it->num_act * ips;  // at most slots * N / 32
   int staged = -1;
-  for (int64_t it = i0; it < i1; ++it) {
+  for (int it = blockIdx.x; it < items;) {
     const int slot = a.act[it / ips], first = (int)(it % ips) * chunk, last = min(N, first + chunk);
     const SlotState& S = a.slots[slot];
     const int dim = S.dim, F = S.nf;
@@ -144,22 +149,34 @@ __global__ void __launch_bounds__(256, MINB) batch_sample_kernel(BatchArgs a) {
     const float* ls = a.fpool + S.seg_off;
     float* out = a.fpool + S.smp_off;
     using SC = StageCfg<MINB>;
-    const bool fits = F <= (dim <= 8 ? SC::f8 : SC::f16);
+    constexpr bool rows = LAY == kLayRows;
+    const bool fits = F <= (dim <= 8 ? (rows ? SC::r8 : SC::f8) : (rows ? SC::r16 : SC::f16));
     if (fits && staged != slot) {
       __syncthreads();  // the previous slot's chains are done with the buffer
-      if (dim <= 8)
-        stage_polytope<8, SC::f8>(At, a.capacity, b, F, dim, smf);
-      else
-        stage_polytope<16, SC::f16>(At, a.capacity, b, F, dim, smf);
+      if (rows) {
+        if (dim <= 8)
+          stage_rows<8>(At, a.capacity, b, F, dim, smf);
+        else
+          stage_rows<16>(At, a.capacity, b, F, dim, smf);
+      } else {
+        if (dim <= 8)
+          stage_polytope<8, SC::f8>(At, a.capacity, b, F, dim, smf);
+        else
+          stage_polytope<16, SC::f16>(At, a.capacity, b, F, dim, smf);
+      }
       __syncthreads();
       staged = slot;
     }
     if (dim <= 8)
-      sample_range<8, U, PK, SC::f8, SC::f16>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u,
-                                              out, G, smf, fits);
-    else
-      sample_range<16, U, PK, SC::f8, SC::f16>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u,
+      sample_range<8, U, LAY, SC::f8, SC::f16>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u,
                                                out, G, smf, fits);
+    else
+      sample_range<16, U, LAY, SC::f8, SC::f16>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u,
+                                                out, G, smf, fits);
+    if (threadIdx.x == 0) next_item = gridDim.x + atomicAdd(&a.it->sample_next, 1);
+    __syncthreads();
+    it = next_item;
+    __syncthreads();  // every thread has read next_item before thread 0 writes the next one
   }
 }
 
@@ -587,7 +604,8 @@ __global__ void __launch_bounds__(1024) batch_compact_sorted_kernel(BatchArgs a)
 }
 
 // Sampler variants the autotuner chooses from: U faces (packed: U face
-// pairs) per lane and trip, MINB resident blocks per SM (register cap).
+// pairs) per lane and trip, MINB resident blocks per SM (register cap), the
+// staged layout (transposed columns, packed column pairs, face rows).
 using SampleFn = void (*)(BatchArgs);
 struct SampleVariant {
   SampleFn fn;
@@ -595,13 +613,21 @@ struct SampleVariant {
   size_t smem;   // staging buffer (StageCfg<minb>::bytes)
   int f8, f16;   // faces staged for dim <= 8 / <= 16
 };
-#define CSD_SAMPLE_VARIANT(U, MINB, PK) \
-  { batch_sample_kernel<U, MINB, PK>, U, MINB, StageCfg<MINB>::bytes, StageCfg<MINB>::f8, StageCfg<MINB>::f16 }
+#define CSD_SAMPLE_VARIANT(U, MINB, LAY)                                                    \
+  {                                                                                         \
+    batch_sample_kernel<U, MINB, LAY>, U, MINB, StageCfg<MINB>::bytes,                      \
+        LAY == kLayRows ? StageCfg<MINB>::r8 : StageCfg<MINB>::f8,                          \
+        LAY == kLayRows ? StageCfg<MINB>::r16 : StageCfg<MINB>::f16                         \
+  }
 static const SampleVariant kSampleVariants[] = {
-    CSD_SAMPLE_VARIANT(1, 2, false), CSD_SAMPLE_VARIANT(2, 2, false), CSD_SAMPLE_VARIANT(1, 3, false),
-    CSD_SAMPLE_VARIANT(2, 3, false), CSD_SAMPLE_VARIANT(4, 2, false), CSD_SAMPLE_VARIANT(4, 3, false),
-    CSD_SAMPLE_VARIANT(1, 2, true),  CSD_SAMPLE_VARIANT(2, 2, true),  CSD_SAMPLE_VARIANT(1, 3, true),
-    CSD_SAMPLE_VARIANT(2, 3, true),  CSD_SAMPLE_VARIANT(1, 4, false), CSD_SAMPLE_VARIANT(2, 4, false),
+    CSD_SAMPLE_VARIANT(1, 2, kLayStrided), CSD_SAMPLE_VARIANT(2, 2, kLayStrided),
+    CSD_SAMPLE_VARIANT(1, 3, kLayStrided), CSD_SAMPLE_VARIANT(2, 3, kLayStrided),
+    CSD_SAMPLE_VARIANT(4, 2, kLayStrided), CSD_SAMPLE_VARIANT(4, 3, kLayStrided),
+    CSD_SAMPLE_VARIANT(1, 2, kLayPacked),  CSD_SAMPLE_VARIANT(2, 2, kLayPacked),
+    CSD_SAMPLE_VARIANT(1, 3, kLayPacked),  CSD_SAMPLE_VARIANT(2, 3, kLayPacked),
+    CSD_SAMPLE_VARIANT(1, 4, kLayStrided), CSD_SAMPLE_VARIANT(2, 4, kLayStrided),
+    CSD_SAMPLE_VARIANT(1, 3, kLayRows),    CSD_SAMPLE_VARIANT(2, 3, kLayRows),
+    CSD_SAMPLE_VARIANT(1, 4, kLayRows),    CSD_SAMPLE_VARIANT(1, 2, kLayRows),
 };
 #undef CSD_SAMPLE_VARIANT
 constexpr int kNumSampleVariants = (int)(sizeof(kSampleVariants) / sizeof(kSampleVariants[0]));
@@ -671,6 +697,7 @@ namespace {
 // autotuner has just run it).
 void launch_iteration(csd_batch_s* h, int num_slots, const BatchArgs& a, cudaStream_t s, cudaEvent_t* ev,
                       bool skip_sample = false) {
+  if (!skip_sample) cudaMemsetAsync(&a.it->sample_next, 0, sizeof(int), s);  // the sampler's work queue
   if (ev) cudaEventRecord(ev[0], s);
   if (!skip_sample)
     kSampleVariants[h->run_variant].fn<<<h->sample_grid[h->run_variant], 256, kSampleVariants[h->run_variant].smem,
@@ -790,6 +817,9 @@ csd_status_t csd_batch_create(const csd_plant_t* plants, int32_t num_plants, int
     h->thr_tab.push_back((1 - o->tau) * o->epsilon * M);
   }
   h->n_max = *std::max_element(h->n_tab.begin(), h->n_tab.end());
+  // the sampler numbers its work items (slot, 32 or more chains) with 32-bit integers
+  CSD_CHECK((int64_t)max_slots * ((h->n_max + 31) / 32) + 4096 < (int64_t)INT32_MAX, CSD_ERR_CAPACITY,
+            "too many slots times samples per iteration");
   h->sm = max_static <= kStaticSmemLimit;
   h->static_floats = h->sm ? max_static / 4 : 0;
   h->check_smem = (size_t)max_wf * sizeof(float) * kWarpsPerBlock + (h->sm ? (size_t)max_static : 0);
@@ -1001,6 +1031,7 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
       for (cudaEvent_t& e : tev) CSD_CUDA_TRY(cudaEventCreate(&e));
       int j = 0;
       for (int v = 0; v < kNumSampleVariants; ++v, ++j) {
+        cudaMemsetAsync(&a.it->sample_next, 0, sizeof(int), st);
         cudaEventRecord(tev[2 * j], st);
         kSampleVariants[v].fn<<<h->sample_grid[v], 256, kSampleVariants[v].smem, st>>>(a);
         cudaEventRecord(tev[2 * j + 1], st);
@@ -1035,8 +1066,11 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
         h->run_variant = bs;
         // for slots whose faces outgrow bs's staging: the fastest variant with more staging room
         int bl = -1;
-        for (int v = 0; v < kNumSampleVariants; ++v)
-          if (kSampleVariants[v].f16 > kSampleVariants[bs].f16 && (bl < 0 || h->tune_ms[v] < h->tune_ms[bl])) bl = v;
+        for (int v = 0; v < kNumSampleVariants; ++v) {
+          const SampleVariant &cv = kSampleVariants[v], &tv = kSampleVariants[bs];
+          const bool roomier = cv.f8 >= tv.f8 && cv.f16 >= tv.f16 && (cv.f8 > tv.f8 || cv.f16 > tv.f16);
+          if (roomier && (bl < 0 || h->tune_ms[v] < h->tune_ms[bl])) bl = v;
+        }
         h->large_variant = bl >= 0 ? bl : bs;
         if (!a.mlp_wb) h->cfg_max = kCheckItemCaps[bc];
         a.cfg_max = h->cfg_max;

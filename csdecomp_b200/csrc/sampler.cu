@@ -48,7 +48,8 @@ __global__ void __launch_bounds__(128) hit_and_run_kernel(const float* __restric
 // Group-per-chain sampler over one polytope given transposed (At[k * ldt +
 // f]); the face count is read on the device. Used by the inflator, whose
 // region grows to hundreds of faces: the polytope is staged in shared memory
-// once per block and the lanes of a group share the face loop.
+// once per block (as face rows while they fit, else as transposed columns)
+// and the lanes of a group share the face loop.
 __global__ void __launch_bounds__(256) hit_and_run_group_kernel(const float* __restrict__ At, int ldt,
                                                                 const float* __restrict__ b,
                                                                 const int* __restrict__ num_faces_dev, int dim,
@@ -61,12 +62,26 @@ __global__ void __launch_bounds__(256) hit_and_run_group_kernel(const float* __r
   const int per = (S + gridDim.x - 1) / gridDim.x;
   const int first = blockIdx.x * per, last = min(S, first + per);
   if (first >= last) return;
+  constexpr int rows8 = (int)(kStageBytes / (kRowStride<8> * sizeof(float)));
+  constexpr int rows16 = (int)(kStageBytes / (kRowStride<16> * sizeof(float)));
   if (dim <= 8) {
+    if (F <= rows8) {
+      stage_rows<8>(At, ldt, b, F, dim, smf);
+      __syncthreads();
+      sample_range<8, 1, kLayRows>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out, G, smf, true);
+      return;
+    }
     const bool staged = F <= kStageFaces8;
     if (staged) stage_polytope<8, kStageFaces8>(At, ldt, b, F, dim, smf);
     __syncthreads();
     sample_range<8, 1>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out, G, smf, staged);
   } else {
+    if (F <= rows16) {
+      stage_rows<16>(At, ldt, b, F, dim, smf);
+      __syncthreads();
+      sample_range<16, 1, kLayRows>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out, G, smf, true);
+      return;
+    }
     const bool staged = F <= kStageFaces16;
     if (staged) stage_polytope<16, kStageFaces16>(At, ldt, b, F, dim, smf);
     __syncthreads();

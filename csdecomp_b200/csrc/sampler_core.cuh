@@ -58,14 +58,17 @@ __device__ __forceinline__ bool run_chain(const float* __restrict__ Ap, const fl
 // serial order, and the theta bounds are max/min reductions, which do not
 // depend on the order, so every chain ends bit for bit where run_chain ends.
 // At is the face matrix transposed, At[k * stride + f], with the stride ST
-// when ST > 0 (a shared-memory copy) and ldt otherwise. x is replicated in
+// when ST > 0 (a shared-memory copy) and ldt otherwise. ROWS: At is instead a
+// face-row copy (stage_rows: row f at At + f * ST, coordinates as float4
+// vectors, b_f at coordinate MAXD) and bp is unused. x is replicated in
 // the group's lanes. A chain whose line search fails keeps stepping without
 // moving (so the groups of a warp stay convergent for the shuffles) and
 // returns false.
-template <int MAXD, int G, int ST, int U = 1>
+template <int MAXD, int G, int ST, int U = 1, bool ROWS = false>
 __device__ __forceinline__ bool run_chain_group(const float* __restrict__ At, int ldt, const float* __restrict__ bp,
                                                 int F, int dim, int mixing, uint32_t k0, uint32_t k1,
                                                 uint32_t chain, uint32_t stream, float* x, int gl) {
+  static_assert(!ROWS || (ST > 0 && ST % 4 == 0 && MAXD % 4 == 0 && ST > MAXD), "face rows: float4 rows with b");
   constexpr int R = (MAXD / 2 + 1 + G - 1) / G;  // job rounds per lane
   const int stride = ST > 0 ? ST : ldt;
   const int npairs = (dim + 1) >> 1;
@@ -114,19 +117,44 @@ __device__ __forceinline__ bool run_chain_group(const float* __restrict__ At, in
       for (int u = 0; u < U; ++u) {
         const int f = f0 + u * G;
         if (U == 1 || f < F) {
-          const float* col = At + f;
-          float a0 = col[0];
-          float ax = __fmul_rn(a0, x[0]);
-          float ad = __fmul_rn(a0, dir[0]);
+          float ax, ad, lb;
+          if constexpr (ROWS) {
+            // one 16-byte shared load per four coordinates
+            const float4* row = reinterpret_cast<const float4*>(At + f * ST);
+            float a[MAXD];
 #pragma unroll
-          for (int k = 1; k < MAXD; ++k) {
-            if (k < dim) {
-              float ak = col[k * stride];
-              ax = __fmaf_rn(ak, x[k], ax);
-              ad = __fmaf_rn(ak, dir[k], ad);
+            for (int q = 0; q < MAXD / 4; ++q) {
+              const float4 v = row[q];
+              a[4 * q] = v.x;
+              a[4 * q + 1] = v.y;
+              a[4 * q + 2] = v.z;
+              a[4 * q + 3] = v.w;
             }
+            ax = __fmul_rn(a[0], x[0]);
+            ad = __fmul_rn(a[0], dir[0]);
+#pragma unroll
+            for (int k = 1; k < MAXD; ++k) {
+              if (k < dim) {
+                ax = __fmaf_rn(a[k], x[k], ax);
+                ad = __fmaf_rn(a[k], dir[k], ad);
+              }
+            }
+            lb = __fsub_rn(At[f * ST + MAXD], ax);
+          } else {
+            const float* col = At + f;
+            float a0 = col[0];
+            ax = __fmul_rn(a0, x[0]);
+            ad = __fmul_rn(a0, dir[0]);
+#pragma unroll
+            for (int k = 1; k < MAXD; ++k) {
+              if (k < dim) {
+                float ak = col[k * stride];
+                ax = __fmaf_rn(ak, x[k], ax);
+                ad = __fmaf_rn(ak, dir[k], ad);
+              }
+            }
+            lb = __fsub_rn(bp[f], ax);
           }
-          float lb = __fsub_rn(bp[f], ax);
           if (ad < 0.0f)
             tmin = fmaxf(tmin, __fdiv_rn(lb, ad));
           else if (ad > 0.0f)
@@ -321,11 +349,21 @@ static_assert(9 * kStageFaces8 >= 17 * kStageFaces16, "staging buffer");
 // Staging capacity of a kernel with MINB resident blocks per SM: the largest
 // buffer that MINB blocks fit in the SM's 227 KB (2 blocks: 3072 / 1536
 // faces, 3 blocks: 2048 / 1024, 4 blocks: 1536 / 768).
+// Face-row staging (stage_rows): row f holds a_f0 .. a_f(MAXD-1) (zero past
+// dim) and b_f at MAXD, kRowStride floats apart. The strides are multiples of
+// 16 bytes for the float4 loads, and 12 and 20 floats put the eight rows a
+// group reads at once in eight disjoint sets of four banks.
+template <int MAXD>
+constexpr int kRowStride = MAXD <= 8 ? 12 : 20;
+
 template <int MINB>
 struct StageCfg {
   static constexpr int f8 = MINB <= 2 ? 3072 : MINB == 3 ? 2048 : 1536;
   static constexpr int f16 = f8 / 2;
   static constexpr size_t bytes = 9 * (size_t)f8 * sizeof(float);
+  // faces the same buffer holds as face rows
+  static constexpr int r8 = (int)(bytes / (kRowStride<8> * sizeof(float)));
+  static constexpr int r16 = (int)(bytes / (kRowStride<16> * sizeof(float)));
   static_assert(9 * f8 >= 17 * f16, "staging buffer");
   static_assert(MINB * bytes <= 227 * 1024, "MINB staging buffers fit one SM");
 };
@@ -340,10 +378,27 @@ __device__ __forceinline__ void stage_polytope(const float* __restrict__ At, int
   for (int f = threadIdx.x; f < F; f += blockDim.x) sm[MAXD * ST + f] = b[f];
 }
 
+// Stages F faces of a transposed polytope (At[k * ldt + f], b[f]) as face
+// rows: F * kRowStride<MAXD> floats of sm (16-byte aligned).
+template <int MAXD>
+__device__ __forceinline__ void stage_rows(const float* __restrict__ At, int ldt, const float* __restrict__ b, int F,
+                                           int dim, float* sm) {
+  constexpr int RS = kRowStride<MAXD>;
+  for (int i = threadIdx.x; i < MAXD * F; i += blockDim.x) {
+    const int k = i / F, f = i - k * F;
+    sm[f * RS + k] = k < dim ? At[(int64_t)k * ldt + f] : 0.f;
+  }
+  for (int f = threadIdx.x; f < F; f += blockDim.x) sm[f * RS + MAXD] = b[f];
+}
+
+// Staged layouts of the group sampler: transposed columns, transposed columns
+// read in packed face pairs, face rows.
+enum : int { kLayStrided = 0, kLayPacked = 1, kLayRows = 2 };
+
 // Chains [first, last) of one polytope by the whole block, G lanes per
 // chain; the trip count is uniform across the block (groups past `last`
 // repeat the last chain and store nothing). A failed chain stores `start`.
-template <int MAXD, int G, int ST, int U, bool PK = false>
+template <int MAXD, int G, int ST, int U, int LAY = kLayStrided>
 __device__ __forceinline__ void sample_chains(const float* __restrict__ At, int ldt, const float* __restrict__ b,
                                               int F, int dim, const float* __restrict__ start, int first, int last,
                                               int mixing, uint32_t k0, uint32_t k1, uint32_t stream,
@@ -358,10 +413,11 @@ __device__ __forceinline__ void sample_chains(const float* __restrict__ At, int 
 #pragma unroll
     for (int k = 0; k < MAXD; ++k) x[k] = k < dim ? start[k] : 0.f;
     bool ok;
-    if constexpr (PK && ST > 0)
+    if constexpr (LAY == kLayPacked && ST > 0)
       ok = run_chain_group_x2<MAXD, G, ST, U>(At, b, F, dim, mixing, k0, k1, (uint32_t)cc, stream, x, gl);
     else
-      ok = run_chain_group<MAXD, G, ST, U>(At, ldt, b, F, dim, mixing, k0, k1, (uint32_t)cc, stream, x, gl);
+      ok = run_chain_group<MAXD, G, ST, U, LAY == kLayRows>(At, ldt, b, F, dim, mixing, k0, k1, (uint32_t)cc, stream,
+                                                           x, gl);
     if (chain < last) group_store<MAXD, G>(x, dim, gl, out + (int64_t)chain * dim, ok, start);
   }
 }
@@ -374,23 +430,24 @@ __host__ __device__ __forceinline__ int group_width(int64_t total, int64_t grid_
 }
 
 // One polytope's chains [first, last) with the polytope staged in `sm` when
-// it fits (sm_ready: already staged), else read from global memory. PK: the
-// staged path takes faces in packed pairs (U pairs per trip).
-template <int MAXD, int U, bool PK = false, int ST8 = kStageFaces8, int ST16 = kStageFaces16>
+// it fits (sm_ready: already staged; by stage_rows for LAY == kLayRows, else
+// by stage_polytope with strides ST8 / ST16), else read from global memory.
+// kLayPacked: the staged path takes faces in packed pairs (U pairs per trip).
+template <int MAXD, int U, int LAY = kLayStrided, int ST8 = kStageFaces8, int ST16 = kStageFaces16>
 __device__ __forceinline__ void sample_range(const float* __restrict__ At, int ldt, const float* __restrict__ b,
                                              int F, int dim, const float* __restrict__ start, int first, int last,
                                              int mixing, uint32_t k0, uint32_t k1, uint32_t stream,
                                              float* __restrict__ out, int G, float* sm, bool staged) {
-  constexpr int ST = MAXD <= 8 ? ST8 : ST16;
+  constexpr int ST = LAY == kLayRows ? kRowStride<MAXD> : MAXD <= 8 ? ST8 : ST16;
   if (staged) {
     const float* sAt = sm;
-    const float* sb = sm + MAXD * ST;
+    const float* sb = LAY == kLayRows ? nullptr : sm + MAXD * ST;
     if (G == 8)
-      sample_chains<MAXD, 8, ST, U, PK>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
+      sample_chains<MAXD, 8, ST, U, LAY>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
     else if (G == 16)
-      sample_chains<MAXD, 16, ST, U, PK>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
+      sample_chains<MAXD, 16, ST, U, LAY>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
     else
-      sample_chains<MAXD, 32, ST, U, PK>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
+      sample_chains<MAXD, 32, ST, U, LAY>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
   } else {
     if (G == 8)
       sample_chains<MAXD, 8, 0, U>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out);
