@@ -61,7 +61,9 @@ struct BatchIter {    // device-side iteration state
   int num_act;        // length of the active-slot list of iteration k
   int max_nf8;        // most faces of an active slot with dim <= 8
   int max_nf16;       // most faces of an active slot with dim > 8
-  int sample_next;    // sampler work items claimed past the first one per block (zeroed before each launch)
+  int sample_next;    // work queues of the sampler, check and bisection launches: items claimed past the
+  int check_next;     // first one per block (each zeroed before every launch that uses it)
+  int bisect_next;
   int pad;
 };
 
@@ -117,12 +119,23 @@ static __device__ __forceinline__ int item_size(int64_t total, int cap, int nw) 
   return (int)(c / nw) * nw;
 }
 
+// Work queue of a launch: block b starts with item b; whenever a block has
+// finished an item it claims the next unclaimed one from `counter` (zeroed
+// before the launch), so blocks that drew costly items (large regions, big
+// plants) do not hold up a launch while others idle. Block-uniform result.
+static __device__ __forceinline__ int claim_item(int* counter) {
+  __shared__ int next;
+  if (threadIdx.x == 0) next = gridDim.x + atomicAdd(counter, 1);
+  __syncthreads();
+  const int it = next;
+  __syncthreads();  // every thread has read `next` before thread 0 writes it again
+  return it;
+}
+
 // ------------------------------------------------------------------ kernels
 // Chains of the active slots in work items (slot, chunk of chains), handed
-// out as a queue: block b starts with item b and claims the next unclaimed
-// item (it->sample_next, zeroed before the launch) whenever it finishes one,
-// so blocks that drew chains of large regions (a slot's cost grows with its
-// faces and dimension) do not hold up the launch while others idle. A block
+// out by the work queue it->sample_next (a slot's cost grows with its faces
+// and dimension, so fixed ranges of items would leave blocks idle). A block
 // stages each new slot's region (At, b) in shared memory and runs its chains
 // G lanes per chain (G from the total chain count: 8 when the batch is full,
 // up to 32 in the tail). Each chain's draws and output row follow from its
@@ -130,7 +143,6 @@ static __device__ __forceinline__ int item_size(int64_t total, int cap, int nw) 
 template <int U, int MINB, int LAY = kLayStrided>
 __global__ void __launch_bounds__(256, MINB) batch_sample_kernel(BatchArgs a) {
   extern __shared__ __align__(16) float smf[];  // the face loop reads float2/float4 vectors
-  __shared__ int next_item;
   const int N = a.n_tab[a.it->k];
   const int64_t total = (int64_t)a.it->num_act * N;
   const int G = group_width(total, (int64_t)gridDim.x * (blockDim.x >> 5));
@@ -173,10 +185,7 @@ __global__ void __launch_bounds__(256, MINB) batch_sample_kernel(BatchArgs a) {
     else
       sample_range<16, U, LAY, SC::f8, SC::f16>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u,
                                                 out, G, smf, fits);
-    if (threadIdx.x == 0) next_item = gridDim.x + atomicAdd(&a.it->sample_next, 1);
-    __syncthreads();
-    it = next_item;
-    __syncthreads();  // every thread has read next_item before thread 0 writes the next one
+    it = claim_item(&a.it->sample_next);
   }
 }
 
@@ -222,7 +231,7 @@ static __device__ __forceinline__ WarpCtx<SM> batch_ctx(const DevPlant& p, float
 
 // Work item = (active slot, chunk of configurations), sized so that the grid
 // gets about four items per block whether 256 slots or one are active; items
-// are dealt round robin to the blocks.
+// are handed out by the work queue it->check_next (plants differ in cost).
 template <bool SM>
 __global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_check_kernel(BatchArgs a, int static_floats) {
   extern __shared__ float4 smem4[];
@@ -236,10 +245,10 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_check_kernel(Bat
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int c = item_size((int64_t)na * N, a.cfg_max, nw);
   const int ips = (N + c - 1) / c;
-  const int64_t items = (int64_t)na * ips;
+  const int items = na * ips;
   const VoxArgs none{nullptr, 0, 0.f, nullptr, nullptr, 0};
-  for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
-    const int slot = a.act[it / ips], first = (int)(it % ips) * c;
+  for (int it = blockIdx.x; it < items; it = claim_item(&a.it->check_next)) {
+    const int slot = a.act[it / ips], first = (it % ips) * c;
     const SlotState& S = a.slots[slot];
     if (!block_plant<SM>(a, S.plant, &sp, &cur, smem4, &bar)) return;
     const WarpCtx<SM> w = batch_ctx<SM>(sp, smem4, static_floats);
@@ -293,10 +302,11 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_bisect_kernel(Ba
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int c = item_size((int64_t)na * a.num_particles, a.part_max, nw);
   const int ips = (a.num_particles + c - 1) / c;
-  const int64_t items = (int64_t)na * ips;
+  const int items = na * ips;
   const VoxArgs none{nullptr, 0, 0.f, nullptr, nullptr, 0};
-  for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
-    const int slot = a.act[it / ips], first = (int)(it % ips) * c;
+  // work queue it->bisect_next: `for` advances through claim_item on every path, `continue` included
+  for (int it = blockIdx.x; it < items; it = claim_item(&a.it->bisect_next)) {
+    const int slot = a.act[it / ips], first = (it % ips) * c;
     const SlotState& S = a.slots[slot];
     if (S.done || first >= S.K) continue;  // uniform across the block
     if (!block_plant<SM>(a, S.plant, &sp, &cur, smem4, &bar)) return;
@@ -457,7 +467,8 @@ __global__ void __launch_bounds__(1024) batch_sort_kernel(BatchArgs a) {
 }
 
 // Round r of the sorted check: the positions of round r of every slot that
-// still needs checking, in (slot, chunk) items as batch_check_kernel.
+// still needs checking, in (slot, chunk) items from the work queue as
+// batch_check_kernel.
 template <bool SM>
 __global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_check_sorted_kernel(BatchArgs a, int static_floats,
                                                                                    int r) {
@@ -474,10 +485,11 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_check_sorted_ker
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int c = item_size((int64_t)na * cnt, a.cfg_max, nw);
   const int ips = (cnt + c - 1) / c;
-  const int64_t items = (int64_t)na * ips;
+  const int items = na * ips;
   const VoxArgs none{nullptr, 0, 0.f, nullptr, nullptr, 0};
-  for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
-    const int slot = a.act[it / ips], first = beg + (int)(it % ips) * c;
+  // work queue it->check_next: `for` advances through claim_item on every path, `continue` included
+  for (int it = blockIdx.x; it < items; it = claim_item(&a.it->check_next)) {
+    const int slot = a.act[it / ips], first = beg + (it % ips) * c;
     const SlotState& S = a.slots[slot];
     if (S.done || !S.need) continue;  // uniform across the block
     if (!block_plant<SM>(a, S.plant, &sp, &cur, smem4, &bar)) return;
@@ -709,6 +721,7 @@ void launch_iteration(csd_batch_s* h, int num_slots, const BatchArgs& a, cudaStr
     batch_sort_kernel<<<num_slots, 1024, kSortMax * sizeof(unsigned long long), s>>>(a);
     if (ev) cudaEventRecord(ev[3], s);
     for (int r = 0; r < a.rounds; ++r) {
+      cudaMemsetAsync(&a.it->check_next, 0, sizeof(int), s);
       if (h->sm)
         batch_check_sorted_kernel<true><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->static_floats,
                                                                                                   r);
@@ -721,6 +734,7 @@ void launch_iteration(csd_batch_s* h, int num_slots, const BatchArgs& a, cudaStr
   } else {
     if (ev) cudaEventRecord(ev[2], s);
     if (ev) cudaEventRecord(ev[3], s);
+    cudaMemsetAsync(&a.it->check_next, 0, sizeof(int), s);
     if (h->sm)
       batch_check_kernel<true><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->static_floats);
     else
@@ -729,6 +743,7 @@ void launch_iteration(csd_batch_s* h, int num_slots, const BatchArgs& a, cudaStr
     batch_compact_kernel<<<num_slots, 1024, 0, s>>>(a);
   }
   if (ev) cudaEventRecord(ev[5], s);
+  cudaMemsetAsync(&a.it->bisect_next, 0, sizeof(int), s);
   if (h->sm)
     batch_bisect_kernel<true><<<h->bisect_grid, 32 * kWarpsPerBlock, h->check_smem, s>>>(a, h->static_floats);
   else
@@ -817,8 +832,8 @@ csd_status_t csd_batch_create(const csd_plant_t* plants, int32_t num_plants, int
     h->thr_tab.push_back((1 - o->tau) * o->epsilon * M);
   }
   h->n_max = *std::max_element(h->n_tab.begin(), h->n_tab.end());
-  // the sampler numbers its work items (slot, 32 or more chains) with 32-bit integers
-  CSD_CHECK((int64_t)max_slots * ((h->n_max + 31) / 32) + 4096 < (int64_t)INT32_MAX, CSD_ERR_CAPACITY,
+  // the stage kernels number their work items (slot, 8 or more configurations) with 32-bit integers
+  CSD_CHECK((int64_t)max_slots * (h->n_max / 8 + 1) + (1 << 20) < (int64_t)INT32_MAX, CSD_ERR_CAPACITY,
             "too many slots times samples per iteration");
   h->sm = max_static <= kStaticSmemLimit;
   h->static_floats = h->sm ? max_static / 4 : 0;
@@ -1039,6 +1054,7 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
       for (int c = 0; c < kNumCheckVariants && !a.mlp_wb; ++c, ++j) {
         BatchArgs ac = a;
         ac.cfg_max = kCheckItemCaps[c];
+        cudaMemsetAsync(&a.it->check_next, 0, sizeof(int), st);
         cudaEventRecord(tev[2 * j], st);
         if (h->sm)
           batch_check_kernel<true><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, st>>>(ac, h->static_floats);
