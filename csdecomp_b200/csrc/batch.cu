@@ -663,7 +663,7 @@ struct csd_batch_s {
   int check_grid = 0, bisect_grid = 0;
   int cfg_max = 128, part_max = 64;
   int sample_variant = 0;     // tuned (or set) variant
-  int large_variant = 1;      // variant once a slot's faces exceed the tuned variant's staging
+  int large_variant = 1;      // variant chosen once a slot's faces exceeded the tuned variant's staging
   int run_variant = 0;        // variant of the current iterations
   bool switch_large = true;   // false after csd_batch_set_shapes: run exactly the set variant
   int sample_grid[csd::kNumSampleVariants] = {};
@@ -703,6 +703,26 @@ struct csd_batch_s {
 using namespace csd;
 
 namespace {
+
+// Sampler variant for regions of up to nf8 (dim <= 8) and nf16 faces: the
+// fastest by tuning time among those whose staging buffer holds them, else
+// the one with the most room (faces beyond it are read from global memory).
+int variant_for(const csd_batch_s* h, int nf8, int nf16) {
+  int best = -1;
+  for (int v = 0; v < kNumSampleVariants; ++v) {
+    const SampleVariant& cv = kSampleVariants[v];
+    if (cv.f8 >= nf8 && cv.f16 >= nf16 && (best < 0 || h->tune_ms[v] < h->tune_ms[best])) best = v;
+  }
+  if (best >= 0) return best;
+  best = 0;
+  for (int v = 1; v < kNumSampleVariants; ++v) {
+    const SampleVariant &cv = kSampleVariants[v], &bv = kSampleVariants[best];
+    const bool roomier = cv.f16 > bv.f16 || (cv.f16 == bv.f16 && cv.f8 > bv.f8);
+    const bool same = cv.f16 == bv.f16 && cv.f8 == bv.f8;
+    if (roomier || (same && h->tune_ms[v] < h->tune_ms[best])) best = v;
+  }
+  return best;
+}
 
 // One iteration's launches on stream s. ev (kStages + 1 events) brackets the
 // stages for the profiling mode; skip_sample leaves out the sampler (the
@@ -1080,14 +1100,8 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
           if (h->tune_ms[kNumSampleVariants + c] < h->tune_ms[kNumSampleVariants + bc]) bc = c;
         h->sample_variant = bs;
         h->run_variant = bs;
-        // for slots whose faces outgrow bs's staging: the fastest variant with more staging room
-        int bl = -1;
-        for (int v = 0; v < kNumSampleVariants; ++v) {
-          const SampleVariant &cv = kSampleVariants[v], &tv = kSampleVariants[bs];
-          const bool roomier = cv.f8 >= tv.f8 && cv.f16 >= tv.f16 && (cv.f8 > tv.f8 || cv.f16 > tv.f16);
-          if (roomier && (bl < 0 || h->tune_ms[v] < h->tune_ms[bl])) bl = v;
-        }
-        h->large_variant = bl >= 0 ? bl : bs;
+        // reported until a region outgrows bs's staging: the variant that would take over then
+        h->large_variant = variant_for(h, kSampleVariants[bs].f8 + 1, kSampleVariants[bs].f16 + 1);
         if (!a.mlp_wb) h->cfg_max = kCheckItemCaps[bc];
         a.cfg_max = h->cfg_max;
         h->graph_slots = -1;  // recapture with the chosen shapes
@@ -1118,12 +1132,16 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
     active_now = h->host_iter->last_active;
     if (active_now == 0) break;
     // a slot's region outgrew the staging buffer of the running variant: continue with the
-    // large-staging variant (identical samples; the graph is captured again once)
-    if (h->switch_large && h->tune_iters == 0 && h->run_variant != h->large_variant) {
+    // fastest variant that stages it (identical samples; the graph is captured again)
+    if (h->switch_large && h->tune_iters == 0) {
       const SampleVariant& rv = kSampleVariants[h->run_variant];
       if (h->host_iter->max_nf8 > rv.f8 || h->host_iter->max_nf16 > rv.f16) {
-        h->run_variant = h->large_variant;
-        if ((s = build_graph(h, n, a))) return s;
+        const int v = variant_for(h, h->host_iter->max_nf8, h->host_iter->max_nf16);
+        if (v != h->run_variant) {
+          h->run_variant = v;
+          h->large_variant = v;
+          if ((s = build_graph(h, n, a))) return s;
+        }
       }
     }
   }
