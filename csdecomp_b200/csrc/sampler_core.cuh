@@ -429,9 +429,9 @@ __host__ __device__ __forceinline__ int group_width(int64_t total, int64_t grid_
   return total >= 8 * grid_warps ? 8 : total >= 4 * grid_warps ? 16 : 32;
 }
 
-// One polytope's chains [first, last) with the polytope staged in `sm` when
-// it fits (sm_ready: already staged; by stage_rows for LAY == kLayRows, else
-// by stage_polytope with strides ST8 / ST16), else read from global memory.
+// One polytope's chains [first, last) read from `sm` when `staged` (the caller
+// staged it: by stage_rows for LAY == kLayRows, else by stage_polytope with
+// strides ST8 / ST16), else from global memory.
 // kLayPacked: the staged path takes faces in packed pairs (U pairs per trip).
 template <int MAXD, int U, int LAY = kLayStrided, int ST8 = kStageFaces8, int ST16 = kStageFaces16>
 __device__ __forceinline__ void sample_range(const float* __restrict__ At, int ldt, const float* __restrict__ b,

@@ -304,12 +304,14 @@ csd_status_t csd_batch_stage_ms(csd_batch_t h, float* stage_ms /* [8] */);
  * csd_batch_inflate, every sampler variant (faces per lane and trip x
  * resident blocks per SM: [1x2, 2x2, 1x3, 2x3, 4x2, 4x3], then packed face
  * pairs (two faces per 64-bit load and per f32x2 FMA) per lane and trip x
- * blocks per SM: [1x2, 2x2, 1x3, 2x3], then unpacked [1x4, 2x4]) and every
- * check work-item cap ([32, 128, 512] configurations) is timed on that
- * iteration's own inputs; the fastest of each is kept for the graph and later
- * calls. All variants give identical samples. csd_batch_tuning reports the
- * choice and the summed time of each variant (variant_ms: 12 sampler entries,
- * then 3 check entries). */
+ * blocks per SM: [1x2, 2x2, 1x3, 2x3], then unpacked [1x4, 2x4], then face
+ * rows (a face's coordinates and b in one row, read as 16-byte vectors)
+ * [1x3, 2x3, 1x4, 1x2]) and every check work-item cap ([32, 128, 512]
+ * configurations) is timed on that iteration's own inputs; the fastest of
+ * each is kept for the graph and later calls. All variants give identical
+ * samples. csd_batch_tuning reports the choice and the summed time of each
+ * variant (variant_ms: 16 sampler entries, then 3 check entries;
+ * *num_variants = 19). */
 csd_status_t csd_batch_autotune(csd_batch_t h, int32_t iterations);
 /* Surrogate-guided checking (mlp: one net per plant of the batch, same
  * dimensions; NULL turns it off). Each iteration then scores every sample
@@ -331,12 +333,15 @@ csd_status_t csd_batch_set_surrogate_rounds(csd_batch_t h, int32_t rounds, int32
  * set variant then runs for every iteration. */
 csd_status_t csd_batch_set_shapes(csd_batch_t h, int32_t sample_variant, int32_t check_item_cap);
 /* Each sampler variant stages a slot's region in shared memory up to a face
- * count set by its blocks per SM (2: 3072 faces for dim <= 8, 1536 above;
- * 3: 2048 / 1024; 4: 1536 / 768); larger regions are read from L2. After
- * tuning, once an active slot outgrows the tuned variant's staging, the
- * iterations continue with the fastest variant that stages more (the graph is
- * captured once more). tuned / large / last_run: the tuned variant, the one
- * used for large regions, the one the last iteration ran. */
+ * count set by its blocks per SM and layout (2: 3072 faces for dim <= 8, 1536
+ * above, as face rows 2304 / 1382; 3: 2048 / 1024, rows 1536 / 921; 4:
+ * 1536 / 768, rows 1152 / 691); larger regions are read from L2. After
+ * tuning, once an active slot outgrows the running variant's staging, the
+ * iterations continue with the fastest variant (by tuning time) that stages
+ * the largest active region, else the roomiest (the graph is captured once
+ * more per switch). tuned / large / last_run: the tuned variant, the one the
+ * last switch chose for large regions (before any switch: the one it would
+ * choose), the one the last iteration ran. */
 csd_status_t csd_batch_sample_variants(csd_batch_t h, int32_t* tuned, int32_t* large, int32_t* last_run);
 csd_status_t csd_batch_tuning(csd_batch_t h, int32_t* sample_variant, int32_t* check_item_cap, float* variant_ms,
                               int32_t* num_variants);
