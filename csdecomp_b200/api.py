@@ -644,6 +644,9 @@ class BatchedEdgeInflator:
         C.check(C.lib().csd_batch_tuning(self._handle, ctypes.byref(sv), ctypes.byref(cap), C.ptr(ms),
                                          ctypes.byref(nv)))
         ns = len(self.SAMPLE_VARIANTS)
+        if nv.value != ns + len(self.CHECK_ITEM_CAPS):
+            raise RuntimeError(f"the library reports {nv.value} tuned shapes, the names list "
+                               f"{ns} sampler variants + {len(self.CHECK_ITEM_CAPS)} check caps")
         t, lg, lr = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
         C.check(C.lib().csd_batch_sample_variants(self._handle, ctypes.byref(t), ctypes.byref(lg), ctypes.byref(lr)))
         return {"sample_variant": self.SAMPLE_VARIANTS[sv.value], "check_item_cap": cap.value,
