@@ -90,7 +90,7 @@ EXPORTS = (
     "csd_check_points", "csd_check_edges", "csd_check_edges_ranked", "csd_visibility_graph", "csd_pair_collision_free", "csd_uniform_sample_hpolyhedra",
     "csd_inflator_create", "csd_inflator_inflate", "csd_inflator_destroy", "csd_eizo", "csd_eizo_noalloc", "csd_edit_regions", "csd_batch_create", "csd_batch_inflate", "csd_batch_configs_checked",
     "csd_batch_set_profiling", "csd_batch_stage_ms", "csd_batch_iteration_profile", "csd_batch_sample_flops",
-    "csd_batch_autotune", "csd_batch_tuning", "csd_batch_set_shapes", "csd_batch_sample_variants", "csd_batch_set_surrogate",
+    "csd_batch_autotune", "csd_batch_tuning", "csd_batch_set_shapes", "csd_batch_sample_variants", "csd_batch_shape_counts", "csd_batch_set_surrogate",
     "csd_batch_set_surrogate_rounds",    "csd_batch_destroy",
     "csd_num_samples_unadaptive", "csd_fp32_fma_probe", "csd_plant_flops", "csd_plant_set_culling",
     "csd_plant_set_voxel_grid",
@@ -121,9 +121,10 @@ def lib() -> ctypes.CDLL:
         L.csd_last_error.restype = ctypes.c_char_p
         L.csd_num_samples_unadaptive.restype = ctypes.c_uint32
         L.csd_num_samples_unadaptive.argtypes = [ctypes.c_float] * 3
+        L.csd_batch_shape_counts.restype = None
         for name in EXPORTS:
             f = getattr(L, name)
-            if name not in ("csd_last_error", "csd_num_samples_unadaptive"):
+            if name not in ("csd_last_error", "csd_num_samples_unadaptive", "csd_batch_shape_counts"):
                 f.restype = ctypes.c_int32
         _lib = L
     return _lib

@@ -1270,6 +1270,11 @@ csd_status_t csd_batch_sample_variants(csd_batch_t h, int32_t* tuned, int32_t* l
   return CSD_OK;
 }
 
+void csd_batch_shape_counts(int32_t* num_sample_variants, int32_t* num_check_caps) {
+  if (num_sample_variants) *num_sample_variants = kNumSampleVariants;
+  if (num_check_caps) *num_check_caps = kNumCheckVariants;
+}
+
 csd_status_t csd_batch_tuning(csd_batch_t h, int32_t* sample_variant, int32_t* check_item_cap, float* variant_ms,
                               int32_t* num_variants) {
   CSD_CHECK(h, CSD_ERR_INVALID, "null batch");

@@ -343,6 +343,10 @@ csd_status_t csd_batch_set_shapes(csd_batch_t h, int32_t sample_variant, int32_t
  * last switch chose for large regions (before any switch: the one it would
  * choose), the one the last iteration ran. */
 csd_status_t csd_batch_sample_variants(csd_batch_t h, int32_t* tuned, int32_t* large, int32_t* last_run);
+/* Number of sampler variants and of check work-item caps the autotuner
+ * chooses from (the index ranges of csd_batch_set_shapes and the entries of
+ * csd_batch_tuning's variant_ms). Needs no device. No reference counterpart. */
+void csd_batch_shape_counts(int32_t* num_sample_variants, int32_t* num_check_caps);
 csd_status_t csd_batch_tuning(csd_batch_t h, int32_t* sample_variant, int32_t* check_item_cap, float* variant_ms,
                               int32_t* num_variants);
 /* Profiling mode, last csd_batch_inflate: per iteration the eight stage times

@@ -28,3 +28,11 @@ def test_library_exports_all_symbols():
 def test_version_and_pure_host_helpers():
     assert _capi.lib().csd_version() >= 10000
     assert _capi.lib().csd_num_samples_unadaptive(0.01, 0.05, 0.5) == 2397
+
+
+def test_batch_shape_counts_match_the_python_names():
+    from csdecomp_b200.api import BatchedEdgeInflator
+    ns, nc = ctypes.c_int32(-1), ctypes.c_int32(-1)
+    _capi.lib().csd_batch_shape_counts(ctypes.byref(ns), ctypes.byref(nc))
+    assert ns.value == len(BatchedEdgeInflator.SAMPLE_VARIANTS)
+    assert nc.value == len(BatchedEdgeInflator.CHECK_ITEM_CAPS)
