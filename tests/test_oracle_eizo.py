@@ -51,3 +51,26 @@ def test_eizo_faces_separate_their_collisions(plants):
     A, b, _ = O.eizo(gp.plant, [0, 0], [1, 0], A0, b0, opt, gp.robot_geometry_ids)
     assert A.shape[0] > A0.shape[0]
     np.testing.assert_allclose(np.linalg.norm(A[A0.shape[0]:], axis=1), 1.0, atol=1e-5)
+
+
+def test_eizo_does_not_depend_on_the_thread_count(plants):
+    """The oracle is the parity checker: its regions must not depend on how
+    many host threads run its point checks."""
+    gp = plants["boxes_in_corners"]
+    A0, b0 = box_domain(gp.lower, gp.upper)
+    opt = EizoOptions(num_particles=500)
+    A1, b1, it1 = O.eizo(gp.plant, [0, 0], [1, 0], A0, b0, opt, gp.robot_geometry_ids, nthreads=1)
+    A4, b4, it4 = O.eizo(gp.plant, [0, 0], [1, 0], A0, b0, opt, gp.robot_geometry_ids, nthreads=4)
+    np.testing.assert_array_equal(A1, A4)
+    np.testing.assert_array_equal(b1, b4)
+    assert it1 == it4
+
+
+def test_eizo_face_capacity_exceeded_raises(plants):
+    gp = plants["boxes_in_corners"]
+    A0, b0 = box_domain(gp.lower, gp.upper)
+    opt = EizoOptions(num_particles=500)
+    A, _, _ = O.eizo(gp.plant, [0, 0], [1, 0], A0, b0, opt, gp.robot_geometry_ids)
+    assert A.shape[0] - A0.shape[0] >= 2
+    with pytest.raises(RuntimeError, match="Max face count exceeded"):
+        O.eizo(gp.plant, [0, 0], [1, 0], A0, b0, opt, gp.robot_geometry_ids, capacity=A0.shape[0] + 1)
