@@ -104,3 +104,20 @@ def test_edit_regions_bad_segment_index(plants, golden):
     dom = box_domain(gp.lower, gp.upper)
     with pytest.raises(RuntimeError):
         O.edit_regions(gp.plant, [[0.6, 0.5]], [3], g["starts"], g["ends"], [dom] * 3, gp.robot_geometry_ids)
+
+
+def test_edit_regions_does_not_depend_on_the_thread_count(plants, golden):
+    g = golden["edit_regions_2d"]
+    gp = plants[g["plant"]]
+    dom = box_domain(gp.lower, gp.upper)
+    col = np.tile(np.array(g["collisions"], np.float32), (g["repeats"], 1))
+    seg = np.repeat(np.arange(g["repeats"], dtype=np.uint32), len(g["collisions"]))
+    outs = [O.edit_regions(gp.plant, col, seg, g["starts"], g["ends"], [dom] * len(g["starts"]),
+                           gp.robot_geometry_ids, g["voxels"], g["voxel_radius"], g["configuration_margin"],
+                           g["bisection_steps"], nthreads=t) for t in (1, 4)]
+    (r1, p1, o1), (r4, p4, o4) = outs
+    np.testing.assert_array_equal(p1, p4)
+    np.testing.assert_array_equal(o1, o4)
+    for (A1, b1), (A4, b4) in zip(r1, r4):
+        np.testing.assert_array_equal(A1, A4)
+        np.testing.assert_array_equal(b1, b4)
