@@ -359,3 +359,48 @@ def test_staging_wait_gives_up_and_is_reported(plants):
     rng = np.random.default_rng(4)
     q = (gp.lower + (gp.upper - gp.lower) * rng.random((500, gp.dim))).astype(np.float32)
     band_parity(gp.plant, q)
+
+
+def edge_band_parity(sc, s, e, mode):
+    """GPU edge verdicts against the oracle's (reference rule, early exit): a
+    differing edge must hold a point within the contact band; the number of
+    points checked equals the oracle's wherever the verdicts agree and the
+    edge is free (a colliding edge may stop at another colliding point, since
+    the GPU visits points coarse to fine)."""
+    gpu, pts = csd.CheckEdgesCollisionFreeCuda(s.T, e.T, sc.plant, 0.01, mode, return_points_checked=True)
+    ref, ref_pts = O.check_edges(sc.plant, s, e, 0.01, mode)
+    diff = np.nonzero(gpu != ref)[0]
+    for i in diff:
+        _, sd = O.signed_distance(sc.plant, O.edge_points(s[i], e[i], 0.01, mode))
+        assert np.abs(sd).min() <= BAND, i
+    free = (gpu == 1) & (ref == 1)
+    np.testing.assert_array_equal(pts[free], ref_pts[free])
+    return gpu, diff
+
+
+def test_config2_edges_vs_oracle_full_size():
+    """Config 2 as written: 10^5 segments with endpoints uniform in the joint
+    limits of the 7-DOF arm (80 spheres + 4 capsules) among 200 world
+    primitives, 0.01 rad step, reference (L2) discretisation. Without a
+    keep-out nearly every configuration collides, so nearly every segment
+    collides at its first point."""
+    sc = scenes.edge_check_scene()
+    n = 100_000
+    s, e = sc.random_configs(n, 201), sc.random_configs(n, 202)
+    gpu, diff = edge_band_parity(sc, s, e, csd.CSD_EDGE_L2_REF)
+    assert len(diff) <= 3
+    assert gpu.sum() <= 10
+
+
+def test_config2_keepout_edges_vs_oracle():
+    """The 0.8 m keep-out variant of config 2 (24% of configurations free),
+    10^4 segments with uniform endpoints plus 2,000 short ones, so that free
+    edges checked to the end (up to ~660 points each) are part of the case."""
+    sc = scenes.edge_check_scene(keepout=0.8)
+    rng = np.random.default_rng(203)
+    s = sc.random_configs(12_000, 204)
+    e = sc.random_configs(12_000, 205)
+    e[10_000:] = (s[10_000:] + rng.normal(0, 0.1, (2_000, 7))).astype(np.float32)
+    gpu, diff = edge_band_parity(sc, s, e, csd.CSD_EDGE_L2_REF)
+    assert len(diff) <= 5
+    assert gpu[10_000:].sum() > 50 and gpu.mean() < 0.5
