@@ -197,6 +197,17 @@ def batch_scene(i: int, seed: int, keepout: float = 0.8) -> Scene:
                      keepout=keepout, arm_spacing=1.4, description=f"14-DOF two-arm, {n} world primitives")
 
 
+def batch_scene_cost(i: int, seed: int) -> float:
+    """Predicted relative cost of inflating in scene i of the batched workload,
+    read from the seed alone (before the scene is built): dimension squared x
+    world primitives. The sampler's face loop is dimension-long and the
+    regions of the two-arm plant grow several times more faces over more
+    iterations; every check visits the world pairs."""
+    n = int(np.random.default_rng(seed).integers(50, 401))  # the first draw of batch_scene
+    d = 7 if i % 2 == 0 else 14
+    return float(d * d * n)
+
+
 def batch_scene_seeds(count: int, seed: int = BATCH_SEED) -> List[int]:
     rng = np.random.default_rng(seed)
     return [int(rng.integers(1 << 30)) for _ in range(count)]
