@@ -591,13 +591,12 @@ class BatchedEdgeInflator:
     slot has its own plant, segment and domain and yields exactly the region
     CudaEdgeInflator.inflateEdge would for the same inputs (no voxels)."""
 
-    SAMPLE_VARIANTS = ("1 face/trip, 2 blocks/SM", "2 faces/trip, 2 blocks/SM", "1 face/trip, 3 blocks/SM",
-                       "2 faces/trip, 3 blocks/SM", "4 faces/trip, 2 blocks/SM", "4 faces/trip, 3 blocks/SM",
-                       "1 packed face pair/trip, 2 blocks/SM", "2 packed face pairs/trip, 2 blocks/SM",
-                       "1 packed face pair/trip, 3 blocks/SM", "2 packed face pairs/trip, 3 blocks/SM",
-                       "1 face/trip, 4 blocks/SM", "2 faces/trip, 4 blocks/SM",
-                       "1 face row/trip, 3 blocks/SM", "2 face rows/trip, 3 blocks/SM",
-                       "1 face row/trip, 4 blocks/SM", "1 face row/trip, 2 blocks/SM")
+    SAMPLE_VARIANTS = ("8 face pairs/lane, 1 block/SM", "8 face pairs/lane, 2 blocks/SM",
+                       "8 face pairs/lane, 3 blocks/SM", "16 face pairs/lane, 1 block/SM",
+                       "16 face pairs/lane, 2 blocks/SM")
+    SAMPLE_FLOP_RULE = ("(2 d + 4) F per chain and mixing step: a . dir (2 d), the carried-slack update (2) and the "
+                        "two theta-bound compares (2) per face, FMA = 2, division not counted; summed over the slots "
+                        "and iterations of the step")
     CHECK_ITEM_CAPS = (32, 128, 512)
 
     def __init__(self, plants: Sequence[MinimalPlant], options: EizoOptions, max_slots: int,
@@ -684,6 +683,9 @@ class BatchedEdgeInflator:
         cfg = np.zeros(n, np.int64)
         C.check(C.lib().csd_batch_configs_checked(self._handle, n, C.ptr(cfg)))
         self.last_configs_checked = cfg
+        nl = ctypes.c_int64(0)
+        C.check(C.lib().csd_batch_last_launches(self._handle, ctypes.byref(nl)))
+        self.last_kernel_launches = int(nl.value)
         out, aoff = [], 0
         for i, d in enumerate(dims):
             Ai = A_out[aoff:aoff + nf[i] * d].reshape(nf[i], d).copy()
@@ -710,7 +712,7 @@ class BatchedEdgeInflator:
         return ms, act
 
     def sample_flops(self) -> float:
-        """Sampler FLOPs of the last inflate in profiling mode (4 d F per chain step)."""
+        """Sampler FLOPs of the last inflate in profiling mode (SAMPLE_FLOP_RULE)."""
         v = ctypes.c_double(0)
         C.check(C.lib().csd_batch_sample_flops(self._handle, ctypes.byref(v)))
         return v.value

@@ -34,7 +34,7 @@ struct SlotState {
   int K;              // collisions kept for this iteration's bisection
   int status;         // 2: face capacity exceeded
   long long a_off;    // floats: region A [capacity][dim]
-  long long at_off;   // floats: region A transposed [dim][capacity]
+  long long pr_off;   // floats: region as face-pair rows [capacity / 2 + 1][pair_stride(dim)]
   long long b_off;    // floats: region b [capacity]
   long long seg_off;  // floats: line start [dim], line end [dim]
   long long smp_off;  // floats: samples [n_max][dim]
@@ -49,7 +49,7 @@ struct SlotState {
   int coll;           // colliding samples found
   int m_chk;          // checked samples among the first M
   int m_coll;         // colliding samples among the first M
-  int pad;
+  int ord;            // 1: checks this iteration's samples in surrogate order; 0: in sample order, all of them
 };
 
 static_assert(sizeof(SlotState) == 144, "slot record size is part of the transfer accounting");
@@ -64,7 +64,7 @@ struct BatchIter {    // device-side iteration state
   int sample_next;    // work queues of the sampler, check and bisection launches: items claimed past the
   int check_next;     // first one per block (each zeroed before every launch that uses it)
   int bisect_next;
-  int pad;
+  int num_ord;        // active slots still checking in surrogate order (surrogate mode)
 };
 
 struct BatchArgs {
@@ -132,71 +132,70 @@ static __device__ __forceinline__ int claim_item(int* counter) {
   return it;
 }
 
+// Staging buffer of a sampler variant with MINB resident blocks per SM: the
+// largest that MINB blocks (with their static shared memory) fit in the SM.
+template <int MINB>
+struct SampleStage {
+  static constexpr size_t bytes = (MINB == 1 ? 200 : MINB == 2 ? 104 : 68) * size_t(1024);
+  static_assert(MINB * (bytes + 2048) <= 227 * 1024, "MINB staging buffers fit one SM");
+};
+
 // ------------------------------------------------------------------ kernels
 // Chains of the active slots in work items (slot, chunk of chains), handed
 // out by the work queue it->sample_next (a slot's cost grows with its faces
 // and dimension, so fixed ranges of items would leave blocks idle). A block
-// stages each new slot's region (At, b) in shared memory and runs its chains
-// G lanes per chain (G from the total chain count: 8 when the batch is full,
-// up to 32 in the tail). Each chain's draws and output row follow from its
-// index alone, so the order in which blocks take items changes no sample.
-template <int U, int MINB, int LAY = kLayStrided>
+// stages each new slot's face-pair rows in shared memory when they fit its
+// buffer (else the chains read them from global memory, through L1) and runs
+// the chains with G lanes each: G from the total chain count (8 when the
+// batch is full, up to 32 in the tail), widened so that no lane holds more
+// than KP face pairs. Each chain's draws and output row follow from its index
+// alone and its arithmetic does not depend on G, so neither the order in
+// which blocks take items nor the variant changes a sample.
+template <int KP, int MINB>
 __global__ void __launch_bounds__(256, MINB) batch_sample_kernel(BatchArgs a) {
-  extern __shared__ __align__(16) float smf[];  // the face loop reads float2/float4 vectors
+  extern __shared__ __align__(16) float smf[];  // the face loop reads 16-byte vectors
+  __shared__ GroupScratch gsa[kMaxWideGroups];
   const int N = a.n_tab[a.it->k];
   const int64_t total = (int64_t)a.it->num_act * N;
-  const int G = group_width(total, (int64_t)gridDim.x * (blockDim.x >> 5));
+  const int G0 = group_width(total, (int64_t)gridDim.x * (blockDim.x >> 5));
   int64_t c = total / (16 * (int64_t)gridDim.x);
   c = c < 32 ? 32 : c > 1024 ? 1024 : c;
   const int chunk = (int)(c / 32) * 32;
   const int ips = (N + chunk - 1) / chunk;
   const int items = a.it->num_act * ips;  // at most slots * N / 32
+  constexpr int stage_floats = (int)(SampleStage<MINB>::bytes / sizeof(float));
   int staged = -1;
   for (int it = blockIdx.x; it < items;) {
     const int slot = a.act[it / ips], first = (int)(it % ips) * chunk, last = min(N, first + chunk);
     const SlotState& S = a.slots[slot];
-    const int dim = S.dim, F = S.nf;
-    const float* At = a.fpool + S.at_off;
-    const float* b = a.fpool + S.b_off;
+    const int dim = S.dim, P = (S.nf + 1) >> 1, rs = pair_stride(dim);
+    const float* rows = a.fpool + S.pr_off;
     const float* ls = a.fpool + S.seg_off;
     float* out = a.fpool + S.smp_off;
-    using SC = StageCfg<MINB>;
-    constexpr bool rows = LAY == kLayRows;
-    const bool fits = F <= (dim <= 8 ? (rows ? SC::r8 : SC::f8) : (rows ? SC::r16 : SC::f16));
+    const int G = pair_group_width(G0, P, KP);  // the batch refuses capacities that need more than 256 lanes
+    const bool fits = P * rs <= stage_floats;
     if (fits && staged != slot) {
       __syncthreads();  // the previous slot's chains are done with the buffer
-      if (rows) {
-        if (dim <= 8)
-          stage_rows<8>(At, a.capacity, b, F, dim, smf);
-        else
-          stage_rows<16>(At, a.capacity, b, F, dim, smf);
-      } else {
-        if (dim <= 8)
-          stage_polytope<8, SC::f8>(At, a.capacity, b, F, dim, smf);
-        else
-          stage_polytope<16, SC::f16>(At, a.capacity, b, F, dim, smf);
-      }
+      stage_pairs(rows, P, rs, smf);
       __syncthreads();
       staged = slot;
     }
+    const float* src = fits ? smf : rows;
     if (dim <= 8)
-      sample_range<8, U, LAY, SC::f8, SC::f16>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u,
-                                               out, G, smf, fits);
+      sample_region<8, KP>(G, src, P, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, gsa);
     else
-      sample_range<16, U, LAY, SC::f8, SC::f16>(At, a.capacity, b, F, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u,
-                                                out, G, smf, fits);
+      sample_region<16, KP>(G, src, P, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, gsa);
     it = claim_item(&a.it->sample_next);
   }
 }
 
-// Block per slot: the domain rows of A into At.
-__global__ void batch_transpose_kernel(BatchArgs a) {
+// Block per slot: the face-pair rows of the domain (start slacks at the
+// slot's segment start).
+__global__ void batch_init_rows_kernel(BatchArgs a) {
   if ((int)blockIdx.x >= a.num_slots) return;
   const SlotState& S = a.slots[blockIdx.x];
-  const float* A = a.fpool + S.a_off;
-  float* At = a.fpool + S.at_off;
-  for (int i = threadIdx.x; i < S.nf * S.dim; i += blockDim.x)
-    At[(int64_t)(i % S.dim) * a.capacity + i / S.dim] = A[i];
+  put_faces(a.fpool + S.a_off, a.fpool + S.b_off, S.nf, S.dim, a.fpool + S.seg_off, a.fpool + S.pr_off, threadIdx.x,
+            blockDim.x);
 }
 
 // Loads plant `pi` into the block's shared DevPlant and stages its statics.
@@ -327,7 +326,7 @@ __global__ void __launch_bounds__(1024) batch_faces_kernel(BatchArgs a) {
     const float* ls = a.fpool + S.seg_off;
     faces_block(S.K, S.dim, a.max_faces, a.capacity, a.margin, ls, ls + S.dim, a.fpool + S.col_off,
                 a.fpool + S.col_off + (int64_t)a.num_particles * S.dim, a.fpool + S.dist_off, a.fpool + S.a_off,
-                a.fpool + S.b_off, &S.nf, &S.cnt, a.fpool + S.at_off);
+                a.fpool + S.b_off, &S.nf, &S.cnt, a.fpool + S.pr_off);
     if (threadIdx.x == 0) {
       S.iters = k + 1;
       S.status = S.cnt.status;
@@ -340,18 +339,20 @@ __global__ void __launch_bounds__(1024) batch_faces_kernel(BatchArgs a) {
 // One block: advances k and rebuilds the active-slot list (ascending).
 __global__ void __launch_bounds__(1024) batch_step_kernel(BatchArgs a) {
   __shared__ int warp_n[32];
-  __shared__ int base, mf8, mf16;
+  __shared__ int base, mf8, mf16, nord;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   if (tid == 0) {
     base = 0;
     mf8 = 0;
     mf16 = 0;
+    nord = 0;
   }
   __syncthreads();
   for (int s0 = 0; s0 < a.num_slots; s0 += blockDim.x) {
     const int s = s0 + tid;
     const bool act = s < a.num_slots && !a.slots[s].done;
     if (act) atomicMax(a.slots[s].dim <= 8 ? &mf8 : &mf16, a.slots[s].nf);
+    if (act && a.slots[s].ord) atomicAdd(&nord, 1);
     const unsigned m = __ballot_sync(0xffffffffu, act);
     if (lane == 0) warp_n[warp] = __popc(m);
     __syncthreads();
@@ -371,6 +372,7 @@ __global__ void __launch_bounds__(1024) batch_step_kernel(BatchArgs a) {
     it->num_act = base;
     it->max_nf8 = mf8;
     it->max_nf16 = mf16;
+    it->num_ord = nord;
   }
 }
 
@@ -388,6 +390,7 @@ __global__ void __launch_bounds__(mlp::kThreads) batch_score_kernel(BatchArgs a)
   if (row0 >= N) return;
   const int slot = a.act[blockIdx.y];
   const SlotState& S = a.slots[slot];
+  if (!S.ord) return;  // this slot checks in sample order: no scores needed
   mlp::FwdGroup G{};
   G.x = a.fpool + S.smp_off;
   G.rows = N;
@@ -423,8 +426,17 @@ __global__ void __launch_bounds__(1024) batch_sort_kernel(BatchArgs a) {
   if ((int)blockIdx.x >= a.it->num_act) return;
   const int slot = a.act[blockIdx.x];
   const int N = a.n_tab[a.it->k];
+  int* ord = a.order + (size_t)slot * a.n_max;
+  uint8_t* flags = a.bpool + a.slots[slot].flag_off;
+  const bool sorted = a.slots[slot].ord != 0;  // uniform across the block
+  if (!sorted)
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+      ord[i] = i;
+      flags[i] = 2;  // unchecked this iteration
+    }
   int P = 1;
   while (P < N) P <<= 1;
+  if (!sorted) P = 0;
   const float* sc = a.scores + (size_t)slot * a.n_max;
   for (int i = threadIdx.x; i < P; i += blockDim.x) {
     unsigned long long key = ~0ull;
@@ -450,12 +462,11 @@ __global__ void __launch_bounds__(1024) batch_sort_kernel(BatchArgs a) {
       }
       __syncthreads();
     }
-  int* ord = a.order + (size_t)slot * a.n_max;
-  uint8_t* flags = a.bpool + a.slots[slot].flag_off;
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
-    ord[i] = (int)(keys[i] & 0xffffffffu);
-    flags[i] = 2;  // unchecked this iteration
-  }
+  if (sorted)
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+      ord[i] = (int)(keys[i] & 0xffffffffu);
+      flags[i] = 2;  // unchecked this iteration
+    }
   if (threadIdx.x == 0) {
     SlotState& S = a.slots[slot];
     S.pos = 0;
@@ -554,7 +565,9 @@ __global__ void __launch_bounds__(256) batch_tally_kernel(BatchArgs a, int r) {
     S.m_coll += mcoll;
     S.pos = end;
     int need;
-    if ((float)S.m_coll > a.thr_tab[k])
+    if (!S.ord)
+      need = end < N;  // sample order: every sample, as the batched form
+    else if ((float)S.m_coll > a.thr_tab[k])
       need = S.coll < a.num_particles && end < N &&
              a.scores[(size_t)blockIdx.x * a.n_max + ord[end]] >= a.stop_logit;
     else
@@ -601,6 +614,9 @@ __global__ void __launch_bounds__(1024) batch_compact_sorted_kernel(BatchArgs a)
     __syncthreads();
   }
   if (tid == 0) {
+    // ordering that left fewer than 1/8 of the samples unchecked is not worth its
+    // scoring, sort and rounds: the slot checks in sample order from now on
+    if (S.ord && 8ll * (N - S.pos) < (long long)N) S.ord = 0;
     S.configs += S.pos;
     S.cnt.total = (uint32_t)base;
     S.cnt.first_m = (uint32_t)S.m_coll;
@@ -615,33 +631,32 @@ __global__ void __launch_bounds__(1024) batch_compact_sorted_kernel(BatchArgs a)
   }
 }
 
-// Sampler variants the autotuner chooses from: U faces (packed: U face
-// pairs) per lane and trip, MINB resident blocks per SM (register cap), the
-// staged layout (transposed columns, packed column pairs, face rows).
+// Sampler variants the autotuner chooses from: KP face pairs per lane at
+// most (register-held slacks; wider groups for larger regions) and MINB
+// resident blocks per SM (register cap and staging buffer). Every variant
+// yields the same samples.
 using SampleFn = void (*)(BatchArgs);
 struct SampleVariant {
   SampleFn fn;
-  int u, minb;
-  size_t smem;   // staging buffer (StageCfg<minb>::bytes)
+  int kp, minb;
+  size_t smem;   // staging buffer (SampleStage<minb>::bytes)
   int f8, f16;   // faces staged for dim <= 8 / <= 16
 };
-#define CSD_SAMPLE_VARIANT(U, MINB, LAY)                                                    \
-  {                                                                                         \
-    batch_sample_kernel<U, MINB, LAY>, U, MINB, StageCfg<MINB>::bytes,                      \
-        LAY == kLayRows ? StageCfg<MINB>::r8 : StageCfg<MINB>::f8,                          \
-        LAY == kLayRows ? StageCfg<MINB>::r16 : StageCfg<MINB>::f16                         \
+#define CSD_SAMPLE_VARIANT(KP, MINB)                                                                 \
+  {                                                                                                  \
+    batch_sample_kernel<KP, MINB>, KP, MINB, SampleStage<MINB>::bytes,                               \
+        2 * (int)(SampleStage<MINB>::bytes / (pair_stride(8) * sizeof(float))),                      \
+        2 * (int)(SampleStage<MINB>::bytes / (pair_stride(16) * sizeof(float)))                      \
   }
 static const SampleVariant kSampleVariants[] = {
-    CSD_SAMPLE_VARIANT(1, 2, kLayStrided), CSD_SAMPLE_VARIANT(2, 2, kLayStrided),
-    CSD_SAMPLE_VARIANT(1, 3, kLayStrided), CSD_SAMPLE_VARIANT(2, 3, kLayStrided),
-    CSD_SAMPLE_VARIANT(4, 2, kLayStrided), CSD_SAMPLE_VARIANT(4, 3, kLayStrided),
-    CSD_SAMPLE_VARIANT(1, 2, kLayPacked),  CSD_SAMPLE_VARIANT(2, 2, kLayPacked),
-    CSD_SAMPLE_VARIANT(1, 3, kLayPacked),  CSD_SAMPLE_VARIANT(2, 3, kLayPacked),
-    CSD_SAMPLE_VARIANT(1, 4, kLayStrided), CSD_SAMPLE_VARIANT(2, 4, kLayStrided),
-    CSD_SAMPLE_VARIANT(1, 3, kLayRows),    CSD_SAMPLE_VARIANT(2, 3, kLayRows),
-    CSD_SAMPLE_VARIANT(1, 4, kLayRows),    CSD_SAMPLE_VARIANT(1, 2, kLayRows),
+    CSD_SAMPLE_VARIANT(8, 1), CSD_SAMPLE_VARIANT(8, 2), CSD_SAMPLE_VARIANT(8, 3),
+    CSD_SAMPLE_VARIANT(16, 1), CSD_SAMPLE_VARIANT(16, 2),
 };
 #undef CSD_SAMPLE_VARIANT
+// Smallest KP of the variants: a region of up to 2 * 256 * kMinKP faces fits
+// every variant's widest group.
+constexpr int kMinKP = 8;
+static_assert(2 * 256 * kMinKP >= kMaxRegionFaces, "every variant samples the largest region");
 constexpr int kNumSampleVariants = (int)(sizeof(kSampleVariants) / sizeof(kSampleVariants[0]));
 // Largest check work item (configurations) the autotuner chooses from.
 constexpr int kCheckItemCaps[] = {32, 128, 512};
@@ -682,6 +697,8 @@ struct csd_batch_s {
   std::vector<int> act_host;
   cudaGraphExec_t graph = nullptr;
   int graph_slots = -1, graph_cfg = -1, graph_variant = -1;
+  int graph_kernels = 0;        // kernel nodes of the captured iteration
+  long long launches = 0;       // kernels launched by the last inflate
   const void* graph_mlp = nullptr;
   cudaStream_t graph_stream = nullptr;
   csd::BatchIter* host_iter = nullptr;
@@ -690,7 +707,7 @@ struct csd_batch_s {
   double stage_ms[csd::kStages] = {};
   std::vector<float> iter_ms;   // profiling mode: [iteration][kStages] of the last inflate
   std::vector<int> iter_active; // slots active at the start of each iteration
-  double sample_flop = 0.0;     // profiling mode: sampler FLOPs of the last inflate (4 d F per chain step)
+  double sample_flop = 0.0;     // profiling mode: sampler FLOPs of the last inflate ((2 d + 4) F per chain step)
   ~csd_batch_s() {
     for (cudaEvent_t e : ev)
       if (e) cudaEventDestroy(e);
@@ -703,6 +720,18 @@ struct csd_batch_s {
 using namespace csd;
 
 namespace {
+
+// Floats of one slot's face-pair rows, and of all its buffers (a multiple of
+// 4, so every slot's rows start 16-byte aligned): pair rows, A, b, segment,
+// samples, collision points and projections, distances.
+size_t pair_floats(const csd_batch_s* h) {
+  return ((size_t)h->capacity / 2 + 1) * (size_t)pair_stride(h->max_dim);
+}
+size_t slot_floats(const csd_batch_s* h) {
+  const size_t D = (size_t)h->max_dim, np = h->opt.num_particles, cap = (size_t)h->capacity;
+  const size_t f = pair_floats(h) + cap * D + cap + 2 * D + (size_t)h->n_max * D + 2 * np * D + np;
+  return (f + 3) & ~size_t(3);
+}
 
 // Sampler variant for regions of up to nf8 (dim <= 8) and nf16 faces: the
 // fastest by tuning time among those whose staging buffer holds them, else
@@ -727,8 +756,9 @@ int variant_for(const csd_batch_s* h, int nf8, int nf16) {
 // One iteration's launches on stream s. ev (kStages + 1 events) brackets the
 // stages for the profiling mode; skip_sample leaves out the sampler (the
 // autotuner has just run it).
-void launch_iteration(csd_batch_s* h, int num_slots, const BatchArgs& a, cudaStream_t s, cudaEvent_t* ev,
-                      bool skip_sample = false) {
+// Returns the number of kernels launched.
+int launch_iteration(csd_batch_s* h, int num_slots, const BatchArgs& a, cudaStream_t s, cudaEvent_t* ev,
+                     bool skip_sample = false) {
   if (!skip_sample) cudaMemsetAsync(&a.it->sample_next, 0, sizeof(int), s);  // the sampler's work queue
   if (ev) cudaEventRecord(ev[0], s);
   if (!skip_sample)
@@ -773,6 +803,8 @@ void launch_iteration(csd_batch_s* h, int num_slots, const BatchArgs& a, cudaStr
   if (ev) cudaEventRecord(ev[7], s);
   batch_step_kernel<<<1, 1024, 0, s>>>(a);
   if (ev) cudaEventRecord(ev[8], s);
+  // sampler; score, sort, (check + tally) per round, compaction | check, compaction; bisect, faces, step
+  return (skip_sample ? 0 : 1) + (a.mlp_wb ? 3 + 2 * a.rounds : 2) + 3;
 }
 
 csd_status_t build_graph(csd_batch_s* h, int num_slots, const BatchArgs& a) {
@@ -786,7 +818,7 @@ csd_status_t build_graph(csd_batch_s* h, int num_slots, const BatchArgs& a) {
   cudaStream_t s = h->graph_stream;
   cudaGraph_t g = nullptr;
   CSD_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-  launch_iteration(h, num_slots, a, s, nullptr);
+  h->graph_kernels = launch_iteration(h, num_slots, a, s, nullptr);
   cudaError_t e = cudaStreamEndCapture(s, &g);
   if (e != cudaSuccess) {
     set_error(std::string("graph capture failed: ") + cudaGetErrorString(e));
@@ -813,6 +845,8 @@ csd_status_t csd_batch_create(const csd_plant_t* plants, int32_t num_plants, int
                               const csd_eizo_options_t* o, int32_t face_capacity, csd_batch_t* out) {
   CSD_CHECK(plants && num_plants > 0 && max_slots > 0 && o && out && face_capacity > 0, CSD_ERR_INVALID,
             "bad batch arguments");
+  CSD_CHECK(face_capacity <= kMaxRegionFaces, CSD_ERR_CAPACITY,
+            "face capacity above " + std::to_string(kMaxRegionFaces) + " (the sampler's largest region)");
   *out = nullptr;
   CSD_CHECK(o->num_particles >= 1 && o->max_iterations >= 1, CSD_ERR_INVALID,
             "num_particles and max_iterations must be positive");
@@ -881,8 +915,7 @@ csd_status_t csd_batch_create(const csd_plant_t* plants, int32_t num_plants, int
     h->sample_grid[v] = device_sm_count() * std::max(1, per_sm);
   }
   // buffers
-  const size_t D = (size_t)h->max_dim, np = o->num_particles, cap = (size_t)face_capacity;
-  const size_t per_slot_f = 2 * cap * D + cap + 2 * D + (size_t)h->n_max * D + 2 * np * D + np;
+  const size_t per_slot_f = slot_floats(h.get());
   if ((s = h->plants_dev.reserve(dps.size() * sizeof(DevPlant))) || (s = h->slots_dev.reserve(max_slots * sizeof(SlotState))) ||
       (s = h->tabs.reserve(h->n_tab.size() * 12 + 64)) || (s = h->fpool.reserve(per_slot_f * max_slots * 4 + 256)) ||
       (s = h->bpool.reserve((size_t)h->n_max * max_slots + 256)) || (s = h->iter.reserve(sizeof(BatchIter))) ||
@@ -928,7 +961,7 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
     }
   } restore{cur, h->device};
   const size_t D = (size_t)h->max_dim, np = h->opt.num_particles, cap = (size_t)h->capacity;
-  const size_t per_slot_f = 2 * cap * D + cap + 2 * D + (size_t)h->n_max * D + 2 * np * D + np;
+  const size_t per_slot_f = slot_floats(h);
   std::vector<SlotState> slots(n);
   size_t qoff = 0, arow = 0;
   cudaStream_t st = h->graph_stream;
@@ -958,10 +991,11 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
     S.dim = d;
     S.domain_faces = f1 - f0;
     S.nf = f1 - f0;
+    S.ord = 1;
     const long long base = (long long)(per_slot_f * i);
-    S.a_off = base;
-    S.at_off = S.a_off + (long long)(cap * D);
-    S.b_off = S.at_off + (long long)(cap * D);
+    S.pr_off = base;  // 16-byte aligned: per_slot_f is a multiple of 4 floats
+    S.a_off = S.pr_off + (long long)pair_floats(h);
+    S.b_off = S.a_off + (long long)(cap * D);
     S.seg_off = S.b_off + (long long)cap;
     S.smp_off = S.seg_off + (long long)(2 * D);
     S.col_off = S.smp_off + (long long)((size_t)h->n_max * D);
@@ -1038,7 +1072,8 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
   }
   a.status = h->status.as<int>();
   CSD_CUDA_TRY(cudaMemsetAsync(h->status.ptr, 0, 16, st));
-  batch_transpose_kernel<<<n, 256, 0, st>>>(a);
+  batch_init_rows_kernel<<<n, 256, 0, st>>>(a);
+  h->launches = 1;
   CSD_CUDA_TRY(cudaGetLastError());
   h->run_variant = h->sample_variant;
   csd_status_t s = build_graph(h, n, a);
@@ -1070,6 +1105,7 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
         cudaEventRecord(tev[2 * j], st);
         kSampleVariants[v].fn<<<h->sample_grid[v], 256, kSampleVariants[v].smem, st>>>(a);
         cudaEventRecord(tev[2 * j + 1], st);
+        ++h->launches;
       }
       for (int c = 0; c < kNumCheckVariants && !a.mlp_wb; ++c, ++j) {
         BatchArgs ac = a;
@@ -1081,8 +1117,9 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
         else
           batch_check_kernel<false><<<h->check_grid, 32 * kWarpsPerBlock, h->check_smem, st>>>(ac, 0);
         cudaEventRecord(tev[2 * j + 1], st);
+        ++h->launches;
       }
-      launch_iteration(h, n, a, st, nullptr, true);
+      h->launches += launch_iteration(h, n, a, st, nullptr, true);
       CSD_CUDA_TRY(cudaGetLastError());
       CSD_CUDA_TRY(cudaStreamSynchronize(st));
       for (int q = 0; q < j; ++q) {
@@ -1108,7 +1145,7 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
         if ((s = build_graph(h, n, a))) return s;
       }
     } else if (h->profile) {
-      launch_iteration(h, n, a, st, h->ev);
+      h->launches += launch_iteration(h, n, a, st, h->ev);
       CSD_CUDA_TRY(cudaGetLastError());
       CSD_CUDA_TRY(cudaEventSynchronize(h->ev[kStages]));
       for (int j = 0; j < kStages; ++j) {
@@ -1121,16 +1158,24 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
       // sampler work of this iteration, from the records before it ran
       for (const SlotState& S : prof_slots)
         if (!S.done)
-          h->sample_flop += (double)h->n_tab[k] * h->opt.mixing_steps * 4.0 * S.dim * S.nf;
+          h->sample_flop += (double)h->n_tab[k] * h->opt.mixing_steps * (2.0 * S.dim + 4.0) * S.nf;
       CSD_CUDA_TRY(cudaMemcpyAsync(prof_slots.data(), h->slots_dev.ptr, n * sizeof(SlotState),
                                    cudaMemcpyDeviceToHost, st));
     } else {
       CSD_CUDA_TRY(cudaGraphLaunch(h->graph, st));
+      h->launches += h->graph_kernels;
     }
     CSD_CUDA_TRY(cudaMemcpyAsync(h->host_iter, h->iter.ptr, sizeof(BatchIter), cudaMemcpyDeviceToHost, st));
     CSD_CUDA_TRY(cudaStreamSynchronize(st));
     active_now = h->host_iter->last_active;
     if (active_now == 0) break;
+    // surrogate mode: once no active slot checks in surrogate order, the remaining
+    // iterations run the batched form's graph (no scoring, sorting or rounds; the
+    // same checks as a slot checking in sample order)
+    if (a.mlp_wb && h->host_iter->num_ord == 0 && h->tune_iters == 0) {
+      a.mlp_wb = nullptr;
+      if ((s = build_graph(h, n, a))) return s;
+    }
     // a slot's region outgrew the staging buffer of the running variant: continue with the
     // fastest variant that stages it (identical samples; the graph is captured again)
     if (h->switch_large && h->tune_iters == 0) {
@@ -1283,6 +1328,12 @@ csd_status_t csd_batch_tuning(csd_batch_t h, int32_t* sample_variant, int32_t* c
   if (num_variants) *num_variants = kNumSampleVariants + kNumCheckVariants;
   if (variant_ms)
     for (int q = 0; q < kNumSampleVariants + kNumCheckVariants; ++q) variant_ms[q] = (float)h->tune_ms[q];
+  return CSD_OK;
+}
+
+csd_status_t csd_batch_last_launches(csd_batch_t h, int64_t* launches) {
+  CSD_CHECK(h && launches, CSD_ERR_INVALID, "null argument");
+  *launches = h->launches;
   return CSD_OK;
 }
 

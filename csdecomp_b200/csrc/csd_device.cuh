@@ -31,6 +31,7 @@ enum : int { J_FIXED = 0, J_REVOLUTE = 1, J_PRISMATIC = 2 };
 enum : int { G_BOX = 0, G_SPHERE = 1, G_CYLINDER = 2, G_CAPSULE = 3 };
 
 constexpr int kMaxDim = 16;          // configuration variables per plant
+constexpr int kMaxRegionFaces = 4096;  // faces of an EI-ZO region (the reference's MAX_NUM_FACES is 4000)
 constexpr int kMaxSlots = 32;        // moving links evaluated per configuration
 constexpr int kWarp = 32;
 

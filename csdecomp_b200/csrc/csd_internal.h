@@ -140,11 +140,14 @@ csd_status_t launch_hit_and_run(const float* A, const float* b, const int32_t* f
                                 const float* starts, int samples_per_poly, int mixing, uint64_t seed,
                                 uint32_t stream_base, int fail_keep, float* out, int* num_failed,
                                 const int* num_faces_dev, cudaStream_t st);
-// warp-per-chain sampler over one polytope stored transposed (At[k * ldt + f])
-csd_status_t launch_hit_and_run_warp(const float* At, int ldt, const float* b, const int* num_faces_dev, int dim,
-                                     const float* start, int S, int mixing, uint64_t seed, uint32_t stream,
-                                     int fail_keep, float* out, cudaStream_t st);
-csd_status_t launch_transpose_faces(const float* A, int F, int d, float* At, int ldt, cudaStream_t st);
+// EI-ZO sampler over one region stored as face-pair rows (sampler_core.cuh,
+// pair_stride(dim) floats per row, start slacks at `start`); the face count is
+// read on the device. A failed chain keeps its start point.
+csd_status_t launch_sample_region(const float* rows, const int* num_faces_dev, int dim, const float* start, int S,
+                                  int mixing, uint64_t seed, uint32_t stream, float* out, cudaStream_t st);
+// Face-pair rows of faces [0, F) of row-major A and b (start slacks at x0).
+csd_status_t launch_put_faces(const float* A, const float* b, int F, int dim, const float* x0, float* rows,
+                              cudaStream_t st);
 
 int device_sm_count();
 

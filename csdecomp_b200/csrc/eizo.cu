@@ -8,7 +8,8 @@
 // maybePlaceFace with two memcpys and a redundancy kernel.
 //
 // Here an iteration is five launches and one 16-byte device-to-host read:
-//   1. hit_and_run_kernel           M_k chains in the current region
+//   1. sample_region_kernel         M_k chains in the current region (face-pair
+//                                    rows, slacks carried from step to step)
 //   2. check_points_kernel          fused FK + pair sweep, one verdict byte each
 //   3. compact_kernel               one block: ordered prefix scan of the
 //                                    colliding samples (the reference's atomicAdd
@@ -65,8 +66,8 @@ __global__ void __launch_bounds__(1024) faces_kernel(int K, int dim, int max_fac
                                                      const float* __restrict__ cols, const float* __restrict__ proj,
                                                      float* __restrict__ dist, float* __restrict__ A,
                                                      float* __restrict__ b, int* __restrict__ num_faces,
-                                                     EizoCounters* cnt, float* __restrict__ At) {
-  faces_block(K, dim, max_faces, capacity, margin, ls, le, cols, proj, dist, A, b, num_faces, cnt, At);
+                                                     EizoCounters* cnt, float* __restrict__ rows) {
+  faces_block(K, dim, max_faces, capacity, margin, ls, le, cols, proj, dist, A, b, num_faces, cnt, rows);
 }
 
 }  // namespace csd
@@ -84,7 +85,7 @@ struct csd_inflator_s {
   std::vector<float> domain_A, domain_b;
   std::vector<uint32_t> vtab_host;
   int num_other = 0;
-  csd::DevBuf A, At, b, nf, samples, flags, cols, proj, dist, seg, vox, vtab, vgrid, cnt;
+  csd::DevBuf A, rows, b, nf, samples, flags, cols, proj, dist, seg, vox, vtab, vgrid, cnt;
   csd::EizoCounters* host_cnt = nullptr;  // pinned
   int* host_nf = nullptr;                 // pinned
   ~csd_inflator_s() {
@@ -137,6 +138,7 @@ csd_status_t csd_inflator_create(csd_plant_t plant, const int32_t* ids, int32_t 
   const int d = plant->dp.dim;
   CSD_CHECK(d >= 1 && d <= kMaxDim, CSD_ERR_DIMENSION, "plant dimension must be in [1, 16]");
   CSD_CHECK(capacity >= F0 && capacity > 0, CSD_ERR_CAPACITY, "face capacity smaller than the domain");
+  CSD_CHECK(capacity <= kMaxRegionFaces, CSD_ERR_CAPACITY, "face capacity above 4096 (the sampler's largest region)");
   CSD_CHECK(o->num_particles >= 1 && o->max_iterations >= 1, CSD_ERR_INVALID, "num_particles and max_iterations must be positive");
   CSD_CHECK(o->tau > 0.f && o->tau < 1.f && o->epsilon > 0.f && o->delta > 0.f, CSD_ERR_INVALID, "bad epsilon/delta/tau");
   // EizoGpuMemory sizing, cuda_edge_inflation_zero_order.cu:448-494
@@ -165,7 +167,8 @@ csd_status_t csd_inflator_create(csd_plant_t plant, const int32_t* ids, int32_t 
   csd_status_t s;
   if ((s = build_voxel_tables(plant, ids, nr, &h->vtab_host, &h->num_other))) return s;
   const size_t np = o->num_particles, mc = (size_t)h->max_configs;
-  if ((s = h->A.reserve((size_t)capacity * d * 4)) || (s = h->At.reserve((size_t)capacity * d * 4)) ||
+  if ((s = h->A.reserve((size_t)capacity * d * 4)) ||
+      (s = h->rows.reserve(((size_t)capacity / 2 + 1) * pair_stride(d) * 4)) ||
       (s = h->b.reserve((size_t)capacity * 4)) ||
       (s = h->nf.reserve(16)) || (s = h->samples.reserve(mc * d * 4)) || (s = h->flags.reserve(mc + 16)) ||
       (s = h->cols.reserve(np * d * 4)) || (s = h->proj.reserve(np * d * 4)) || (s = h->dist.reserve(np * 4)) ||
@@ -175,8 +178,6 @@ csd_status_t csd_inflator_create(csd_plant_t plant, const int32_t* ids, int32_t 
   if (F0) {
     CSD_CUDA_TRY(cudaMemcpy(h->A.ptr, dA, (size_t)F0 * d * 4, cudaMemcpyHostToDevice));
     CSD_CUDA_TRY(cudaMemcpy(h->b.ptr, db, (size_t)F0 * 4, cudaMemcpyHostToDevice));
-    if ((s = launch_transpose_faces(h->A.as<float>(), F0, d, h->At.as<float>(), capacity, 0))) return s;
-    CSD_CUDA_TRY(cudaDeviceSynchronize());
   }
   if (!h->vtab_host.empty())
     CSD_CUDA_TRY(cudaMemcpy(h->vtab.ptr, h->vtab_host.data(), h->vtab_host.size() * 4, cudaMemcpyHostToDevice));
@@ -230,6 +231,9 @@ csd_status_t csd_inflator_inflate(csd_inflator_t h, const float* ls, const float
   const float* ls_d = h->seg.as<float>();
   const float* le_d = ls_d + d;
   csd_status_t s;
+  // the domain's face-pair rows with their slacks at this segment's start
+  if ((s = launch_put_faces(h->A.as<float>(), h->b.as<float>(), h->domain_faces, d, ls_d, h->rows.as<float>(), st)))
+    return s;
   VoxelTables vt;
   if (nv > 0 && !h->vtab_host.empty()) {
     vt.vox = h->vox.as<float>();
@@ -250,8 +254,8 @@ csd_status_t csd_inflator_inflate(csd_inflator_t h, const float* ls, const float
     float delta_k = (float)(6 * o.delta / (M_PI * M_PI * (it + 1) * (it + 1)));
     uint32_t M = csd_num_samples_unadaptive(o.epsilon, delta_k, o.tau);
     uint32_t N = std::max(M, o.num_particles);
-    if ((s = launch_hit_and_run_warp(h->At.as<float>(), h->capacity, h->b.as<float>(), h->nf.as<int>(), d, ls_d,
-                                     (int)N, (int)o.mixing_steps, o.seed, 0u, 1, h->samples.as<float>(), st)))
+    if ((s = launch_sample_region(h->rows.as<float>(), h->nf.as<int>(), d, ls_d, (int)N, (int)o.mixing_steps, o.seed,
+                                  0u, h->samples.as<float>(), st)))
       return s;
     if ((s = launch_check_points(p, h->samples.as<float>(), N, vt, h->flags.as<uint8_t>(), st))) return s;
     compact_kernel<<<1, 1024, 0, st>>>(h->flags.as<uint8_t>(), h->samples.as<float>(), (int)N, (int)M,
@@ -290,7 +294,7 @@ csd_status_t csd_inflator_inflate(csd_inflator_t h, const float* ls, const float
     faces_kernel<<<1, 1024, 0, st>>>((int)K, d, (int)o.max_hyperplanes_per_iteration, h->capacity,
                                      o.configuration_margin, ls_d, le_d, h->cols.as<float>(), h->proj.as<float>(),
                                      h->dist.as<float>(), h->A.as<float>(), h->b.as<float>(), h->nf.as<int>(), cnt,
-                                     h->At.as<float>());
+                                     h->rows.as<float>());
     CSD_CUDA_TRY(cudaGetLastError());
     rec.num_collisions_updated = (int32_t)K;
     auto t1 = std::chrono::high_resolution_clock::now();
@@ -387,6 +391,7 @@ extern "C" csd_status_t csd_eizo_noalloc(csd_plant_t plant, const float* ls, con
   CSD_CHECK(d >= 1 && d <= kMaxDim, CSD_ERR_DIMENSION, "plant dimension must be in [1, 16]");
   CSD_CHECK(capacity >= F0 && capacity > 0 && F0 <= 0.9 * capacity, CSD_ERR_CAPACITY,
             "The domain polyhedron is already reserving almost all of the allocated faces.");
+  CSD_CHECK(capacity <= kMaxRegionFaces, CSD_ERR_CAPACITY, "face capacity above 4096 (the sampler's largest region)");
   CSD_CHECK(o->num_particles >= 1 && o->max_iterations >= 1, CSD_ERR_INVALID,
             "num_particles and max_iterations must be positive");
   CSD_CHECK(o->tau > 0.f && o->tau < 1.f && o->epsilon > 0.f && o->delta > 0.f, CSD_ERR_INVALID,
@@ -411,10 +416,11 @@ extern "C" csd_status_t csd_eizo_noalloc(csd_plant_t plant, const float* ls, con
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   const size_t vtab_words = (size_t)plant->dp.num_tiles + (size_t)nr;
   const size_t sz_A = al((size_t)capacity * d * 4), sz_b = al((size_t)capacity * 4), sz_nf = 256,
+               sz_rows = al(((size_t)capacity / 2 + 1) * pair_stride(d) * 4),
                sz_samples = al(max_configs * d * 4), sz_flags = al(max_configs), sz_cols = al(np * d * 4),
                sz_dist = al(np * 4), sz_seg = al(2 * (size_t)d * 4), sz_vox = al((size_t)nv * 12),
                sz_vtab = al(vtab_words * 4), sz_cnt = 256;
-  const size_t need = sz_A + sz_b + sz_nf + sz_samples + sz_flags + 2 * sz_cols + sz_dist + sz_seg + sz_vox +
+  const size_t need = sz_A + sz_rows + sz_b + sz_nf + sz_samples + sz_flags + 2 * sz_cols + sz_dist + sz_seg + sz_vox +
                       sz_vtab + sz_cnt;
   if (need > kNoAllocScratchBytes) {
     set_error("csd_eizo_noalloc needs " + std::to_string(need) + " bytes of scratch for these options, more than its " +
@@ -441,6 +447,7 @@ extern "C" csd_status_t csd_eizo_noalloc(csd_plant_t plant, const float* ls, con
     return p;
   };
   float* A = (float*)take(sz_A);
+  float* rows = (float*)take(sz_rows);
   float* b = (float*)take(sz_b);
   int* nf = (int*)take(sz_nf);
   float* samples = (float*)take(sz_samples);
@@ -479,6 +486,7 @@ extern "C" csd_status_t csd_eizo_noalloc(csd_plant_t plant, const float* ls, con
   CSD_CUDA_TRY(cudaMemcpyAsync(seg + d, le, d * 4, cudaMemcpyHostToDevice, st));
   if (nv) CSD_CUDA_TRY(cudaMemcpyAsync(vox, voxels, (size_t)nv * 12, cudaMemcpyHostToDevice, st));
   if (vtab_words) CSD_CUDA_TRY(cudaMemcpyAsync(vtab, vt_host, (T + num_other) * 4, cudaMemcpyHostToDevice, st));
+  if ((s = launch_put_faces(A, b, F0, d, seg, rows, st))) return s;  // the domain's face-pair rows
   CSD_CUDA_TRY(cudaStreamSynchronize(st));  // host staging arrays go out of scope below
   VoxelTables vt;
   if (nv > 0 && nr > 0) {
@@ -497,8 +505,7 @@ extern "C" csd_status_t csd_eizo_noalloc(csd_plant_t plant, const float* ls, con
     float delta_k = (float)(6 * o->delta / (M_PI * M_PI * (it + 1) * (it + 1)));
     uint32_t M = csd_num_samples_unadaptive(o->epsilon, delta_k, o->tau);
     uint32_t N = std::max(M, o->num_particles);
-    if ((s = launch_hit_and_run(A, b, nullptr, 1, d, seg, (int)N, (int)o->mixing_steps, o->seed, 0u, 1, samples,
-                                nullptr, nf, st)))
+    if ((s = launch_sample_region(rows, nf, d, seg, (int)N, (int)o->mixing_steps, o->seed, 0u, samples, st)))
       return s;
     if ((s = launch_check_points(plant, samples, N, vt, flags, st))) return s;
     compact_kernel<<<1, 1024, 0, st>>>(flags, samples, (int)N, (int)M, (int)o->num_particles, d, cols, cnt);
@@ -530,7 +537,7 @@ extern "C" csd_status_t csd_eizo_noalloc(csd_plant_t plant, const float* ls, con
     if ((s = launch_bisect(plant, (int)K, d, (int)o->bisection_steps, seg, seg + d, va, cols, proj, dist, st))) return s;
     faces_kernel<<<1, 1024, 0, st>>>((int)K, d, (int)o->max_hyperplanes_per_iteration, capacity,
                                      o->configuration_margin, seg, seg + d, cols, proj, dist, A, b, nf, cnt,
-                                     nullptr);
+                                     rows);
     CSD_CUDA_TRY(cudaGetLastError());
     rec.num_collisions_updated = (int32_t)K;
     rec.iteration_time_ms =

@@ -5,6 +5,7 @@
 #include <cfloat>
 
 #include "check_core.cuh"
+#include "sampler_core.cuh"
 
 namespace csd {
 
@@ -114,13 +115,14 @@ static __device__ __forceinline__ void bisect_particle(const DevPlant& p, const 
 }
 
 // One block places up to max_faces faces (greedy, nearest collision first).
-// At (optional) receives the faces transposed, At[k * capacity + f].
+// rows (optional) receives each face as a face-pair row with its start slack
+// at ls (put_face), the layout the EI-ZO sampler reads.
 static __device__ __forceinline__ void faces_block(int K, int dim, int max_faces, int capacity, float margin,
                                                    const float* __restrict__ ls, const float* __restrict__ le,
                                                    const float* __restrict__ cols, const float* __restrict__ proj,
                                                    float* __restrict__ dist, float* __restrict__ A,
                                                    float* __restrict__ b, int* __restrict__ num_faces,
-                                                   EizoCounters* cnt, float* __restrict__ At = nullptr) {
+                                                   EizoCounters* cnt, float* __restrict__ rows = nullptr) {
   __shared__ float red_v[32];
   __shared__ int red_i[32];
   __shared__ float face[kMaxDim + 1];
@@ -196,9 +198,9 @@ static __device__ __forceinline__ void faces_block(int K, int dim, int max_faces
       bb = __fadd_rn(bb, relax);
       for (int k = 0; k < dim; ++k) {
         A[(size_t)nf * dim + k] = a[k];
-        if (At) At[(size_t)k * capacity + nf] = a[k];
         face[k] = a[k];
       }
+      if (rows) put_face(rows, dim, nf, a, bb, ls);
       b[nf] = bb;
       face[dim] = bb;
       dist[s] = FLT_MAX;

@@ -45,83 +45,72 @@ __global__ void __launch_bounds__(128) hit_and_run_kernel(const float* __restric
     if (k < dim) dst[k] = ok ? x[k] : fail_keep ? starts[(int64_t)poly * dim + k] : __int_as_float(0x7fc00000);
 }
 
-// Group-per-chain sampler over one polytope given transposed (At[k * ldt +
-// f]); the face count is read on the device. Used by the inflator, whose
-// region grows to hundreds of faces: the polytope is staged in shared memory
-// once per block (as face rows while they fit, else as transposed columns)
-// and the lanes of a group share the face loop.
-__global__ void __launch_bounds__(256) hit_and_run_group_kernel(const float* __restrict__ At, int ldt,
-                                                                const float* __restrict__ b,
-                                                                const int* __restrict__ num_faces_dev, int dim,
-                                                                const float* __restrict__ start, int S, int mixing,
-                                                                uint32_t k0, uint32_t k1, uint32_t stream,
-                                                                float* __restrict__ out) {
-  extern __shared__ __align__(16) float smf[];  // the face loop reads float2/float4 vectors
+// EI-ZO sampler over one region (the single inflation and the
+// allocation-free inflation), whose face count is read on the device: the
+// region's face-pair rows are staged in shared memory once per block when
+// they fit (else the chains read them from global memory, through L1), and
+// the block's chains run with G lanes each (sampler_core.cuh; G from the
+// chain count, widened so that a lane holds at most kRegionKP face pairs).
+constexpr int kRegionKP = 8;
+constexpr size_t kRegionStageBytes = 104 * 1024;  // two blocks per SM
+static_assert(kMaxRegionFaces <= 2 * 256 * kRegionKP, "the widest group samples the largest region");
+
+__global__ void __launch_bounds__(256, 2) sample_region_kernel(const float* __restrict__ rows,
+                                                              const int* __restrict__ num_faces_dev, int dim,
+                                                              const float* __restrict__ start, int S, int mixing,
+                                                              uint32_t k0, uint32_t k1, uint32_t stream,
+                                                              float* __restrict__ out) {
+  extern __shared__ __align__(16) float smf[];  // the face loop reads 16-byte vectors
+  __shared__ GroupScratch gsa[kMaxWideGroups];
   const int F = *num_faces_dev;
-  const int G = group_width(S, (int64_t)gridDim.x * (blockDim.x >> 5));
+  const int P = (F + 1) >> 1, rs = pair_stride(dim);
+  const int G = pair_group_width(group_width(S, (int64_t)gridDim.x * (blockDim.x >> 5)), P, kRegionKP);
   const int per = (S + gridDim.x - 1) / gridDim.x;
   const int first = blockIdx.x * per, last = min(S, first + per);
-  if (first >= last) return;
-  constexpr int rows8 = (int)(kStageBytes / (kRowStride<8> * sizeof(float)));
-  constexpr int rows16 = (int)(kStageBytes / (kRowStride<16> * sizeof(float)));
-  if (dim <= 8) {
-    if (F <= rows8) {
-      stage_rows<8>(At, ldt, b, F, dim, smf);
-      __syncthreads();
-      sample_range<8, 1, kLayRows>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out, G, smf, true);
-      return;
-    }
-    const bool staged = F <= kStageFaces8;
-    if (staged) stage_polytope<8, kStageFaces8>(At, ldt, b, F, dim, smf);
+  if (first >= last || G == 0) return;  // uniform across the block (the host bounds F)
+  const bool fits = (size_t)P * rs * sizeof(float) <= kRegionStageBytes;
+  if (fits) {
+    stage_pairs(rows, P, rs, smf);
     __syncthreads();
-    sample_range<8, 1>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out, G, smf, staged);
-  } else {
-    if (F <= rows16) {
-      stage_rows<16>(At, ldt, b, F, dim, smf);
-      __syncthreads();
-      sample_range<16, 1, kLayRows>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out, G, smf, true);
-      return;
-    }
-    const bool staged = F <= kStageFaces16;
-    if (staged) stage_polytope<16, kStageFaces16>(At, ldt, b, F, dim, smf);
-    __syncthreads();
-    sample_range<16, 1>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out, G, smf, staged);
   }
+  const float* src = fits ? smf : rows;
+  if (dim <= 8)
+    sample_region<8, kRegionKP>(G, src, P, dim, start, first, last, mixing, k0, k1, stream, out, gsa);
+  else
+    sample_region<16, kRegionKP>(G, src, P, dim, start, first, last, mixing, k0, k1, stream, out, gsa);
 }
 
-csd_status_t launch_hit_and_run_warp(const float* At, int ldt, const float* b, const int* num_faces_dev, int dim,
-                                     const float* start, int S, int mixing, uint64_t seed, uint32_t stream,
-                                     int fail_keep, float* out, cudaStream_t st) {
+csd_status_t launch_sample_region(const float* rows, const int* num_faces_dev, int dim, const float* start, int S,
+                                  int mixing, uint64_t seed, uint32_t stream, float* out, cudaStream_t st) {
   if (S <= 0) return CSD_OK;
   CSD_CHECK(dim >= 1 && dim <= kMaxDim, CSD_ERR_DIMENSION, "dimension must be in [1, 16]");
-  CSD_CHECK(fail_keep, CSD_ERR_INVALID, "the group sampler keeps the start point of failed chains");
   static bool attr_set[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 64 || !attr_set[dev]) {
-    CSD_CUDA_TRY(cudaFuncSetAttribute(hit_and_run_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kStageBytes));
+    CSD_CUDA_TRY(cudaFuncSetAttribute(sample_region_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kRegionStageBytes));
     if (dev < 64) attr_set[dev] = true;
   }
   const int sms = device_sm_count();
   const int blocks = (int)std::min<int64_t>(((int64_t)S + 7) / 8, (int64_t)sms * 2);
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-  hit_and_run_group_kernel<<<blocks, 256, kStageBytes, st>>>(At, ldt, b, num_faces_dev, dim, start, S, mixing, k0,
-                                                              k1, stream, out);
+  sample_region_kernel<<<blocks, 256, kRegionStageBytes, st>>>(rows, num_faces_dev, dim, start, S, mixing, k0, k1,
+                                                                stream, out);
   CSD_CUDA_TRY(cudaGetLastError());
   return CSD_OK;
 }
 
-// Transposes F rows of A (row-major, d columns) into At (At[k * ldt + f]).
-__global__ void transpose_faces_kernel(const float* __restrict__ A, int F, int d, float* __restrict__ At, int ldt) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < F * d; i += gridDim.x * blockDim.x)
-    At[(int64_t)(i % d) * ldt + i / d] = A[i];
+__global__ void put_faces_kernel(const float* __restrict__ A, const float* __restrict__ b, int F, int dim,
+                                 const float* __restrict__ x0, float* __restrict__ rows) {
+  put_faces(A, b, F, dim, x0, rows, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
-csd_status_t launch_transpose_faces(const float* A, int F, int d, float* At, int ldt, cudaStream_t st) {
+csd_status_t launch_put_faces(const float* A, const float* b, int F, int dim, const float* x0, float* rows,
+                              cudaStream_t st) {
   if (F <= 0) return CSD_OK;
-  const int blocks = std::min((F * d + 255) / 256, 1024);
-  transpose_faces_kernel<<<blocks, 256, 0, st>>>(A, F, d, At, ldt);
+  const int pairs = (F + 1) / 2;
+  put_faces_kernel<<<(pairs + 127) / 128, 128, 0, st>>>(A, b, F, dim, x0, rows);
   CSD_CUDA_TRY(cudaGetLastError());
   return CSD_OK;
 }

@@ -49,137 +49,6 @@ __device__ __forceinline__ bool run_chain(const float* __restrict__ Ap, const fl
   return true;
 }
 
-// The same chain run by a group of G lanes (G = 8, 16 or 32; 32 / G chains
-// per warp). Jobs 0..ceil(dim/2)-1 are the Gaussian pairs and job ceil(dim/2)
-// the theta uniform, each drawn from the Philox block and words the serial
-// step_draws uses; lane gl of the group draws jobs gl, gl + G, ... and the
-// direction is broadcast by shuffles. The group's lanes split the faces
-// f = gl, gl + G, ...: each face's slack and A dir are accumulated in the
-// serial order, and the theta bounds are max/min reductions, which do not
-// depend on the order, so every chain ends bit for bit where run_chain ends.
-// At is the face matrix transposed, At[k * stride + f], with the stride ST
-// when ST > 0 (a shared-memory copy) and ldt otherwise. ROWS: At is instead a
-// face-row copy (stage_rows: row f at At + f * ST, coordinates as float4
-// vectors, b_f at coordinate MAXD) and bp is unused. x is replicated in
-// the group's lanes. A chain whose line search fails keeps stepping without
-// moving (so the groups of a warp stay convergent for the shuffles) and
-// returns false.
-template <int MAXD, int G, int ST, int U = 1, bool ROWS = false>
-__device__ __forceinline__ bool run_chain_group(const float* __restrict__ At, int ldt, const float* __restrict__ bp,
-                                                int F, int dim, int mixing, uint32_t k0, uint32_t k1,
-                                                uint32_t chain, uint32_t stream, float* x, int gl) {
-  static_assert(!ROWS || (ST > 0 && ST % 4 == 0 && MAXD % 4 == 0 && ST > MAXD), "face rows: float4 rows with b");
-  constexpr int R = (MAXD / 2 + 1 + G - 1) / G;  // job rounds per lane
-  const int stride = ST > 0 ? ST : ldt;
-  const int npairs = (dim + 1) >> 1;
-  bool ok = true;
-  for (int step = 0; step < mixing; ++step) {
-    float c0[R], c1[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      c0[r] = 0.f;
-      c1[r] = 0.f;
-      const int job = gl + r * G;
-      if (job <= npairs) {
-        const int word = 2 * job;
-        uint32_t w[4];
-        philox4x32_10((uint32_t)step, chain, stream, (uint32_t)(word >> 2), k0, k1, w);
-        const uint32_t wa = (word & 2) ? w[2] : w[0];
-        const uint32_t wb = (word & 2) ? w[3] : w[1];
-        if (job < npairs) {
-          float u = u01_open0(wa);
-          float v = u01_open1(wb);
-          float rad = __fsqrt_rn(__fmul_rn(-2.0f, log_unit(u)));
-          float sn, cs;
-          sincos_2pi(v, &sn, &cs);
-          c0[r] = __fmul_rn(rad, cs);
-          c1[r] = __fmul_rn(rad, sn);
-        } else {
-          c0[r] = u01_open0(wa);
-        }
-      }
-    }
-    float dir[MAXD];
-#pragma unroll
-    for (int k = 0; k < MAXD; ++k) {
-      const int p = k >> 1;
-      dir[k] = __shfl_sync(0xffffffffu, (k & 1) ? c1[p / G] : c0[p / G], p % G, G);
-    }
-    float utv = c0[0];
-#pragma unroll
-    for (int r = 1; r < R; ++r)
-      if (npairs / G == r) utv = c0[r];
-    const float ut = __shfl_sync(0xffffffffu, utv, npairs % G, G);
-    float tmax = FLT_MAX, tmin = -FLT_MAX;
-    // U faces per lane and trip (independent dot products for the scheduler)
-    for (int f0 = gl; f0 < F; f0 += G * U) {
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int f = f0 + u * G;
-        if (U == 1 || f < F) {
-          float ax, ad, lb;
-          if constexpr (ROWS) {
-            // one 16-byte shared load per four coordinates
-            const float4* row = reinterpret_cast<const float4*>(At + f * ST);
-            float a[MAXD];
-#pragma unroll
-            for (int q = 0; q < MAXD / 4; ++q) {
-              const float4 v = row[q];
-              a[4 * q] = v.x;
-              a[4 * q + 1] = v.y;
-              a[4 * q + 2] = v.z;
-              a[4 * q + 3] = v.w;
-            }
-            ax = __fmul_rn(a[0], x[0]);
-            ad = __fmul_rn(a[0], dir[0]);
-#pragma unroll
-            for (int k = 1; k < MAXD; ++k) {
-              if (k < dim) {
-                ax = __fmaf_rn(a[k], x[k], ax);
-                ad = __fmaf_rn(a[k], dir[k], ad);
-              }
-            }
-            lb = __fsub_rn(At[f * ST + MAXD], ax);
-          } else {
-            const float* col = At + f;
-            float a0 = col[0];
-            ax = __fmul_rn(a0, x[0]);
-            ad = __fmul_rn(a0, dir[0]);
-#pragma unroll
-            for (int k = 1; k < MAXD; ++k) {
-              if (k < dim) {
-                float ak = col[k * stride];
-                ax = __fmaf_rn(ak, x[k], ax);
-                ad = __fmaf_rn(ak, dir[k], ad);
-              }
-            }
-            lb = __fsub_rn(bp[f], ax);
-          }
-          if (ad < 0.0f)
-            tmin = fmaxf(tmin, __fdiv_rn(lb, ad));
-          else if (ad > 0.0f)
-            tmax = fminf(tmax, __fdiv_rn(lb, ad));
-        }
-      }
-    }
-#pragma unroll
-    for (int o = G / 2; o; o >>= 1) {
-      tmin = fmaxf(tmin, __shfl_xor_sync(0xffffffffu, tmin, o, G));
-      tmax = fminf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o, G));
-    }
-    if (isinf(tmax) || isinf(tmin) || tmax < tmin) ok = false;
-    if (ok) {
-      double th = __dadd_rn(__dmul_rn((double)ut, __dsub_rn(__dmul_rn(0.999999, (double)tmax), (double)tmin)),
-                            (double)tmin);
-      float theta = __double2float_rn(th);
-#pragma unroll
-      for (int k = 0; k < MAXD; ++k)
-        if (k < dim) x[k] = __fmaf_rn(theta, dir[k], x[k]);
-    }
-  }
-  return ok;
-}
-
 // ---- packed FP32 pairs (sm_100 f32x2): each half is an IEEE round-to-nearest
 // operation, so a packed result is bit for bit the two scalar results.
 __device__ __forceinline__ uint64_t f2_pack(float lo, float hi) {
@@ -206,25 +75,116 @@ __device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
   return d;
 }
 
-// run_chain_group over a staged polytope (row stride ST, even; 8-byte aligned
-// rows) with faces taken in adjacent pairs (f, f + 1), f even: one 64-bit
-// shared-memory load brings coordinate k of both faces, and one packed FMA
-// per dot product advances both. The configuration and the direction are
-// kept duplicated in both halves ((x_k, x_k), (d_k, d_k)) so they pair with
-// any face pair. Per face the operations and their order are those of
-// run_chain_group (product, FMAs in coordinate order, b - A x, division), and
-// the theta bounds are order-independent reductions, so the chain ends bit
-// for bit where run_chain ends. U pairs per lane and trip.
-template <int MAXD, int G, int ST, int U>
-__device__ __forceinline__ bool run_chain_group_x2(const float* __restrict__ At, const float* __restrict__ bp, int F,
-                                                   int dim, int mixing, uint32_t k0, uint32_t k1, uint32_t chain,
-                                                   uint32_t stream, float* x, int gl) {
-  static_assert(ST > 0 && ST % 2 == 0, "packed faces need an even staged stride");
-  constexpr int R = (MAXD / 2 + 1 + G - 1) / G;
+// ---------------------------------------------------------------------------
+// EI-ZO sampling: hit-and-run with carried slacks over face pairs.
+//
+// Every chain of an EI-ZO iteration starts at the segment's start point x0,
+// so the slack b_f - a_f . x0 of a face at the start of a chain is common to
+// all chains. It is computed once, when the face is written (put_face), in the
+// serial chain's order (product of coordinate 0, fused multiply-adds in
+// coordinate order, then b minus that). A chain carries its slacks: after a
+// step of length theta along dir it updates s_f = fma(-theta, a_f . dir, s_f),
+// so a mixing step costs one dim-long dot product per face instead of two
+// (the reference recomputes b - A x every step,
+// csdecomp/src/planning/cuda_hit_and_run_sampling.cu:83-104). The theta
+// bounds, the theta draw (0.999999 scales theta_max only, :106-107) and the
+// position update are the serial chain's.
+//
+// Face-pair rows: row p holds faces 2p and 2p + 1 interleaved, coordinate k of
+// face 2p + h at float 2k + h (k < MAXD, zero past dim), the two start slacks
+// at 2 MAXD and 2 MAXD + 1, then two unused floats: 2 MAXD + 4 floats, a
+// multiple of 16 bytes. A face that does not exist yet (the partner of the
+// last face of an odd count) is a zero row: its a . dir is zero, so it bounds
+// nothing and its slack never changes. One 16-byte load brings two
+// coordinates of both faces, and one packed FMA (fma.rn.f32x2, each half an
+// IEEE round-to-nearest FMA) advances both faces' dot products.
+__host__ __device__ constexpr int pair_maxd(int dim) { return dim <= 8 ? 8 : 16; }
+__host__ __device__ constexpr int pair_stride(int dim) { return 2 * pair_maxd(dim) + 4; }
+
+// Writes face f (coordinates a[0..dim), offset b) of a region whose chains
+// start at x0. An even f also clears its partner half.
+__device__ __forceinline__ void put_face(float* __restrict__ rows, int dim, int f, const float* a, float b,
+                                         const float* __restrict__ x0) {
+  const int md = pair_maxd(dim), h = f & 1;
+  float* r = rows + (size_t)(f >> 1) * pair_stride(dim);
+  float ax = __fmul_rn(a[0], x0[0]);
+  for (int k = 1; k < dim; ++k) ax = __fmaf_rn(a[k], x0[k], ax);
+  for (int k = 0; k < md; ++k) r[2 * k + h] = k < dim ? a[k] : 0.f;
+  r[2 * md + h] = __fsub_rn(b, ax);
+  if (!h) {
+    for (int k = 0; k < md; ++k) r[2 * k + 1] = 0.f;
+    r[2 * md + 1] = 0.f;
+  }
+}
+
+// Pair rows of faces [0, F) of a row-major A (F x dim) and b; thread t of
+// nthreads writes whole pairs t, t + nthreads, ...
+__device__ __forceinline__ void put_faces(const float* __restrict__ A, const float* __restrict__ b, int F, int dim,
+                                          const float* __restrict__ x0, float* __restrict__ rows, int t,
+                                          int nthreads) {
+  for (int p = t; p < (F + 1) / 2; p += nthreads) {
+    put_face(rows, dim, 2 * p, A + (size_t)(2 * p) * dim, b[2 * p], x0);
+    if (2 * p + 1 < F) put_face(rows, dim, 2 * p + 1, A + (size_t)(2 * p + 1) * dim, b[2 * p + 1], x0);
+  }
+}
+
+// theta bounds of one face (slack s, a . dir = ad): the reference's rule.
+__device__ __forceinline__ void theta_bound(float s, float ad, float& tmin, float& tmax) {
+  if (ad < 0.0f)
+    tmin = fmaxf(tmin, __fdiv_rn(s, ad));
+  else if (ad > 0.0f)
+    tmax = fminf(tmax, __fdiv_rn(s, ad));
+}
+
+// Shared scratch of a group wider than a warp (G = 64, 128, 256 lanes): the
+// step's direction and theta uniform, and each warp's partial theta bounds,
+// double buffered by step parity (a warp cannot run two steps ahead of the
+// group's barriers).
+struct GroupScratch {
+  float dir[2][17];
+  float red[2][8][2];
+};
+constexpr int kMaxWideGroups = 4;  // 256 threads / 64 lanes
+
+__device__ __forceinline__ void group_bar(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// Lanes per chain: at least `g` (set by the chain count) and enough that
+// each lane holds at most KP face pairs; 0 if even 256 lanes do not.
+__host__ __device__ __forceinline__ int pair_group_width(int g, int P, int KP) {
+  while (g <= 256 && (long long)g * KP < P) g <<= 1;
+  return g <= 256 ? g : 0;
+}
+
+// One chain run by a group of G lanes over a region of P face pairs (staged in
+// shared memory or read from global memory). Lane gl holds pairs gl + G j
+// (j < KP) and their slacks and a . dir values in registers, and coordinates
+// gl + G r of the position (xl). The draws are the serial chain's: job j <
+// ceil(dim/2) is Gaussian pair j, job ceil(dim/2) the theta uniform, lane gl
+// drawing jobs gl, gl + G, ...; the direction is broadcast by shuffles (G <=
+// 32) or through GroupScratch (wider groups, named barrier bar_id). The theta
+// bounds are max/min reductions, which do not depend on the order, so every
+// chain ends bit for bit where the oracle's serial chain ends whatever G.
+// A chain whose line search fails keeps stepping without moving (the group's
+// lanes stay convergent) and returns false.
+template <int MAXD, int G, int KP>
+__device__ __forceinline__ bool run_chain_pairs(const float* __restrict__ rows, int P, int dim, int mixing,
+                                                uint32_t k0, uint32_t k1, uint32_t chain, uint32_t stream,
+                                                float* xl, int gl, GroupScratch* gs, int bar_id) {
+  constexpr int RS = 2 * MAXD + 4;
+  constexpr int R = (MAXD / 2 + 1 + G - 1) / G;  // job rounds per lane
+  constexpr int XL = (MAXD + G - 1) / G;         // position coordinates per lane
+  static_assert(G <= 32 || R == 1, "wide groups draw in their first warp");
   const int npairs = (dim + 1) >> 1;
-  uint64_t xx[MAXD];
+  uint64_t s2[KP], a2[KP];
 #pragma unroll
-  for (int k = 0; k < MAXD; ++k) xx[k] = f2_pack(x[k], x[k]);
+  for (int j = 0; j < KP; ++j) {
+    const int p = gl + G * j;
+    s2[j] = p < P ? *reinterpret_cast<const uint64_t*>(rows + (size_t)p * RS + 2 * MAXD) : 0ull;
+    a2[j] = 0ull;  // with nth = -0 the first update leaves every slack as it is
+  }
+  float nth = -0.0f;
   bool ok = true;
   for (int step = 0; step < mixing; ++step) {
     float c0[R], c1[R];
@@ -252,174 +212,177 @@ __device__ __forceinline__ bool run_chain_group_x2(const float* __restrict__ At,
         }
       }
     }
-    uint64_t dd[MAXD];
+    uint64_t dd[MAXD];  // (dir_k, dir_k)
+    float ut;
+    if constexpr (G <= 32) {
 #pragma unroll
-    for (int k = 0; k < MAXD; ++k) {
-      const int p = k >> 1;
-      const float dk = __shfl_sync(0xffffffffu, (k & 1) ? c1[p / G] : c0[p / G], p % G, G);
-      dd[k] = f2_pack(dk, dk);
+      for (int k = 0; k < MAXD; ++k) {
+        const int p = k >> 1;
+        const float dk = __shfl_sync(0xffffffffu, (k & 1) ? c1[p / G] : c0[p / G], p % G, G);
+        dd[k] = f2_pack(dk, dk);
+      }
+      float utv = c0[0];
+#pragma unroll
+      for (int r = 1; r < R; ++r)
+        if (npairs / G == r) utv = c0[r];
+      ut = __shfl_sync(0xffffffffu, utv, npairs % G, G);
+    } else {
+      float* db = gs->dir[step & 1];
+      if (gl < npairs) {
+        db[2 * gl] = c0[0];
+        db[2 * gl + 1] = c1[0];
+      } else if (gl == npairs) {
+        db[16] = c0[0];
+      }
+      group_bar(bar_id, G);
+#pragma unroll
+      for (int k = 0; k < MAXD; ++k) {
+        const float dk = db[k];  // entries past dim are never used
+        dd[k] = f2_pack(dk, dk);
+      }
+      ut = db[16];
     }
-    float utv = c0[0];
-#pragma unroll
-    for (int r = 1; r < R; ++r)
-      if (npairs / G == r) utv = c0[r];
-    const float ut = __shfl_sync(0xffffffffu, utv, npairs % G, G);
     float tmax = FLT_MAX, tmin = -FLT_MAX;
-    for (int f0 = 2 * gl; f0 < F; f0 += 2 * G * U) {
+    const uint64_t nth2 = f2_pack(nth, nth);
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int f = f0 + 2 * G * u;
-        if (U == 1 || f < F) {
-          const float* col = At + f;
-          uint64_t a = *reinterpret_cast<const uint64_t*>(col);
-          uint64_t ax = f2_mul(a, xx[0]);
-          uint64_t ad = f2_mul(a, dd[0]);
+    for (int j = 0; j < KP; ++j) {
+      const int p = gl + G * j;
+      if (p < P) {
+        const uint64_t s = f2_fma(nth2, a2[j], s2[j]);  // the previous step's slack update
+        s2[j] = s;
+        const ulonglong2* row = reinterpret_cast<const ulonglong2*>(rows + (size_t)p * RS);
+        uint64_t acc = 0ull;
 #pragma unroll
-          for (int k = 1; k < MAXD; ++k) {
-            if (k < dim) {
-              a = *reinterpret_cast<const uint64_t*>(col + k * ST);
-              ax = f2_fma(a, xx[k], ax);
-              ad = f2_fma(a, dd[k], ad);
-            }
-          }
-          const uint64_t lb2 = f2_sub(*reinterpret_cast<const uint64_t*>(bp + f), ax);
-          float lb0, lb1, ad0, ad1;
-          f2_unpack(lb2, &lb0, &lb1);
-          f2_unpack(ad, &ad0, &ad1);
-          if (ad0 < 0.0f)
-            tmin = fmaxf(tmin, __fdiv_rn(lb0, ad0));
-          else if (ad0 > 0.0f)
-            tmax = fminf(tmax, __fdiv_rn(lb0, ad0));
-          if (f + 1 < F) {  // the pair's second face (row entries past F are never used)
-            if (ad1 < 0.0f)
-              tmin = fmaxf(tmin, __fdiv_rn(lb1, ad1));
-            else if (ad1 > 0.0f)
-              tmax = fminf(tmax, __fdiv_rn(lb1, ad1));
+        for (int q = 0; q < MAXD / 2; ++q) {
+          if (2 * q < dim) {
+            const ulonglong2 v = row[q];  // coordinates 2q and 2q + 1 of both faces
+            acc = q == 0 ? f2_mul(v.x, dd[0]) : f2_fma(v.x, dd[2 * q], acc);
+            if (2 * q + 1 < dim) acc = f2_fma(v.y, dd[2 * q + 1], acc);
           }
         }
+        a2[j] = acc;
+        float sa, sb, aa, ab;
+        f2_unpack(s, &sa, &sb);
+        f2_unpack(acc, &aa, &ab);
+        theta_bound(sa, aa, tmin, tmax);
+        theta_bound(sb, ab, tmin, tmax);
       }
     }
+    if constexpr (G <= 32) {
 #pragma unroll
-    for (int o = G / 2; o; o >>= 1) {
-      tmin = fmaxf(tmin, __shfl_xor_sync(0xffffffffu, tmin, o, G));
-      tmax = fminf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o, G));
+      for (int o = G / 2; o; o >>= 1) {
+        tmin = fmaxf(tmin, __shfl_xor_sync(0xffffffffu, tmin, o, G));
+        tmax = fminf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o, G));
+      }
+    } else {
+#pragma unroll
+      for (int o = 16; o; o >>= 1) {
+        tmin = fmaxf(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
+        tmax = fminf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+      }
+      float(*red)[2] = gs->red[step & 1];
+      if ((gl & 31) == 0) {
+        red[gl >> 5][0] = tmin;
+        red[gl >> 5][1] = tmax;
+      }
+      group_bar(bar_id, G);
+      tmin = red[0][0];
+      tmax = red[0][1];
+#pragma unroll
+      for (int w = 1; w < G / 32; ++w) {
+        tmin = fmaxf(tmin, red[w][0]);
+        tmax = fminf(tmax, red[w][1]);
+      }
     }
     if (isinf(tmax) || isinf(tmin) || tmax < tmin) ok = false;
+    nth = -0.0f;
     if (ok) {
       double th = __dadd_rn(__dmul_rn((double)ut, __dsub_rn(__dmul_rn(0.999999, (double)tmax), (double)tmin)),
                             (double)tmin);
       const float theta = __double2float_rn(th);
-      const uint64_t tt = f2_pack(theta, theta);
 #pragma unroll
-      for (int k = 0; k < MAXD; ++k)
-        if (k < dim) xx[k] = f2_fma(tt, dd[k], xx[k]);
+      for (int r = 0; r < XL; ++r) {
+        const int k = gl + G * r;
+        float dk = 0.f, hi;
+#pragma unroll
+        for (int kk = 0; kk < MAXD; ++kk)
+          if (kk == k) f2_unpack(dd[kk], &dk, &hi);
+        if (k < dim) xl[r] = __fmaf_rn(theta, dk, xl[r]);
+      }
+      nth = -theta;
     }
-  }
-#pragma unroll
-  for (int k = 0; k < MAXD; ++k) {
-    float lo, hi;
-    f2_unpack(xx[k], &lo, &hi);
-    x[k] = lo;
   }
   return ok;
 }
 
-// Writes coordinates gl, gl + G, ... of a group-replicated vector.
-template <int MAXD, int G>
-__device__ __forceinline__ void group_store(const float* x, int dim, int gl, float* __restrict__ dst, bool ok,
-                                            const float* __restrict__ fallback) {
-#pragma unroll
-  for (int r = 0; r < (MAXD + G - 1) / G; ++r) {
-    const int k = gl + r * G;
-    float v = 0.f;
-#pragma unroll
-    for (int j = 0; j < MAXD; ++j)
-      if (j == k) v = x[j];
-    if (k < dim) dst[k] = ok ? v : fallback[k];
-  }
-}
-
-// Shared-memory staging of one polytope for the group sampler: rows
-// k < dim of At at stride ST, then b at row MAXD. Sized (MAXD + 1) * ST floats.
-constexpr int kStageFaces8 = 2048;   // faces staged for dim <= 8
-constexpr int kStageFaces16 = 1024;  // faces staged for dim <= 16
-constexpr size_t kStageBytes = 9 * kStageFaces8 * sizeof(float);
-static_assert(9 * kStageFaces8 >= 17 * kStageFaces16, "staging buffer");
-
-// Staging capacity of a kernel with MINB resident blocks per SM: the largest
-// buffer that MINB blocks fit in the SM's 227 KB (2 blocks: 3072 / 1536
-// faces, 3 blocks: 2048 / 1024, 4 blocks: 1536 / 768).
-// Face-row staging (stage_rows): row f holds a_f0 .. a_f(MAXD-1) (zero past
-// dim) and b_f at MAXD, kRowStride floats apart. The strides are multiples of
-// 16 bytes for the float4 loads, and 12 and 20 floats put the eight rows a
-// group reads at once in eight disjoint sets of four banks.
-template <int MAXD>
-constexpr int kRowStride = MAXD <= 8 ? 12 : 20;
-
-template <int MINB>
-struct StageCfg {
-  static constexpr int f8 = MINB <= 2 ? 3072 : MINB == 3 ? 2048 : 1536;
-  static constexpr int f16 = f8 / 2;
-  static constexpr size_t bytes = 9 * (size_t)f8 * sizeof(float);
-  // faces the same buffer holds as face rows
-  static constexpr int r8 = (int)(bytes / (kRowStride<8> * sizeof(float)));
-  static constexpr int r16 = (int)(bytes / (kRowStride<16> * sizeof(float)));
-  static_assert(9 * f8 >= 17 * f16, "staging buffer");
-  static_assert(MINB * bytes <= 227 * 1024, "MINB staging buffers fit one SM");
-};
-
-template <int MAXD, int ST>
-__device__ __forceinline__ void stage_polytope(const float* __restrict__ At, int ldt, const float* __restrict__ b,
-                                               int F, int dim, float* sm) {
-  for (int i = threadIdx.x; i < dim * F; i += blockDim.x) {
-    const int k = i / F, f = i - k * F;
-    sm[k * ST + f] = At[(int64_t)k * ldt + f];
-  }
-  for (int f = threadIdx.x; f < F; f += blockDim.x) sm[MAXD * ST + f] = b[f];
-}
-
-// Stages F faces of a transposed polytope (At[k * ldt + f], b[f]) as face
-// rows: F * kRowStride<MAXD> floats of sm (16-byte aligned).
-template <int MAXD>
-__device__ __forceinline__ void stage_rows(const float* __restrict__ At, int ldt, const float* __restrict__ b, int F,
-                                           int dim, float* sm) {
-  constexpr int RS = kRowStride<MAXD>;
-  for (int i = threadIdx.x; i < MAXD * F; i += blockDim.x) {
-    const int k = i / F, f = i - k * F;
-    sm[f * RS + k] = k < dim ? At[(int64_t)k * ldt + f] : 0.f;
-  }
-  for (int f = threadIdx.x; f < F; f += blockDim.x) sm[f * RS + MAXD] = b[f];
-}
-
-// Staged layouts of the group sampler: transposed columns, transposed columns
-// read in packed face pairs, face rows.
-enum : int { kLayStrided = 0, kLayPacked = 1, kLayRows = 2 };
-
-// Chains [first, last) of one polytope by the whole block, G lanes per
-// chain; the trip count is uniform across the block (groups past `last`
-// repeat the last chain and store nothing). A failed chain stores `start`.
-template <int MAXD, int G, int ST, int U, int LAY = kLayStrided>
-__device__ __forceinline__ void sample_chains(const float* __restrict__ At, int ldt, const float* __restrict__ b,
-                                              int F, int dim, const float* __restrict__ start, int first, int last,
-                                              int mixing, uint32_t k0, uint32_t k1, uint32_t stream,
-                                              float* __restrict__ out) {
-  const int lane = threadIdx.x & 31, gl = lane & (G - 1);
-  const int gid = (threadIdx.x >> 5) * (32 / G) + lane / G;
-  const int ngroups = (blockDim.x >> 5) * (32 / G);
+// Chains [first, last) of one region by the whole block (256 threads), G
+// lanes per chain; groups past `last` repeat the last chain and store
+// nothing, so every group takes the same number of trips (wide groups meet
+// at named barriers 1 + group index). A failed chain stores `start`.
+template <int MAXD, int G, int KP>
+__device__ __forceinline__ void sample_chains_pairs(const float* __restrict__ rows, int P, int dim,
+                                                    const float* __restrict__ start, int first, int last, int mixing,
+                                                    uint32_t k0, uint32_t k1, uint32_t stream,
+                                                    float* __restrict__ out, GroupScratch* gsa) {
+  constexpr int XL = (MAXD + G - 1) / G;
+  const int gl = threadIdx.x & (G - 1), gid = threadIdx.x / G, ngroups = blockDim.x / G;
+  GroupScratch* gs = G > 32 ? gsa + gid : nullptr;
   for (int c0 = first; c0 < last; c0 += ngroups) {
     const int chain = c0 + gid;
     const int cc = chain < last ? chain : last - 1;
-    float x[MAXD];
+    float xl[XL];
 #pragma unroll
-    for (int k = 0; k < MAXD; ++k) x[k] = k < dim ? start[k] : 0.f;
-    bool ok;
-    if constexpr (LAY == kLayPacked && ST > 0)
-      ok = run_chain_group_x2<MAXD, G, ST, U>(At, b, F, dim, mixing, k0, k1, (uint32_t)cc, stream, x, gl);
-    else
-      ok = run_chain_group<MAXD, G, ST, U, LAY == kLayRows>(At, ldt, b, F, dim, mixing, k0, k1, (uint32_t)cc, stream,
-                                                           x, gl);
-    if (chain < last) group_store<MAXD, G>(x, dim, gl, out + (int64_t)chain * dim, ok, start);
+    for (int r = 0; r < XL; ++r) {
+      const int k = gl + G * r;
+      xl[r] = k < dim ? start[k] : 0.f;
+    }
+    const bool ok = run_chain_pairs<MAXD, G, KP>(rows, P, dim, mixing, k0, k1, (uint32_t)cc, stream, xl, gl, gs,
+                                                 1 + gid);
+    if (chain < last) {
+#pragma unroll
+      for (int r = 0; r < XL; ++r) {
+        const int k = gl + G * r;
+        if (k < dim) out[(int64_t)chain * dim + k] = ok ? xl[r] : start[k];
+      }
+    }
   }
+}
+
+// The chains of one region with G lanes each (G from pair_group_width, one of
+// 8 .. 256).
+template <int MAXD, int KP>
+__device__ __forceinline__ void sample_region(int G, const float* __restrict__ rows, int P, int dim,
+                                              const float* __restrict__ start, int first, int last, int mixing,
+                                              uint32_t k0, uint32_t k1, uint32_t stream, float* __restrict__ out,
+                                              GroupScratch* gsa) {
+  switch (G) {
+    case 8:
+      sample_chains_pairs<MAXD, 8, KP>(rows, P, dim, start, first, last, mixing, k0, k1, stream, out, gsa);
+      break;
+    case 16:
+      sample_chains_pairs<MAXD, 16, KP>(rows, P, dim, start, first, last, mixing, k0, k1, stream, out, gsa);
+      break;
+    case 32:
+      sample_chains_pairs<MAXD, 32, KP>(rows, P, dim, start, first, last, mixing, k0, k1, stream, out, gsa);
+      break;
+    case 64:
+      sample_chains_pairs<MAXD, 64, KP>(rows, P, dim, start, first, last, mixing, k0, k1, stream, out, gsa);
+      break;
+    case 128:
+      sample_chains_pairs<MAXD, 128, KP>(rows, P, dim, start, first, last, mixing, k0, k1, stream, out, gsa);
+      break;
+    default:
+      sample_chains_pairs<MAXD, 256, KP>(rows, P, dim, start, first, last, mixing, k0, k1, stream, out, gsa);
+      break;
+  }
+}
+
+// Copies P pair rows (stride floats each, 16-byte multiples) to shared memory.
+__device__ __forceinline__ void stage_pairs(const float* __restrict__ rows, int P, int stride, float* sm) {
+  const float4* src = reinterpret_cast<const float4*>(rows);
+  float4* dst = reinterpret_cast<float4*>(sm);
+  const int n = P * stride / 4;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
 }
 
 // Group width for `total` chains over `grid_warps` resident warps: 8 lanes
@@ -427,35 +390,6 @@ __device__ __forceinline__ void sample_chains(const float* __restrict__ At, int 
 // groups when there are few (the tail of an inflation).
 __host__ __device__ __forceinline__ int group_width(int64_t total, int64_t grid_warps) {
   return total >= 8 * grid_warps ? 8 : total >= 4 * grid_warps ? 16 : 32;
-}
-
-// One polytope's chains [first, last) read from `sm` when `staged` (the caller
-// staged it: by stage_rows for LAY == kLayRows, else by stage_polytope with
-// strides ST8 / ST16), else from global memory.
-// kLayPacked: the staged path takes faces in packed pairs (U pairs per trip).
-template <int MAXD, int U, int LAY = kLayStrided, int ST8 = kStageFaces8, int ST16 = kStageFaces16>
-__device__ __forceinline__ void sample_range(const float* __restrict__ At, int ldt, const float* __restrict__ b,
-                                             int F, int dim, const float* __restrict__ start, int first, int last,
-                                             int mixing, uint32_t k0, uint32_t k1, uint32_t stream,
-                                             float* __restrict__ out, int G, float* sm, bool staged) {
-  constexpr int ST = LAY == kLayRows ? kRowStride<MAXD> : MAXD <= 8 ? ST8 : ST16;
-  if (staged) {
-    const float* sAt = sm;
-    const float* sb = LAY == kLayRows ? nullptr : sm + MAXD * ST;
-    if (G == 8)
-      sample_chains<MAXD, 8, ST, U, LAY>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
-    else if (G == 16)
-      sample_chains<MAXD, 16, ST, U, LAY>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
-    else
-      sample_chains<MAXD, 32, ST, U, LAY>(sAt, ST, sb, F, dim, start, first, last, mixing, k0, k1, stream, out);
-  } else {
-    if (G == 8)
-      sample_chains<MAXD, 8, 0, U>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out);
-    else if (G == 16)
-      sample_chains<MAXD, 16, 0, U>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out);
-    else
-      sample_chains<MAXD, 32, 0, U>(At, ldt, b, F, dim, start, first, last, mixing, k0, k1, stream, out);
-  }
 }
 
 }  // namespace csd

@@ -301,17 +301,13 @@ csd_status_t csd_batch_configs_checked(csd_batch_t h, int32_t n, int64_t* config
 csd_status_t csd_batch_set_profiling(csd_batch_t h, int32_t enable);
 csd_status_t csd_batch_stage_ms(csd_batch_t h, float* stage_ms /* [8] */);
 /* Autotuner: during the first `iterations` iterations of the next
- * csd_batch_inflate, every sampler variant (faces per lane and trip x
- * resident blocks per SM: [1x2, 2x2, 1x3, 2x3, 4x2, 4x3], then packed face
- * pairs (two faces per 64-bit load and per f32x2 FMA) per lane and trip x
- * blocks per SM: [1x2, 2x2, 1x3, 2x3], then unpacked [1x4, 2x4], then face
- * rows (a face's coordinates and b in one row, read as 16-byte vectors)
- * [1x3, 2x3, 1x4, 1x2]) and every check work-item cap ([32, 128, 512]
- * configurations) is timed on that iteration's own inputs; the fastest of
- * each is kept for the graph and later calls. All variants give identical
- * samples. csd_batch_tuning reports the choice and the summed time of each
- * variant (variant_ms: 16 sampler entries, then 3 check entries;
- * *num_variants = 19). */
+ * csd_batch_inflate, every sampler variant (face pairs a lane holds at most x
+ * resident blocks per SM: [8x1, 8x2, 8x3, 16x1, 16x2]) and every check
+ * work-item cap ([32, 128, 512] configurations) is timed on that iteration's
+ * own inputs; the fastest of each is kept for the graph and later calls. All
+ * variants give identical samples. csd_batch_tuning reports the choice and
+ * the summed time of each variant (variant_ms: 5 sampler entries, then 3 check
+ * entries; *num_variants = 8). */
 csd_status_t csd_batch_autotune(csd_batch_t h, int32_t iterations);
 /* Surrogate-guided checking (mlp: one net per plant of the batch, same
  * dimensions; NULL turns it off). Each iteration then scores every sample
@@ -322,7 +318,10 @@ csd_status_t csd_batch_autotune(csd_batch_t h, int32_t iterations);
  * stop_probability. Every verdict used is the exact checker's; the
  * admissibility test (first M samples) is unchanged; the bisected particles
  * are the first num_particles collisions found, in sample order (the plain
- * form's particles whenever no colliding sample was left unchecked). */
+ * form's particles whenever no colliding sample was left unchecked). A slot
+ * whose ordered check left fewer than 1/8 of its samples unchecked checks in
+ * sample order (every sample, no scoring) for the rest of the call; once no
+ * active slot orders, the call continues with the batched form's graph. */
 csd_status_t csd_batch_set_surrogate(csd_batch_t h, csd_mlp_t mlp, float stop_probability);
 /* Round schedule of the surrogate-guided check: round r covers sorted
  * positions up to first_round * (2^(r+1) - 1), the last round the rest
@@ -332,16 +331,16 @@ csd_status_t csd_batch_set_surrogate_rounds(csd_batch_t h, int32_t rounds, int32
  * sampler variant index as above, check work-item cap a multiple of 8. The
  * set variant then runs for every iteration. */
 csd_status_t csd_batch_set_shapes(csd_batch_t h, int32_t sample_variant, int32_t check_item_cap);
-/* Each sampler variant stages a slot's region in shared memory up to a face
- * count set by its blocks per SM and layout (2: 3072 faces for dim <= 8, 1536
- * above, as face rows 2304 / 1382; 3: 2048 / 1024, rows 1536 / 921; 4:
- * 1536 / 768, rows 1152 / 691); larger regions are read from L2. After
- * tuning, once an active slot outgrows the running variant's staging, the
- * iterations continue with the fastest variant (by tuning time) that stages
- * the largest active region, else the roomiest (the graph is captured once
- * more per switch). tuned / large / last_run: the tuned variant, the one the
- * last switch chose for large regions (before any switch: the one it would
- * choose), the one the last iteration ran. */
+/* Each sampler variant stages a slot's region (face-pair rows) in shared
+ * memory up to a face count set by its blocks per SM (1: 5120 faces for dim
+ * <= 8, 2844 above; 2: 2662 / 1478; 3: 1740 / 966); larger regions are read
+ * from global memory through L1. After tuning, once an active slot outgrows
+ * the running variant's staging, the iterations continue with the fastest
+ * variant (by tuning time) that stages the largest active region, else the
+ * roomiest (the graph is captured once more per switch). tuned / large /
+ * last_run: the tuned variant, the one the last switch chose for large
+ * regions (before any switch: the one it would choose), the one the last
+ * iteration ran. */
 csd_status_t csd_batch_sample_variants(csd_batch_t h, int32_t* tuned, int32_t* large, int32_t* last_run);
 /* Number of sampler variants and of check work-item caps the autotuner
  * chooses from (the index ranges of csd_batch_set_shapes and the entries of
@@ -355,9 +354,14 @@ csd_status_t csd_batch_tuning(csd_batch_t h, int32_t* sample_variant, int32_t* c
 csd_status_t csd_batch_iteration_profile(csd_batch_t h, int32_t cap, float* stage_ms, int32_t* active,
                                          int32_t* count);
 /* Profiling mode, last csd_batch_inflate: algorithmic FLOPs of the sampling
- * stage, 4 d F per chain and mixing step (two length-d dot products per face,
- * FMA = 2), summed over the active slots' N_k chains of every iteration. */
+ * stage, (2 d + 4) F per chain and mixing step (a . dir, the slack update and
+ * the two theta-bound compares per face; FMA = 2, division not counted),
+ * summed over the active slots' N_k chains of every iteration. */
 csd_status_t csd_batch_sample_flops(csd_batch_t h, double* flops);
+/* Kernels the last csd_batch_inflate launched (graph nodes counted per
+ * replay, plus the autotuner's and the profiling mode's launches). No
+ * reference counterpart. */
+csd_status_t csd_batch_last_launches(csd_batch_t h, int64_t* launches);
 
 csd_status_t csd_batch_destroy(csd_batch_t batch);
 

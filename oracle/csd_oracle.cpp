@@ -837,6 +837,47 @@ bool run_chain(const float* A, const float* b, int F, int d, const float* x0, in
   return true;
 }
 
+// One EI-ZO chain with carried slacks (the GPU's EI-ZO sampler,
+// csdecomp_b200/csrc/sampler_core.cuh run_chain_pairs): the start slacks
+// s_f = b_f - a_f . x0 (product of coordinate 0, fmaf in coordinate order,
+// then b minus that); per step one dot product a_f . dir per face (same
+// order), the theta bounds of cuda_hit_and_run_sampling.cu:83-104 from
+// s_f / (a_f . dir), theta as in :106-107, then x_k = fmaf(theta, dir_k, x_k)
+// and s_f = fmaf(-theta, a_f . dir, s_f). The reference recomputes b - A x
+// every step instead; the draws, the bounds and theta are its. s and ad are
+// F floats of scratch.
+bool run_chain_carried(const float* A, const float* b, int F, int d, const float* x0, int mixing, uint64_t seed,
+                       uint32_t chain, uint32_t stream, float* x, float* s, float* ad) {
+  for (int i = 0; i < d; ++i) x[i] = x0[i];
+  for (int f = 0; f < F; ++f) {
+    const float* a = A + (int64_t)f * d;
+    float ax = a[0] * x0[0];
+    for (int k = 1; k < d; ++k) ax = std::fmaf(a[k], x0[k], ax);
+    s[f] = b[f] - ax;
+  }
+  float dir[16];
+  for (int st = 0; st < mixing; ++st) {
+    float ut;
+    step_draws(seed, chain, stream, (uint32_t)st, d, dir, &ut);
+    float tmax = FLT_MAX, tmin = -FLT_MAX;
+    for (int f = 0; f < F; ++f) {
+      const float* a = A + (int64_t)f * d;
+      float v = a[0] * dir[0];
+      for (int k = 1; k < d; ++k) v = std::fmaf(a[k], dir[k], v);
+      ad[f] = v;
+      if (v < 0.0f)
+        tmin = std::max(tmin, s[f] / v);
+      else if (v > 0.0f)
+        tmax = std::min(tmax, s[f] / v);
+    }
+    if (std::isinf(tmax) || std::isinf(tmin) || tmax < tmin) return false;
+    float theta = (float)((double)ut * (0.999999 * (double)tmax - (double)tmin) + (double)tmin);
+    for (int k = 0; k < d; ++k) x[k] = std::fmaf(theta, dir[k], x[k]);
+    for (int f = 0; f < F; ++f) s[f] = std::fmaf(-theta, ad[f], s[f]);
+  }
+  return true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -885,7 +926,8 @@ uint32_t orc_num_samples_unadaptive(float epsilon, float delta, float tau) {
 
 // EI-ZO: executeEizo, cuda_edge_inflation_zero_order.cu:109-338, with the
 // collision compaction of cuda_set_builder_utils.cu:168-186 made
-// deterministic (first colliding samples in index order).
+// deterministic (first colliding samples in index order) and the sampler's
+// slacks carried from step to step (run_chain_carried).
 int orc_eizo(const orc_plant_t* p, const float* ls, const float* le, const float* voxels,
              int32_t nv, float vr, const int32_t* rids, int32_t nr, const orc_eizo_options_t* o,
              float* A, float* b, int32_t* num_faces, int32_t capacity, orc_checker_fn checker,
@@ -907,13 +949,18 @@ int orc_eizo(const orc_plant_t* p, const float* ls, const float* le, const float
     uint32_t M = orc_num_samples_unadaptive(o->epsilon, delta_k, o->tau);
     uint32_t N = std::max(M, o->num_particles);
     samples.assign((size_t)N * d, 0.f);
-    int nf = 0;
-    orc_hit_and_run(A, b, F, d, ls, (int32_t)N, (int32_t)o->mixing_steps, o->seed, 0u,
-                    samples.data(), &nf, nthreads);
     // chains that fail keep their start point (inside the region)
-    for (uint32_t s = 0; s < N; ++s)
-      if (std::isnan(samples[(size_t)s * d]))
-        for (int k = 0; k < d; ++k) samples[(size_t)s * d + k] = ls[k];
+#pragma omp parallel
+    {
+      std::vector<float> sl(F), adv(F);
+#pragma omp for schedule(static)
+      for (int64_t c = 0; c < (int64_t)N; ++c) {
+        float x[16];
+        const bool ok = run_chain_carried(A, b, F, d, ls, (int)o->mixing_steps, o->seed, (uint32_t)c, 0u, x,
+                                          sl.data(), adv.data());
+        for (int k = 0; k < d; ++k) samples[(size_t)c * d + k] = ok ? x[k] : ls[k];
+      }
+    }
     flags.assign(N, 0);
     if (check(samples.data(), N, flags.data())) return -3;
     uint32_t total = 0, first_m = 0;

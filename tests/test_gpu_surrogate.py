@@ -148,3 +148,28 @@ def test_ranked_edges_bad_arguments():
         csd.CheckEdgesCollisionFreeRankedCuda(q0.T, q1.T, S7.plant, bank, 0, top=33)
     with pytest.raises(ValueError):
         csd.CheckEdgesCollisionFreeRankedCuda(q0.T, q1.T, S7.plant, bank, 5)
+
+
+def test_surrogate_turns_itself_off_where_ordering_cannot_save():
+    """With num_particles = N_0 = 4000 and stop probability 0, the first
+    iteration of a slot checks every sample (it cannot hold num_particles
+    collisions before its last sample), so ordering saves nothing: each slot
+    checks in sample order from its second iteration on and the call
+    continues with the batched form's graph (6 kernels per iteration instead
+    of 13). The regions equal the batched form's: no colliding sample was
+    left unchecked."""
+    bank, _, _ = trained_bank(epochs=2)
+    opt = csd.EizoOptions(num_particles=4000, mixing_steps=20, max_iterations=12)
+    plain, cfg_plain, slots, starts, ends = run(None, opt)
+    b = csd.BatchedEdgeInflator([S7.plant, S14.plant], opt, max_slots=6, face_capacity=400, autotune_iterations=0)
+    b.set_surrogate(bank, 0.0)
+    surr = b.inflate(slots, starts, ends, [DOMS[p] for p in slots])
+    for P, R in zip(surr, plain):
+        np.testing.assert_array_equal(P.A(), R.A())
+        np.testing.assert_array_equal(P.b(), R.b())
+    np.testing.assert_array_equal(b.last_configs_checked, cfg_plain)
+    iters = int(b.last_iterations.max())
+    assert iters >= 2
+    # init kernel + one surrogate iteration (sample, score, sort, 3 x (check, tally), compaction,
+    # bisect, faces, step) + batched iterations (sample, check, compaction, bisect, faces, step)
+    assert b.last_kernel_launches == 1 + 13 + 6 * (iters - 1)
