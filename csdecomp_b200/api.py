@@ -378,6 +378,9 @@ class EizoIterationInfo:
     num_collisions_updated: int = 0
     num_faces_placed: int = 0
     iteration_time_ms: float = 0.0
+    # dim x K collision points after bisection (cuda_edge_inflation_zero_order.h:46); kept, as the
+    # reference keeps them, only with track_iteration_information and dim <= 3, else empty
+    points_post_bisection: np.ndarray = field(default_factory=lambda: np.zeros((0, 0), np.float32))
 
 
 @dataclass
@@ -446,6 +449,15 @@ class CudaEdgeInflator:
                                              len(self._iters), ctypes.byref(nit), None))
         info = EizoInfo([EizoIterationInfo(*[getattr(self._iters[i], n) for n, _ in C.EizoIterC._fields_])
                          for i in range(nit.value)])
+        if d <= 3 and self._options.track_iteration_information:
+            for i, it in enumerate(info.iteration_info):
+                cnt = ctypes.c_int32(0)
+                C.check(C.lib().csd_inflator_points_post_bisection(self._handle, i, None, 0, ctypes.byref(cnt)))
+                if cnt.value:
+                    pts = np.zeros((cnt.value, d), np.float32)
+                    C.check(C.lib().csd_inflator_points_post_bisection(self._handle, i, C.ptr(pts), cnt.value,
+                                                                       ctypes.byref(cnt)))
+                    it.points_post_bisection = np.ascontiguousarray(pts.T)
         self.last_info = info
         if verbose:
             print("======================== Set builder ===========================")

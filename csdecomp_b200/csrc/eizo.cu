@@ -88,6 +88,9 @@ struct csd_inflator_s {
   csd::DevBuf A, rows, b, nf, samples, flags, cols, proj, dist, seg, vox, vtab, vgrid, cnt;
   csd::EizoCounters* host_cnt = nullptr;  // pinned
   int* host_nf = nullptr;                 // pinned
+  // last inflate, track_iteration_information and dim <= 3: the collision points after
+  // bisection of each iteration that placed faces ([K][dim] each), for plotting
+  std::vector<std::vector<float>> points_post_bisection;
   ~csd_inflator_s() {
     if (host_cnt) cudaFreeHost(host_cnt);
     if (host_nf) cudaFreeHost(host_nf);
@@ -246,6 +249,8 @@ csd_status_t csd_inflator_inflate(csd_inflator_t h, const float* ls, const float
   }
   const VoxArgs va = vox_args(vt);
   EizoCounters* cnt = h->cnt.as<EizoCounters>();
+  const bool keep_points = o.track_iteration_information && d <= 3;
+  h->points_post_bisection.clear();
   int nit = 0;
   int last_with_faces = -1;
   auto t_prev = std::chrono::high_resolution_clock::now();
@@ -291,6 +296,12 @@ csd_status_t csd_inflator_inflate(csd_inflator_t h, const float* ls, const float
     if ((s = launch_bisect(p, (int)K, d, (int)o.bisection_steps, ls_d, le_d, va, h->cols.as<float>(),
                            h->proj.as<float>(), h->dist.as<float>(), st)))
       return s;
+    if (keep_points) {  // as executeEizo keeps them for dim <= 3 (cuda_edge_inflation_zero_order.cu:323-335)
+      h->points_post_bisection.resize(nit + 1);
+      std::vector<float>& pts = h->points_post_bisection[nit];
+      pts.resize((size_t)K * d);
+      CSD_CUDA_TRY(cudaMemcpyAsync(pts.data(), h->cols.ptr, pts.size() * 4, cudaMemcpyDeviceToHost, st));
+    }
     faces_kernel<<<1, 1024, 0, st>>>((int)K, d, (int)o.max_hyperplanes_per_iteration, h->capacity,
                                      o.configuration_margin, ls_d, le_d, h->cols.as<float>(), h->proj.as<float>(),
                                      h->dist.as<float>(), h->A.as<float>(), h->b.as<float>(), h->nf.as<int>(), cnt,
@@ -320,6 +331,18 @@ csd_status_t csd_inflator_inflate(csd_inflator_t h, const float* ls, const float
   if ((s = plant_status(p, st))) return s;
   *num_faces = F;
   if (num_iters) *num_iters = nit;
+  return CSD_OK;
+}
+
+csd_status_t csd_inflator_points_post_bisection(csd_inflator_t h, int32_t iteration, float* points, int32_t capacity,
+                                               int32_t* count) {
+  CSD_CHECK(h && count && iteration >= 0 && (capacity == 0 || points), CSD_ERR_INVALID, "bad arguments");
+  *count = 0;
+  if (iteration >= (int32_t)h->points_post_bisection.size()) return CSD_OK;
+  const std::vector<float>& pts = h->points_post_bisection[iteration];
+  *count = (int32_t)(pts.size() / h->dim);
+  const size_t n = std::min<size_t>(pts.size(), (size_t)capacity * h->dim);
+  if (n) std::memcpy(points, pts.data(), n * 4);
   return CSD_OK;
 }
 

@@ -1,39 +1,39 @@
 """Small, reproducible launches of the hot kernels for profiler captures.
 
-  python -m csdecomp_b200.profile_cases check_points [--configs N] [--no-cull]
+  python profile_cases.py check_points [--configs N] [--no-cull]
       one warm-up and one timed check_points launch on N collision-free
       configurations of the 7-DOF arm (80 spheres + 4 capsules) in 200 world
       primitives (with --no-cull every pair is evaluated: the full sweep)
-  python -m csdecomp_b200.profile_cases batch [--slots S] [--iterations I]
+  python profile_cases.py batch [--slots S] [--iterations I]
       [--sample-variant V] [--check-item-cap C] [--per-iteration]
       S inflations of the batched EI-ZO workload (first S scenes), at most I
       iterations, launched stage by stage (profiling mode) with the given
       sampler variant and check work-item cap (defaults: the shapes the
       autotuner picks on a B200)
 
-  python -m csdecomp_b200.profile_cases point_check [--configs N]
+  python profile_cases.py point_check [--configs N]
       config 1: 7-DOF arm, 40 spheres, 20 world boxes; N uniform configurations
-  python -m csdecomp_b200.profile_cases edge_check [--edges E]
+  python profile_cases.py edge_check [--edges E]
       config 2: 7-DOF arm, 80 spheres + 4 capsules, 200 world primitives; E
       segments with endpoints uniform in the joint limits, 0.01 rad step
-  python -m csdecomp_b200.profile_cases eizo_single [--regions R]
+  python profile_cases.py eizo_single [--regions R]
       config 3: R single inflations (CudaEdgeInflator) on the 7-DOF /
       200-primitive scene, seed edges U[0.1, 0.5] rad
 
-  python -m csdecomp_b200.profile_cases visibility_graph [--nodes n]
+  python profile_cases.py visibility_graph [--nodes n]
       VisibilityGraph over n free configurations of the config-3 scene, 0.01 rad
       step (n (n - 1) / 2 edges checked on the device)
-  python -m csdecomp_b200.profile_cases voxel_check [--configs N] [--voxels V]
+  python profile_cases.py voxel_check [--configs N] [--voxels V]
       checkCollisionFreeVoxelsCuda at scale: the config-2 arm (80 spheres + 4
       capsules, 200 world primitives) against V voxels of radius 0.02 m
       (uniform in a 3 x 3 x 1.5 m box around the arm, none within 0.9 m of its
       base, so that verdicts are mixed), N uniform configurations; with and
       without the voxel hash grid
-  python -m csdecomp_b200.profile_cases edge_check_ranked [--edges E]
+  python profile_cases.py edge_check_ranked [--edges E]
       config-2 arm with a 0.8 m keep-out (mixed verdicts): E edges from free
       starts, lengths U[0.05, 1.0] rad; unranked checks against checks ranked
       by a surrogate trained on 65,536 labelled configurations of the scene
-  python -m csdecomp_b200.profile_cases edit_regions [--regions R] [--collisions C]
+  python profile_cases.py edit_regions [--regions R] [--collisions C]
       EditRegionsCuda on the config-3 scene: R box regions around seed edges,
       C colliding configurations drawn inside each, 9 bisection steps
 
@@ -44,8 +44,12 @@ from __future__ import annotations
 import argparse
 import ctypes
 import json
+import os
+import sys
 
 import numpy as np
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
 
 def check_points(n: int, cull: bool = True) -> None:
@@ -329,7 +333,7 @@ def main() -> None:
     ap.add_argument("--collisions", type=int, default=512, help="edit_regions: collisions per region")
     ap.add_argument("--voxels", type=int, default=10000, help="voxel_check: voxels")
     ap.add_argument("--iterations", type=int, default=12)
-    ap.add_argument("--sample-variant", type=int, default=3)
+    ap.add_argument("--sample-variant", type=int, default=1)  # index into BatchedEdgeInflator.SAMPLE_VARIANTS
     ap.add_argument("--check-item-cap", type=int, default=128)
     ap.add_argument("--per-iteration", action="store_true", help="batch: stage times and active slots per iteration")
     a = ap.parse_args()

@@ -5,6 +5,10 @@ available; the fixtures are committed so tests never read it):
     python tests/golden/make_golden.py /root/reference
 
 Outputs
+  ref_assets/  the reference's test models as loader fixtures: every
+               csdecomp/tests/test_assets/*.urdf and directives/*.yml, copied
+               as they are (text only; the meshes they name are not copied,
+               the loaders read no meshes)
   plants.npz   plant tables of the reference test robots, parsed from
                csdecomp/tests/test_assets/*.urdf, directives/kinova_sens_on_table.yml
                and the inline URDF of edge_inflation_zero_order_test.cpp:72-115
@@ -17,6 +21,7 @@ from __future__ import annotations
 import json
 import os
 import re
+import shutil
 import sys
 
 import numpy as np
@@ -55,8 +60,19 @@ def dump_plant(out: dict, name: str, parser: URDFParser) -> None:
     out[f"{name}/link_names"] = np.array([n for n, _ in names])
 
 
+def copy_assets(assets: str) -> None:
+    dst = os.path.join(HERE, "ref_assets")
+    os.makedirs(os.path.join(dst, "directives"), exist_ok=True)
+    for sub, ext in (("", ".urdf"), ("directives", ".yml")):
+        src = os.path.join(assets, sub)
+        for f in sorted(os.listdir(src)):
+            if f.endswith(ext):
+                shutil.copyfile(os.path.join(src, f), os.path.join(dst, sub, f))
+
+
 def main(ref: str) -> None:
     assets = os.path.join(ref, "csdecomp", "tests", "test_assets")
+    copy_assets(assets)
     out: dict = {}
     for name in ("2_branch_5dof", "3dofrobot", "3dofrobot_prismatic", "3dofrobot_spheres", "movable_block"):
         p = URDFParser()
@@ -177,4 +193,6 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: make_golden.py <root of the reference source tree>")
+    main(sys.argv[1])

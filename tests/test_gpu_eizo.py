@@ -135,3 +135,25 @@ def test_inflator_is_deterministic_and_reusable(plants):
     c = inf.inflateEdge([0, 0], [1, 0], None, 0.01, verbose=False)
     np.testing.assert_array_equal(a.A(), c.A())
     assert not np.array_equal(a.A(), b.A()) or a.A().shape != b.A().shape
+
+
+def test_points_post_bisection_2d(plants):
+    """EizoIterationInfo.points_post_bisection (kept for dim <= 3 with
+    track_iteration_information, as the reference does): dim x K points,
+    K = num_collisions_updated, every one in collision."""
+    gp = plants["boxes_in_corners"]
+    opt = csd.EizoOptions(num_particles=500, track_iteration_information=True)
+    inf = csd.CudaEdgeInflator(gp.plant, gp.robot_geometry_ids, opt, domain_of(gp))
+    inf.inflateEdge([-0.5, 0.0], [0.0, 0.5], None, 0.01, verbose=False)
+    its = inf.last_info.iteration_info
+    placed = [it for it in its if it.num_collisions_updated > 0]
+    assert placed
+    for it in placed:
+        pts = it.points_post_bisection
+        assert pts.shape == (2, it.num_collisions_updated)
+        assert not csd.CheckCollisionFreeCuda(pts, gp.plant).any()
+    assert its[-1].points_post_bisection.size == 0 or its[-1].num_collisions_updated > 0
+    opt.track_iteration_information = False
+    inf = csd.CudaEdgeInflator(gp.plant, gp.robot_geometry_ids, opt, domain_of(gp))
+    inf.inflateEdge([-0.5, 0.0], [0.0, 0.5], None, 0.01, verbose=False)
+    assert all(it.points_post_bisection.size == 0 for it in inf.last_info.iteration_info)

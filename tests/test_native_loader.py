@@ -2,8 +2,9 @@
 C++ callers) against the Python loader, whose tables the golden fixtures pin:
 identical MinimalPlant tables, robot geometry ids, limits and geometry names
 on generated URDFs, on the directives fixture in tests/golden/loader, and on
-the reference's own test assets when that tree is present; the same errors on
-malformed models. No GPU is used."""
+the reference's own test models (tests/golden/ref_assets, copied there by
+tests/golden/make_golden.py); the same errors on malformed models. No GPU is
+used."""
 import os
 
 import numpy as np
@@ -14,7 +15,7 @@ from csdecomp_b200.plant import URDFParser
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LOADER = os.path.join(HERE, "golden", "loader")
-REF_ASSETS = "/root/reference/csdecomp/tests/test_assets"
+REF_ASSETS = os.path.join(HERE, "golden", "ref_assets")  # the reference's test models (make_golden.py)
 
 
 def assert_same(py: URDFParser, nat: C.NativeURDFParser):
@@ -98,7 +99,6 @@ def test_directives_fixture():
     assert nat.geometry_index("arm::elbow & pad::2") == 2  # entity decoded, collision counter per link
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_ASSETS), reason="reference test assets not present")
 def test_reference_assets():
     """Every URDF and directives file of the reference's test assets: same
     tables, or the same error (most single-model URDFs are not welded to the
