@@ -51,6 +51,7 @@ SURROGATE_EPOCHS = 6
 SURROGATE_SEED = 5000
 SURROGATE_STOP = 0.01         # predicted collision probability below which a decided slot stops checking
 SURROGATE_ROUNDS = 3
+QUEUE_STEPS = 4               # timed steps whose inflations the queued form runs in one call
 CPU_SAMPLE_SCENES = (0, 1, 2, 3)
 CPU_SAMPLE = ("scenes 0-3 of the workload (7-DOF, 14-DOF, 7-DOF, 14-DOF), each scene's first seed edge (found with "
               "the oracle's checker), one inflation per step in that order, cycled; the same inflations in the "
@@ -531,7 +532,8 @@ def main():
         torch.cuda.synchronize()
         if nvtx:
             torch.cuda.nvtx.range_push("timed")
-        r = dict(dev_s=0.0, wall_s=0.0, configs=0, launches=0, faces=[], iters=[], h2d=0, d2h=0, first=None)
+        r = dict(dev_s=0.0, wall_s=0.0, configs=0, launches=0, faces=[], iters=[], h2d=0, d2h=0, first=None,
+                 kept=[], step_s=[])
         for s in range(args.warmup, steps_total):
             q0s, q1s = step_inputs(s)
             flush.fill_(1)  # L2 flush between steps (outside the timed window)
@@ -542,13 +544,16 @@ def main():
             r["dev_s"] += batch.last_device_ms * 1e-3
             if r["first"] is None:
                 r["first"] = regions
+            if len(r["kept"]) < QUEUE_STEPS:
+                r["kept"].append(regions)
+            r["step_s"].append(batch.last_device_ms * 1e-3)
             r["configs"] += int(batch.last_configs_checked.sum())
             r["launches"] += batch.last_kernel_launches
             r["faces"] += [p.A().shape[0] for p in regions]
             r["iters"] += [int(x) for x in batch.last_iterations]
             r["h2d"] += sum(sc.dim * 8 + d.A().nbytes + d.b().nbytes for sc, d in zip(scs, doms)) + 8 * nslots + 4
             r["d2h"] += sum(p.A().nbytes + p.b().nbytes for p in regions) + 16 * int(batch.last_iterations.max()) \
-                + 144 * nslots
+                + 152 * nslots
         torch.cuda.synchronize()
         if nvtx:
             torch.cuda.nvtx.range_pop()
@@ -599,10 +604,29 @@ def main():
         plain_s += e0.elapsed_time(e1) * 1e-3
         identical &= bool(np.array_equal(P.A(), first_regions[i].A()) and np.array_equal(P.b(), first_regions[i].b()))
         del inf
+    # queued form: the inflations of the first QUEUE_STEPS timed steps in one call on the same slots (each
+    # later inflation starts in the first slot that frees up), against those steps one call each
+    qsteps = len(rb["kept"])
+    qi0, qi1, qdom, qplant = [], [], [], []
+    for j in range(qsteps):
+        a0, a1 = step_inputs(args.warmup + j)
+        qi0 += a0
+        qi1 += a1
+        qdom += doms
+        qplant += slot_plant
+    flush.fill_(1)
+    torch.cuda.synchronize()
+    qregions = batched.inflate(qplant, qi0, qi1, qdom)
+    queued_s = batched.last_device_ms * 1e-3
+    per_call_s = float(sum(rb["step_s"][:qsteps]))
+    q_identical = all(np.array_equal(P.A(), R.A()) and np.array_equal(P.b(), R.b())
+                      for P, R in zip(qregions, [x for regs in rb["kept"] for x in regs]))
     if dist:
         dev_s, wall_s, configs_all = reduce_timing(dist, dev, rs["dev_s"], rs["wall_s"], float(rs["configs"]))
         b_dev, _, b_cfg = reduce_timing(dist, dev, rb["dev_s"], rb["wall_s"], float(rb["configs"]))
         plain_s, _, regions_step = reduce_timing(dist, dev, plain_s, 0.0, float(nslots))
+        queued_s, _, _ = reduce_timing(dist, dev, queued_s, 0.0, 0.0)
+        per_call_s, _, _ = reduce_timing(dist, dev, per_call_s, 0.0, 0.0)
         idn = torch.tensor([1.0 if identical else 0.0], device=dev)
         dist.all_reduce(idn, op=dist.ReduceOp.MIN)
         identical = bool(idn.item() == 1.0)
@@ -645,6 +669,13 @@ def main():
                 "plain_gpu": {"value": plain, "unit": "regions/s",
                               "sample": "the first timed step's inflations, one CudaEdgeInflator.inflateEdge "
                                         "call each", "identical_to_batched": identical},
+                "queued_gpu": {"value": regions_step * qsteps / queued_s, "unit": "regions/s",
+                               "same_inflations_one_call_per_step": regions_step * qsteps / per_call_s,
+                               "inflations": int(regions_step * qsteps), "slots_per_gpu": nslots,
+                               "identical_to_batched": q_identical,
+                               "form": f"the inflations of the first {qsteps} timed steps in one BatchedEdgeInflator "
+                                       "call on the same slots (each later inflation starts in the first slot that "
+                                       "frees up), against the same steps one call each (batched form)"},
                 "surrogate_batched_over_plain": value / plain,
                 "batched_over_plain": batched_value / plain,
                 "faces": {"mean": float(faces.mean()), "p50": float(np.median(faces)),

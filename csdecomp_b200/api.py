@@ -601,7 +601,9 @@ def EditRegionsCuda(collisions, line_segment_idxs, line_start_points, line_end_p
 class BatchedEdgeInflator:
     """Many EI-ZO inflations advancing together on the GPU (csd_batch_*): each
     slot has its own plant, segment and domain and yields exactly the region
-    CudaEdgeInflator.inflateEdge would for the same inputs (no voxels)."""
+    CudaEdgeInflator.inflateEdge would for the same inputs (no voxels).
+    inflate() takes any number of inflations: up to max_slots run at once and
+    the rest start in slots as earlier ones finish."""
 
     SAMPLE_VARIANTS = ("8 face pairs/lane, 1 block/SM", "8 face pairs/lane, 2 blocks/SM",
                        "8 face pairs/lane, 3 blocks/SM", "16 face pairs/lane, 1 block/SM",

@@ -50,9 +50,11 @@ struct SlotState {
   int m_chk;          // checked samples among the first M
   int m_coll;         // colliding samples among the first M
   int ord;            // 1: checks this iteration's samples in surrogate order; 0: in sample order, all of them
+  int k;              // the slot's iteration (slots refilled during a call run different iterations)
+  int harvested;      // finished and listed for the host by the step kernel
 };
 
-static_assert(sizeof(SlotState) == 144, "slot record size is part of the transfer accounting");
+static_assert(sizeof(SlotState) == 152, "slot record size is part of the transfer accounting");
 
 struct BatchIter {    // device-side iteration state
   int k;              // current iteration
@@ -65,6 +67,8 @@ struct BatchIter {    // device-side iteration state
   int check_next;     // first one per block (each zeroed before every launch that uses it)
   int bisect_next;
   int num_ord;        // active slots still checking in surrogate order (surrogate mode)
+  int n_act;          // largest N_k of the active slots (work-item sizing)
+  int num_fin;        // slots that finished in the last iteration, listed in BatchArgs::fin
 };
 
 struct BatchArgs {
@@ -89,6 +93,7 @@ struct BatchArgs {
   uint8_t* bpool;
   BatchIter* it;
   int* act;           // active-slot list of iteration k (slot indices, ascending)
+  int* fin;           // slots that finished in the last iteration (the host harvests and refills them)
   // surrogate mode (mlp_wb null: off)
   const void* mlp_wb;
   const float* mlp_params;
@@ -155,7 +160,7 @@ template <int KP, int MINB>
 __global__ void __launch_bounds__(256, MINB) batch_sample_kernel(BatchArgs a) {
   extern __shared__ __align__(16) float smf[];  // the face loop reads 16-byte vectors
   __shared__ GroupScratch gsa[kMaxWideGroups];
-  const int N = a.n_tab[a.it->k];
+  const int N = a.it->n_act;  // items per slot are sized by the largest active N_k
   const int64_t total = (int64_t)a.it->num_act * N;
   const int G0 = group_width(total, (int64_t)gridDim.x * (blockDim.x >> 5));
   int64_t c = total / (16 * (int64_t)gridDim.x);
@@ -166,8 +171,14 @@ __global__ void __launch_bounds__(256, MINB) batch_sample_kernel(BatchArgs a) {
   constexpr int stage_floats = (int)(SampleStage<MINB>::bytes / sizeof(float));
   int staged = -1;
   for (int it = blockIdx.x; it < items;) {
-    const int slot = a.act[it / ips], first = (int)(it % ips) * chunk, last = min(N, first + chunk);
+    const int slot = a.act[it / ips], first = (int)(it % ips) * chunk;
     const SlotState& S = a.slots[slot];
+    const int Ns = a.n_tab[S.k];
+    if (first >= Ns) {  // past this slot's chains (uniform across the block)
+      it = claim_item(&a.it->sample_next);
+      continue;
+    }
+    const int last = min(Ns, first + chunk);
     const int dim = S.dim, P = (S.nf + 1) >> 1, rs = pair_stride(dim);
     const float* rows = a.fpool + S.pr_off;
     const float* ls = a.fpool + S.seg_off;
@@ -189,11 +200,12 @@ __global__ void __launch_bounds__(256, MINB) batch_sample_kernel(BatchArgs a) {
   }
 }
 
-// Block per slot: the face-pair rows of the domain (start slacks at the
-// slot's segment start).
-__global__ void batch_init_rows_kernel(BatchArgs a) {
-  if ((int)blockIdx.x >= a.num_slots) return;
-  const SlotState& S = a.slots[blockIdx.x];
+// Block per slot (slots slot0, slot0 + 1, ...): the face-pair rows of the
+// domain (start slacks at the slot's segment start).
+__global__ void batch_init_rows_kernel(BatchArgs a, int slot0) {
+  const int slot = slot0 + (int)blockIdx.x;
+  if (slot >= a.num_slots) return;
+  const SlotState& S = a.slots[slot];
   put_faces(a.fpool + S.a_off, a.fpool + S.b_off, S.nf, S.dim, a.fpool + S.seg_off, a.fpool + S.pr_off, threadIdx.x,
             blockDim.x);
 }
@@ -239,7 +251,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_check_kernel(Bat
   __shared__ int cur;
   if (threadIdx.x == 0) cur = -1;
   __syncthreads();
-  const int N = a.n_tab[a.it->k];
+  const int N = a.it->n_act;  // items per slot are sized by the largest active N_k
   const int na = a.it->num_act;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int c = item_size((int64_t)na * N, a.cfg_max, nw);
@@ -249,11 +261,13 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_check_kernel(Bat
   for (int it = blockIdx.x; it < items; it = claim_item(&a.it->check_next)) {
     const int slot = a.act[it / ips], first = (it % ips) * c;
     const SlotState& S = a.slots[slot];
+    const int Ns = a.n_tab[S.k];
+    if (first >= Ns) continue;  // uniform across the block
     if (!block_plant<SM>(a, S.plant, &sp, &cur, smem4, &bar)) return;
     const WarpCtx<SM> w = batch_ctx<SM>(sp, smem4, static_floats);
     const float* smp = a.fpool + S.smp_off;
     uint8_t* flags = a.bpool + S.flag_off;
-    const int last = std::min(N, first + c);
+    const int last = std::min(Ns, first + c);
     for (int i = first + warp; i < last; i += nw) {
       if (lane < sp.dim) w.qs[lane] = smp[(int64_t)i * sp.dim + lane];
       __syncwarp();
@@ -268,7 +282,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_check_kernel(Bat
 __global__ void __launch_bounds__(1024) batch_compact_kernel(BatchArgs a) {
   SlotState& S = a.slots[blockIdx.x];
   if (S.done) return;
-  const int k = a.it->k;
+  const int k = S.k;
   const int N = a.n_tab[k], M = a.m_tab[k];
   if (S.status == 2) {  // the previous faces kernel ran out of capacity
     if (threadIdx.x == 0) S.done = 1;
@@ -321,7 +335,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_bisect_kernel(Ba
 // Block per slot: greedy faces, iteration bookkeeping, active-slot count.
 __global__ void __launch_bounds__(1024) batch_faces_kernel(BatchArgs a) {
   SlotState& S = a.slots[blockIdx.x];
-  const int k = a.it->k;
+  const int k = S.k;
   if (!S.done) {
     const float* ls = a.fpool + S.seg_off;
     faces_block(S.K, S.dim, a.max_faces, a.capacity, a.margin, ls, ls + S.dim, a.fpool + S.col_off,
@@ -339,20 +353,30 @@ __global__ void __launch_bounds__(1024) batch_faces_kernel(BatchArgs a) {
 // One block: advances k and rebuilds the active-slot list (ascending).
 __global__ void __launch_bounds__(1024) batch_step_kernel(BatchArgs a) {
   __shared__ int warp_n[32];
-  __shared__ int base, mf8, mf16, nord;
+  __shared__ int base, mf8, mf16, nord, nmax, nfin;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
   if (tid == 0) {
     base = 0;
     mf8 = 0;
     mf16 = 0;
     nord = 0;
+    nmax = 0;
+    nfin = 0;
   }
   __syncthreads();
   for (int s0 = 0; s0 < a.num_slots; s0 += blockDim.x) {
     const int s = s0 + tid;
     const bool act = s < a.num_slots && !a.slots[s].done;
-    if (act) atomicMax(a.slots[s].dim <= 8 ? &mf8 : &mf16, a.slots[s].nf);
-    if (act && a.slots[s].ord) atomicAdd(&nord, 1);
+    if (act) {
+      SlotState& S = a.slots[s];
+      S.k += 1;  // the slot finished its iteration and runs the next
+      atomicMax(S.dim <= 8 ? &mf8 : &mf16, S.nf);
+      atomicMax(&nmax, a.n_tab[min(S.k, a.max_iters - 1)]);
+      if (S.ord) atomicAdd(&nord, 1);
+    } else if (s < a.num_slots && !a.slots[s].harvested) {
+      a.slots[s].harvested = 1;
+      a.fin[atomicAdd(&nfin, 1)] = s;  // finished this iteration: the host collects it
+    }
     const unsigned m = __ballot_sync(0xffffffffu, act);
     if (lane == 0) warp_n[warp] = __popc(m);
     __syncthreads();
@@ -373,6 +397,8 @@ __global__ void __launch_bounds__(1024) batch_step_kernel(BatchArgs a) {
     it->max_nf8 = mf8;
     it->max_nf16 = mf16;
     it->num_ord = nord;
+    it->n_act = nmax;
+    it->num_fin = nfin;
   }
 }
 
@@ -385,11 +411,11 @@ __global__ void __launch_bounds__(mlp::kThreads) batch_score_kernel(BatchArgs a)
   __shared__ uint64_t bars[2];
   __shared__ uint32_t tmem_base;
   if ((int)blockIdx.y >= a.it->num_act) return;
-  const int N = a.n_tab[a.it->k];
-  const int row0 = blockIdx.x * 128;
-  if (row0 >= N) return;
   const int slot = a.act[blockIdx.y];
   const SlotState& S = a.slots[slot];
+  const int N = a.n_tab[S.k];
+  const int row0 = blockIdx.x * 128;
+  if (row0 >= N) return;
   if (!S.ord) return;  // this slot checks in sample order: no scores needed
   mlp::FwdGroup G{};
   G.x = a.fpool + S.smp_off;
@@ -425,7 +451,7 @@ __global__ void __launch_bounds__(1024) batch_sort_kernel(BatchArgs a) {
   extern __shared__ unsigned long long keys[];
   if ((int)blockIdx.x >= a.it->num_act) return;
   const int slot = a.act[blockIdx.x];
-  const int N = a.n_tab[a.it->k];
+  const int N = a.n_tab[a.slots[slot].k];
   int* ord = a.order + (size_t)slot * a.n_max;
   uint8_t* flags = a.bpool + a.slots[slot].flag_off;
   const bool sorted = a.slots[slot].ord != 0;  // uniform across the block
@@ -489,7 +515,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_check_sorted_ker
   __shared__ int cur;
   if (threadIdx.x == 0) cur = -1;
   __syncthreads();
-  const int N = a.n_tab[a.it->k];
+  const int N = a.it->n_act;  // items are sized by the largest active N_k
   const int beg = round_begin(a, r, N), end = round_end(a, r, N), cnt = end - beg;
   if (cnt <= 0) return;
   const int na = a.it->num_act;
@@ -500,15 +526,16 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) batch_check_sorted_ker
   const VoxArgs none{nullptr, 0, 0.f, nullptr, nullptr, 0};
   // work queue it->check_next: `for` advances through claim_item on every path, `continue` included
   for (int it = blockIdx.x; it < items; it = claim_item(&a.it->check_next)) {
-    const int slot = a.act[it / ips], first = beg + (it % ips) * c;
+    const int slot = a.act[it / ips];
     const SlotState& S = a.slots[slot];
-    if (S.done || !S.need) continue;  // uniform across the block
+    const int Ns = a.n_tab[S.k], end_s = round_end(a, r, Ns), first = round_begin(a, r, Ns) + (it % ips) * c;
+    if (S.done || !S.need || first >= end_s) continue;  // uniform across the block
     if (!block_plant<SM>(a, S.plant, &sp, &cur, smem4, &bar)) return;
     const WarpCtx<SM> w = batch_ctx<SM>(sp, smem4, static_floats);
     const float* smp = a.fpool + S.smp_off;
     const int* ord = a.order + (size_t)slot * a.n_max;
     uint8_t* flags = a.bpool + S.flag_off;
-    const int last = min(end, first + c);
+    const int last = min(end_s, first + c);
     for (int p = first + warp; p < last; p += nw) {
       const int i = ord[p];
       if (lane < sp.dim) w.qs[lane] = smp[(int64_t)i * sp.dim + lane];
@@ -530,7 +557,7 @@ __global__ void __launch_bounds__(256) batch_tally_kernel(BatchArgs a, int r) {
   __shared__ int red[3][8];
   SlotState& S = a.slots[blockIdx.x];
   if (S.done || !S.need) return;
-  const int k = a.it->k, N = a.n_tab[k], M = a.m_tab[k];
+  const int k = S.k, N = a.n_tab[k], M = a.m_tab[k];
   const int beg = round_begin(a, r, N), end = round_end(a, r, N);
   const int* ord = a.order + (size_t)blockIdx.x * a.n_max;
   const uint8_t* flags = a.bpool + S.flag_off;
@@ -589,7 +616,7 @@ __global__ void __launch_bounds__(1024) batch_compact_sorted_kernel(BatchArgs a)
     if (threadIdx.x == 0) S.done = 1;
     return;
   }
-  const int k = a.it->k, N = a.n_tab[k];
+  const int k = S.k, N = a.n_tab[k];
   const int dim = S.dim;
   const uint8_t* flags = a.bpool + S.flag_off;
   const float* smp = a.fpool + S.smp_off;
@@ -687,13 +714,13 @@ struct csd_batch_s {
   int tuned_iters = 0;
   std::vector<int> n_tab, m_tab;
   std::vector<float> thr_tab;
-  csd::DevBuf plants_dev, slots_dev, tabs, fpool, bpool, iter, act;
+  csd::DevBuf plants_dev, slots_dev, tabs, fpool, bpool, iter, act, fin;
   // surrogate mode
   csd_mlp_t mlp = nullptr;
   float stop_logit = 0.f;
   int rounds = 3, round_base = 1024;
   csd::DevBuf scores, order, status;
-  std::vector<csd::SlotState> host_slots;
+  std::vector<long long> job_configs;  // configurations checked per inflation of the last call
   std::vector<int> act_host;
   cudaGraphExec_t graph = nullptr;
   int graph_slots = -1, graph_cfg = -1, graph_variant = -1;
@@ -919,7 +946,8 @@ csd_status_t csd_batch_create(const csd_plant_t* plants, int32_t num_plants, int
   if ((s = h->plants_dev.reserve(dps.size() * sizeof(DevPlant))) || (s = h->slots_dev.reserve(max_slots * sizeof(SlotState))) ||
       (s = h->tabs.reserve(h->n_tab.size() * 12 + 64)) || (s = h->fpool.reserve(per_slot_f * max_slots * 4 + 256)) ||
       (s = h->bpool.reserve((size_t)h->n_max * max_slots + 256)) || (s = h->iter.reserve(sizeof(BatchIter))) ||
-      (s = h->act.reserve((size_t)max_slots * 4)) || (s = h->status.reserve(16)))
+      (s = h->act.reserve((size_t)max_slots * 4)) || (s = h->fin.reserve((size_t)max_slots * 4)) ||
+      (s = h->status.reserve(16)))
     return s;
   CSD_CUDA_TRY(cudaMemcpy(h->plants_dev.ptr, dps.data(), dps.size() * sizeof(DevPlant), cudaMemcpyHostToDevice));
   int* t = h->tabs.as<int>();
@@ -947,7 +975,7 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
                                const float* ends, const float* domain_A, const float* domain_b,
                                const int32_t* domain_face_offsets, float* A_out, float* b_out, int32_t* num_faces,
                                int32_t* num_iterations, float* device_ms) {
-  CSD_CHECK(h && n >= 0 && n <= h->max_slots, CSD_ERR_INVALID, "bad slot count");
+  CSD_CHECK(h && n >= 0, CSD_ERR_INVALID, "bad inflation count");
   if (n == 0) return CSD_OK;
   CSD_CHECK(slot_plant && starts && ends && domain_A && domain_b && domain_face_offsets && A_out && b_out && num_faces,
             CSD_ERR_INVALID, "null argument");
@@ -962,9 +990,10 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
   } restore{cur, h->device};
   const size_t D = (size_t)h->max_dim, np = h->opt.num_particles, cap = (size_t)h->capacity;
   const size_t per_slot_f = slot_floats(h);
-  std::vector<SlotState> slots(n);
-  size_t qoff = 0, arow = 0;
-  cudaStream_t st = h->graph_stream;
+  const int ns = std::min<int>(n, h->max_slots);  // slots in use; inflations past them wait for a free slot
+  // every inflation's inputs are checked before any work starts
+  std::vector<size_t> q_off(n), a_row(n), out_off(n);
+  size_t qoff = 0, arow = 0, ooff = 0;
   for (int i = 0; i < n; ++i) {
     const int pi = slot_plant[i];
     CSD_CHECK(pi >= 0 && pi < (int)h->plants.size(), CSD_ERR_INVALID, "slot plant index out of range");
@@ -979,20 +1008,28 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
         float ax = 0.f;
         for (int k = 0; k < d; ++k) ax += domain_A[arow + (size_t)f * d + k] * x[k];
         if (!(ax <= domain_b[f0 + f] + 1e-9f)) {
-          set_error("slot " + std::to_string(i) + ": line segment endpoints must lie in the domain");
+          set_error("inflation " + std::to_string(i) + ": line segment endpoints must lie in the domain");
           return CSD_ERR_NOT_CONTAINED;
         }
       }
     }
+    q_off[i] = qoff;
+    a_row[i] = arow;
+    out_off[i] = ooff;
+    qoff += d;
     arow += (size_t)(f1 - f0) * d;
-    SlotState& S = slots[i];
-    S = SlotState{};
-    S.plant = pi;
-    S.dim = d;
-    S.domain_faces = f1 - f0;
-    S.nf = f1 - f0;
+    ooff += cap * d;
+  }
+  cudaStream_t st = h->graph_stream;
+  // the record of slot `slot` starting inflation `job`, and the upload of that inflation's domain and segment
+  auto record = [&](int slot, int job) {
+    SlotState S{};
+    S.plant = slot_plant[job];
+    S.dim = h->plants[S.plant]->dp.dim;
+    S.domain_faces = domain_face_offsets[job + 1] - domain_face_offsets[job];
+    S.nf = S.domain_faces;
     S.ord = 1;
-    const long long base = (long long)(per_slot_f * i);
+    const long long base = (long long)(per_slot_f * slot);
     S.pr_off = base;  // 16-byte aligned: per_slot_f is a multiple of 4 floats
     S.a_off = S.pr_off + (long long)pair_floats(h);
     S.b_off = S.a_off + (long long)(cap * D);
@@ -1000,45 +1037,41 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
     S.smp_off = S.seg_off + (long long)(2 * D);
     S.col_off = S.smp_off + (long long)((size_t)h->n_max * D);
     S.dist_off = S.col_off + (long long)(2 * np * D);
-    S.flag_off = (long long)h->n_max * i;
-    qoff += d;
+    S.flag_off = (long long)h->n_max * slot;
+    return S;
+  };
+  auto upload = [&](const SlotState& S, int job) -> csd_status_t {
+    const int d = S.dim, F = S.nf;
+    float* fp = h->fpool.as<float>();
+    CSD_CUDA_TRY(cudaMemcpyAsync(fp + S.a_off, domain_A + a_row[job], (size_t)F * d * 4, cudaMemcpyHostToDevice, st));
+    CSD_CUDA_TRY(cudaMemcpyAsync(fp + S.b_off, domain_b + domain_face_offsets[job], (size_t)F * 4,
+                                 cudaMemcpyHostToDevice, st));
+    CSD_CUDA_TRY(cudaMemcpyAsync(fp + S.seg_off, starts + q_off[job], d * 4, cudaMemcpyHostToDevice, st));
+    CSD_CUDA_TRY(cudaMemcpyAsync(fp + S.seg_off + d, ends + q_off[job], d * 4, cudaMemcpyHostToDevice, st));
+    return CSD_OK;
+  };
+  std::vector<SlotState> slots(ns);
+  std::vector<int> slot_job(ns);
+  csd_status_t s;
+  for (int i = 0; i < ns; ++i) {
+    slots[i] = record(i, i);
+    slot_job[i] = i;
+    if ((s = upload(slots[i], i))) return s;
   }
-  // domain rows of slot i are rows [f0, f1) of domain_A with that slot's dim
-  {
-    size_t arow = 0;  // float offset into domain_A
-    for (int i = 0; i < n; ++i) {
-      const int d = slots[i].dim;
-      const int F = slots[i].nf;
-      const int f0 = domain_face_offsets[i];
-      (void)f0;
-      CSD_CUDA_TRY(cudaMemcpyAsync(h->fpool.as<float>() + slots[i].a_off, domain_A + arow, (size_t)F * d * 4,
-                                   cudaMemcpyHostToDevice, st));
-      CSD_CUDA_TRY(cudaMemcpyAsync(h->fpool.as<float>() + slots[i].b_off, domain_b + domain_face_offsets[i],
-                                   (size_t)F * 4, cudaMemcpyHostToDevice, st));
-      arow += (size_t)F * d;
-    }
-    size_t q = 0;
-    for (int i = 0; i < n; ++i) {
-      const int d = slots[i].dim;
-      CSD_CUDA_TRY(cudaMemcpyAsync(h->fpool.as<float>() + slots[i].seg_off, starts + q, d * 4,
-                                   cudaMemcpyHostToDevice, st));
-      CSD_CUDA_TRY(cudaMemcpyAsync(h->fpool.as<float>() + slots[i].seg_off + d, ends + q, d * 4,
-                                   cudaMemcpyHostToDevice, st));
-      q += d;
-    }
-  }
-  CSD_CUDA_TRY(cudaMemcpyAsync(h->slots_dev.ptr, slots.data(), n * sizeof(SlotState), cudaMemcpyHostToDevice, st));
+  int next_job = ns;
+  CSD_CUDA_TRY(cudaMemcpyAsync(h->slots_dev.ptr, slots.data(), ns * sizeof(SlotState), cudaMemcpyHostToDevice, st));
   BatchIter zero{};
-  zero.num_act = n;
+  zero.num_act = ns;
+  zero.n_act = h->n_tab[0];
   *h->host_iter = zero;
   CSD_CUDA_TRY(cudaMemcpyAsync(h->iter.ptr, h->host_iter, sizeof(BatchIter), cudaMemcpyHostToDevice, st));
-  h->act_host.resize(n);
-  for (int i = 0; i < n; ++i) h->act_host[i] = i;
-  CSD_CUDA_TRY(cudaMemcpyAsync(h->act.ptr, h->act_host.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st));
+  h->act_host.resize(ns);
+  for (int i = 0; i < ns; ++i) h->act_host[i] = i;
+  CSD_CUDA_TRY(cudaMemcpyAsync(h->act.ptr, h->act_host.data(), (size_t)ns * 4, cudaMemcpyHostToDevice, st));
   BatchArgs a{};
   a.slots = h->slots_dev.as<SlotState>();
   a.plants = h->plants_dev.as<DevPlant>();
-  a.num_slots = n;
+  a.num_slots = ns;
   a.n_max = h->n_max;
   a.max_iters = (int)h->opt.max_iterations;
   a.num_particles = (int)h->opt.num_particles;
@@ -1057,6 +1090,7 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
   a.bpool = h->bpool.as<uint8_t>();
   a.it = h->iter.as<BatchIter>();
   a.act = h->act.as<int>();
+  a.fin = h->fin.as<int>();
   a.cfg_max = h->cfg_max;
   a.part_max = h->part_max;
   if (h->mlp) {
@@ -1072,12 +1106,32 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
   }
   a.status = h->status.as<int>();
   CSD_CUDA_TRY(cudaMemsetAsync(h->status.ptr, 0, 16, st));
-  batch_init_rows_kernel<<<n, 256, 0, st>>>(a);
+  batch_init_rows_kernel<<<ns, 256, 0, st>>>(a, 0);
   h->launches = 1;
   CSD_CUDA_TRY(cudaGetLastError());
   h->run_variant = h->sample_variant;
-  csd_status_t s = build_graph(h, n, a);
-  if (s) return s;
+  if ((s = build_graph(h, ns, a))) return s;
+  // collected results: a finished slot's region, iteration count and configurations go to its inflation
+  h->job_configs.assign(n, 0);
+  std::vector<char> done_job(n, 0);
+  auto harvest = [&](int slot, const SlotState& S) -> csd_status_t {
+    const int job = slot_job[slot];
+    if (job < 0 || done_job[job]) return CSD_OK;
+    if (S.status == 2) {
+      set_error("Max face count exceeded in inflation " + std::to_string(job));
+      return CSD_ERR_CAPACITY;
+    }
+    num_faces[job] = S.nf;
+    if (num_iterations) num_iterations[job] = S.iters;
+    h->job_configs[job] = S.configs;
+    CSD_CUDA_TRY(cudaMemcpyAsync(A_out + out_off[job], h->fpool.as<float>() + S.a_off, (size_t)S.nf * S.dim * 4,
+                                 cudaMemcpyDeviceToHost, st));
+    CSD_CUDA_TRY(cudaMemcpyAsync(b_out + (size_t)job * cap, h->fpool.as<float>() + S.b_off, (size_t)S.nf * 4,
+                                 cudaMemcpyDeviceToHost, st));
+    done_job[job] = 1;
+    slot_job[slot] = -1;
+    return CSD_OK;
+  };
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   if (device_ms) {
     CSD_CUDA_TRY(cudaEventCreate(&ev0));
@@ -1089,8 +1143,9 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
   h->sample_flop = 0.0;
   std::vector<SlotState> prof_slots;
   if (h->profile) prof_slots = slots;  // the records as uploaded: faces of the domain
-  int active_now = n;
-  for (uint32_t k = 0; k < h->opt.max_iterations; ++k) {
+  std::vector<int> fin;
+  int active_now = ns;
+  for (;;) {
     if (h->tune_iters > 0) {
       // every sampler variant and check item size on this iteration's inputs
       // (both stages are idempotent: a rerun writes the same samples and
@@ -1119,7 +1174,7 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
         cudaEventRecord(tev[2 * j + 1], st);
         ++h->launches;
       }
-      h->launches += launch_iteration(h, n, a, st, nullptr, true);
+      h->launches += launch_iteration(h, ns, a, st, nullptr, true);
       CSD_CUDA_TRY(cudaGetLastError());
       CSD_CUDA_TRY(cudaStreamSynchronize(st));
       for (int q = 0; q < j; ++q) {
@@ -1142,10 +1197,10 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
         if (!a.mlp_wb) h->cfg_max = kCheckItemCaps[bc];
         a.cfg_max = h->cfg_max;
         h->graph_slots = -1;  // recapture with the chosen shapes
-        if ((s = build_graph(h, n, a))) return s;
+        if ((s = build_graph(h, ns, a))) return s;
       }
     } else if (h->profile) {
-      h->launches += launch_iteration(h, n, a, st, h->ev);
+      h->launches += launch_iteration(h, ns, a, st, h->ev);
       CSD_CUDA_TRY(cudaGetLastError());
       CSD_CUDA_TRY(cudaEventSynchronize(h->ev[kStages]));
       for (int j = 0; j < kStages; ++j) {
@@ -1158,8 +1213,8 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
       // sampler work of this iteration, from the records before it ran
       for (const SlotState& S : prof_slots)
         if (!S.done)
-          h->sample_flop += (double)h->n_tab[k] * h->opt.mixing_steps * (2.0 * S.dim + 4.0) * S.nf;
-      CSD_CUDA_TRY(cudaMemcpyAsync(prof_slots.data(), h->slots_dev.ptr, n * sizeof(SlotState),
+          h->sample_flop += (double)h->n_tab[S.k] * h->opt.mixing_steps * (2.0 * S.dim + 4.0) * S.nf;
+      CSD_CUDA_TRY(cudaMemcpyAsync(prof_slots.data(), h->slots_dev.ptr, ns * sizeof(SlotState),
                                    cudaMemcpyDeviceToHost, st));
     } else {
       CSD_CUDA_TRY(cudaGraphLaunch(h->graph, st));
@@ -1168,13 +1223,52 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
     CSD_CUDA_TRY(cudaMemcpyAsync(h->host_iter, h->iter.ptr, sizeof(BatchIter), cudaMemcpyDeviceToHost, st));
     CSD_CUDA_TRY(cudaStreamSynchronize(st));
     active_now = h->host_iter->last_active;
+    // slots that finished: collect their inflations and start queued ones in them
+    const int nfin = h->host_iter->num_fin;
+    if (nfin > 0 && next_job < n) {
+      fin.resize(nfin);
+      CSD_CUDA_TRY(cudaMemcpyAsync(fin.data(), h->fin.ptr, (size_t)nfin * 4, cudaMemcpyDeviceToHost, st));
+      CSD_CUDA_TRY(cudaStreamSynchronize(st));
+      std::sort(fin.begin(), fin.end());
+      std::vector<int> refilled;
+      for (int slot : fin) {
+        SlotState S{};
+        CSD_CUDA_TRY(cudaMemcpyAsync(&S, h->slots_dev.as<SlotState>() + slot, sizeof(SlotState),
+                                     cudaMemcpyDeviceToHost, st));
+        CSD_CUDA_TRY(cudaStreamSynchronize(st));
+        if ((s = harvest(slot, S))) return s;
+        if (next_job >= n) continue;
+        const int job = next_job++;
+        slots[slot] = record(slot, job);
+        slot_job[slot] = job;
+        if ((s = upload(slots[slot], job))) return s;
+        CSD_CUDA_TRY(cudaMemcpyAsync(h->slots_dev.as<SlotState>() + slot, &slots[slot], sizeof(SlotState),
+                                     cudaMemcpyHostToDevice, st));
+        batch_init_rows_kernel<<<1, 256, 0, st>>>(a, slot);
+        ++h->launches;
+        refilled.push_back(slot);
+      }
+      if (!refilled.empty()) {
+        // append the refilled slots to the next iteration's active list
+        const int na = h->host_iter->num_act;
+        CSD_CUDA_TRY(cudaMemcpyAsync(h->act.as<int>() + na, refilled.data(), refilled.size() * 4,
+                                     cudaMemcpyHostToDevice, st));
+        h->host_iter->num_act = na + (int)refilled.size();
+        h->host_iter->n_act = std::max(h->host_iter->n_act, h->n_tab[0]);
+        CSD_CUDA_TRY(cudaMemcpyAsync(h->iter.ptr, h->host_iter, sizeof(BatchIter), cudaMemcpyHostToDevice, st));
+        CSD_CUDA_TRY(cudaStreamSynchronize(st));
+        active_now += (int)refilled.size();
+        if (h->profile)
+          for (int slot : refilled) prof_slots[slot] = slots[slot];
+      }
+    }
     if (active_now == 0) break;
     // surrogate mode: once no active slot checks in surrogate order, the remaining
     // iterations run the batched form's graph (no scoring, sorting or rounds; the
     // same checks as a slot checking in sample order)
-    if (a.mlp_wb && h->host_iter->num_ord == 0 && h->tune_iters == 0) {
+    if (a.mlp_wb && h->host_iter->num_ord == 0 && next_job >= n && h->tune_iters == 0) {
       a.mlp_wb = nullptr;
-      if ((s = build_graph(h, n, a))) return s;
+      if ((s = build_graph(h, ns, a))) return s;
     }
     // a slot's region outgrew the staging buffer of the running variant: continue with the
     // fastest variant that stages it (identical samples; the graph is captured again)
@@ -1185,7 +1279,7 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
         if (v != h->run_variant) {
           h->run_variant = v;
           h->large_variant = v;
-          if ((s = build_graph(h, n, a))) return s;
+          if ((s = build_graph(h, ns, a))) return s;
         }
       }
     }
@@ -1197,7 +1291,7 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
   }
-  CSD_CUDA_TRY(cudaMemcpyAsync(slots.data(), h->slots_dev.ptr, n * sizeof(SlotState), cudaMemcpyDeviceToHost, st));
+  CSD_CUDA_TRY(cudaMemcpyAsync(slots.data(), h->slots_dev.ptr, ns * sizeof(SlotState), cudaMemcpyDeviceToHost, st));
   int kstat = 0;
   CSD_CUDA_TRY(cudaMemcpyAsync(&kstat, h->status.ptr, 4, cudaMemcpyDeviceToHost, st));
   CSD_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1207,23 +1301,14 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
   }
   for (csd_plant_t pl : h->plants)
     if ((s = plant_status(pl, st))) return s;
-  h->host_slots.assign(slots.begin(), slots.end());
-  size_t aoff = 0;
-  for (int i = 0; i < n; ++i) {
-    const SlotState& S = slots[i];
-    if (S.status == 2) {
-      set_error("Max face count exceeded in slot " + std::to_string(i));
-      return CSD_ERR_CAPACITY;
-    }
-    num_faces[i] = S.nf;
-    if (num_iterations) num_iterations[i] = S.iters;
-    CSD_CUDA_TRY(cudaMemcpyAsync(A_out + aoff, h->fpool.as<float>() + S.a_off, (size_t)S.nf * S.dim * 4,
-                                 cudaMemcpyDeviceToHost, st));
-    CSD_CUDA_TRY(cudaMemcpyAsync(b_out + (size_t)i * h->capacity, h->fpool.as<float>() + S.b_off, (size_t)S.nf * 4,
-                                 cudaMemcpyDeviceToHost, st));
-    aoff += (size_t)h->capacity * S.dim;
-  }
+  for (int i = 0; i < ns; ++i)
+    if ((s = harvest(i, slots[i]))) return s;
   CSD_CUDA_TRY(cudaStreamSynchronize(st));
+  for (int j = 0; j < n; ++j)
+    if (!done_job[j]) {
+      set_error("inflation " + std::to_string(j) + " was not completed");
+      return CSD_ERR_CUDA;
+    }
   return CSD_OK;
 }
 
@@ -1356,9 +1441,9 @@ csd_status_t csd_batch_iteration_profile(csd_batch_t h, int32_t cap, float* stag
 }
 
 csd_status_t csd_batch_configs_checked(csd_batch_t h, int32_t n, int64_t* configs) {
-  CSD_CHECK(h && configs && n >= 0 && n <= (int)h->host_slots.size(), CSD_ERR_INVALID,
-            "slot count exceeds the last batch");
-  for (int i = 0; i < n; ++i) configs[i] = h->host_slots[i].configs;
+  CSD_CHECK(h && configs && n >= 0 && n <= (int)h->job_configs.size(), CSD_ERR_INVALID,
+            "count exceeds the inflations of the last call");
+  for (int i = 0; i < n; ++i) configs[i] = h->job_configs[i];
   return CSD_OK;
 }
 

@@ -284,14 +284,18 @@ typedef struct csd_batch_s* csd_batch_t;
 /* csd_mlp_t (the surrogate bank, functions csd_mlp_* below) is declared above csd_check_edges_ranked. */
 csd_status_t csd_batch_create(const csd_plant_t* plants, int32_t num_plants, int32_t max_slots,
                               const csd_eizo_options_t* options, int32_t face_capacity, csd_batch_t* out);
-/* n slots: slot i uses plants[slot_plant[i]] (dim d_i); starts/ends hold the
- * segments back to back (d_i floats each); the domain of slot i is rows
- * [domain_face_offsets[i], domain_face_offsets[i+1]) of domain_b and the same
- * rows of domain_A, stored back to back with d_i floats per row. Region i is
- * written to A_out at float offset sum_{j<i} face_capacity * d_j (row-major,
- * d_i floats per row) and b_out at i * face_capacity; num_faces[i] rows. All
- * arrays are host memory; the call synchronises before returning. device_ms
- * (optional) receives the GPU time from the first to the last iteration. */
+/* n inflations: inflation i uses plants[slot_plant[i]] (dim d_i);
+ * starts/ends hold the segments back to back (d_i floats each); the domain of
+ * inflation i is rows [domain_face_offsets[i], domain_face_offsets[i+1]) of
+ * domain_b and the same rows of domain_A, stored back to back with d_i floats
+ * per row. Region i is written to A_out at float offset sum_{j<i}
+ * face_capacity * d_j (row-major, d_i floats per row) and b_out at i *
+ * face_capacity; num_faces[i] rows. n may exceed max_slots: inflations
+ * 0..max_slots-1 start at once and each later one starts in the first slot
+ * that frees up (slots then run different iterations; each inflation still
+ * computes exactly what csd_inflator_inflate computes). All arrays are host
+ * memory; the call synchronises before returning. device_ms (optional)
+ * receives the GPU time from the first to the last iteration. */
 csd_status_t csd_batch_inflate(csd_batch_t batch, int32_t n, const int32_t* slot_plant, const float* starts,
                                const float* ends, const float* domain_A, const float* domain_b,
                                const int32_t* domain_face_offsets, float* A_out, float* b_out, int32_t* num_faces,

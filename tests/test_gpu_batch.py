@@ -111,3 +111,39 @@ def test_autotuned_batch_reports_and_matches_fixed_shapes():
     for g, r in zip(got, ref):
         np.testing.assert_array_equal(g.A(), r.A())
         np.testing.assert_array_equal(g.b(), r.b())
+
+
+def test_queued_inflations_refill_slots():
+    """More inflations than slots: each later inflation starts in the first slot
+    that frees up, so slots run different iterations at once. Every region
+    still equals the single inflation's bit for bit, with the same iteration
+    count, and the configurations checked equal a batch that holds them all."""
+    s7 = scenes.arm_scene(31, num_spheres=40, num_capsules=2, num_world_boxes=30, num_world_spheres=30, keepout=0.8)
+    s14 = scenes.arm_scene(32, num_spheres=40, num_capsules=2, num_world_boxes=20, num_world_spheres=20, arms=2,
+                           keepout=0.9, arm_spacing=1.4)
+    opt = csd.EizoOptions(num_particles=600, mixing_steps=20, max_iterations=40)
+    cap = 400
+    e7 = free_edges(s7, 4, 0.3, 1)
+    e14 = free_edges(s14, 3, 0.3, 2)
+    slots = [1, 0, 0, 1, 0, 1, 0]
+    edges = [e14[0], e7[0], e7[1], e14[1], e7[2], e14[2], e7[3]]
+    scn = [s7, s14]
+    doms = [box(scn[i]) for i in slots]
+    small = csd.BatchedEdgeInflator([s7.plant, s14.plant], opt, max_slots=3, face_capacity=cap)
+    got = small.inflate(slots, [e[0] for e in edges], [e[1] for e in edges], doms)
+    its, cfg = small.last_iterations.copy(), small.last_configs_checked.copy()
+    assert len(got) == len(edges) and len(set(its)) > 1
+    full = csd.BatchedEdgeInflator([s7.plant, s14.plant], opt, max_slots=8, face_capacity=cap)
+    ref_all = full.inflate(slots, [e[0] for e in edges], [e[1] for e in edges], doms)
+    np.testing.assert_array_equal(cfg, full.last_configs_checked)
+    for i, (pi, e) in enumerate(zip(slots, edges)):
+        inf = csd.CudaEdgeInflator(scn[pi].plant, scn[pi].inspector.robot_geometry_ids, opt, box(scn[pi]),
+                                   face_capacity=cap)
+        ref = inf.inflateEdge(e[0], e[1], None, 0.0, verbose=False)
+        np.testing.assert_array_equal(got[i].A(), ref.A(), err_msg=f"inflation {i}")
+        np.testing.assert_array_equal(got[i].b(), ref.b(), err_msg=f"inflation {i}")
+        np.testing.assert_array_equal(got[i].A(), ref_all[i].A())
+        assert its[i] == len(inf.last_info.iteration_info)
+    # the handle serves a later call with fewer inflations than slots
+    again = small.inflate(slots[:2], [e[0] for e in edges[:2]], [e[1] for e in edges[:2]], doms[:2])
+    np.testing.assert_array_equal(again[0].A(), got[0].A())
