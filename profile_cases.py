@@ -4,7 +4,7 @@
       one warm-up and one timed check_points launch on N collision-free
       configurations of the 7-DOF arm (80 spheres + 4 capsules) in 200 world
       primitives (with --no-cull every pair is evaluated: the full sweep)
-  python profile_cases.py batch [--slots S] [--iterations I]
+  python profile_cases.py batch [--slots S] [--iterations I] [--dim {7,14}]
       [--sample-variant V] [--check-item-cap C] [--per-iteration]
       S inflations of the batched EI-ZO workload (first S scenes), at most I
       iterations, launched stage by stage (profiling mode) with the given
@@ -36,6 +36,11 @@
   python profile_cases.py edit_regions [--regions R] [--collisions C]
       EditRegionsCuda on the config-3 scene: R box regions around seed edges,
       C colliding configurations drawn inside each, 9 bisection steps
+
+  python profile_cases.py mlp [--nets K] [--rows R] [--train-steps T]
+      surrogate bank of K 14-input nets: T Adam steps of 512 rows per net
+      (tensor-core backward GEMMs) and one scoring pass of R rows per net
+      (fused tensor-core forward)
 
 Each prints the device time of what it ran (CUDA events, after one warm-up).
 """
@@ -81,7 +86,8 @@ def check_points(n: int, cull: bool = True) -> None:
                       "flop_per_config": h.flops()["total"], "launch_ms": ms[-1]}))
 
 
-def batch(slots: int, iterations: int, sample_variant: int, check_item_cap: int, per_iteration: bool = False) -> None:
+def batch(slots: int, iterations: int, sample_variant: int, check_item_cap: int, per_iteration: bool = False,
+          dim: int = 0) -> None:
     import csdecomp_b200 as csd
     from csdecomp_b200 import scenes
     eizo = dict(num_particles=2000, mixing_steps=50, bisection_steps=9, max_hyperplanes_per_iteration=10,
@@ -89,6 +95,8 @@ def batch(slots: int, iterations: int, sample_variant: int, check_item_cap: int,
     scs, edges = [], []
     seeds = scenes.batch_scene_seeds(4 * slots + 64)
     for i, s in enumerate(seeds):
+        if dim and (7 if i % 2 == 0 else 14) != dim:
+            continue
         sc = scenes.batch_scene(i, s)
         e = scenes.seed_edges(sc, 1, 3000 + 101 * i, lambda q: csd.CheckCollisionFreeCuda(q.T, sc.plant),
                               lambda a, b: csd.CheckEdgesCollisionFreeCuda(a.T, b.T, sc.plant))
@@ -107,12 +115,31 @@ def batch(slots: int, iterations: int, sample_variant: int, check_item_cap: int,
     b.set_shapes(sample_variant, check_item_cap)
     b.set_profiling(True)
     b.inflate(list(range(len(scs))), [e[0] for e in edges], [e[1] for e in edges], doms)
-    out = {"case": "batch", "slots": len(scs), "stage_ms": b.stage_ms(), "iterations": b.last_iterations.tolist()}
+    out = {"case": "batch", "slots": len(scs), "stage_ms": b.stage_ms(), "iterations": b.last_iterations.tolist(),
+           "sample_flop": b.sample_flops(), "sample_variant": b.SAMPLE_VARIANTS[sample_variant]}
     if per_iteration:
         ms, act = b.iteration_profile()
         out["per_iteration"] = {"active": act.tolist(), "total_ms": ms.sum(1).round(3).tolist(),
                                 "stages": list(b.STAGES), "stage_ms": ms.round(3).tolist()}
     print(json.dumps(out))
+
+
+def mlp(nets: int, rows: int, steps: int) -> None:
+    """Surrogate bank of `nets` 14-input nets: `steps` Adam steps of 512 rows
+    per net (backward GEMMs, gemm_kernel) and one scoring pass of `rows` rows
+    per net (fused forward, mlp_forward_kernel), each timed after a warm-up."""
+    import torch
+    from csdecomp_b200.surrogate import CollisionSurrogate
+    rng = np.random.default_rng(3)
+    bank = CollisionSurrogate([14] * nets, seed=1)
+    xs = [rng.uniform(-np.pi, np.pi, (rows, 14)).astype(np.float32) for _ in range(nets)]
+    ys = [(np.linalg.norm(x, axis=1) < 5.0).astype(np.uint8) for x in xs]
+    t_train, _ = _timed(lambda: bank.train(xs, ys, batch=512, epochs=512 * steps / rows, lr=1e-3), reps=2)
+    t_fwd, _ = _timed(lambda: bank.logits(list(enumerate(xs))), reps=3)
+    fwd_flop = 2.0 * nets * rows * (16 * 256 + 2 * 256 * 256 + 256)
+    print(json.dumps({"case": "mlp", "nets": nets, "rows_per_net": rows, "train_steps": steps,
+                      "train_ms": t_train, "forward_ms": t_fwd, "forward_flop": fwd_flop,
+                      "forward_tflops_incl_copies": fwd_flop / t_fwd / 1e9}))
 
 
 def _timed(fn, reps: int = 3):
@@ -323,7 +350,7 @@ def edge_check_ranked(n: int) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["check_points", "batch", "point_check", "edge_check", "eizo_single",
-                                     "visibility_graph", "edit_regions", "voxel_check", "edge_check_ranked"])
+                                     "visibility_graph", "edit_regions", "voxel_check", "edge_check_ranked", "mlp"])
     ap.add_argument("--configs", type=int, default=1 << 20)
     ap.add_argument("--no-cull", action="store_true", help="check_points: link-level broad phase off (full sweep)")
     ap.add_argument("--slots", type=int, default=24)
@@ -336,6 +363,10 @@ def main() -> None:
     ap.add_argument("--sample-variant", type=int, default=1)  # index into BatchedEdgeInflator.SAMPLE_VARIANTS
     ap.add_argument("--check-item-cap", type=int, default=128)
     ap.add_argument("--per-iteration", action="store_true", help="batch: stage times and active slots per iteration")
+    ap.add_argument("--dim", type=int, default=0, choices=[0, 7, 14], help="batch: only 7-DOF or 14-DOF scenes")
+    ap.add_argument("--nets", type=int, default=64, help="mlp: nets in the bank")
+    ap.add_argument("--rows", type=int, default=16384, help="mlp: rows per net")
+    ap.add_argument("--train-steps", type=int, default=32, help="mlp: Adam steps")
     a = ap.parse_args()
     if a.case == "check_points":
         check_points(a.configs, not a.no_cull)
@@ -353,8 +384,10 @@ def main() -> None:
         voxel_check(a.configs, a.voxels)
     elif a.case == "edge_check_ranked":
         edge_check_ranked(a.edges)
+    elif a.case == "mlp":
+        mlp(a.nets, a.rows, a.train_steps)
     else:
-        batch(a.slots, a.iterations, a.sample_variant, a.check_item_cap, a.per_iteration)
+        batch(a.slots, a.iterations, a.sample_variant, a.check_item_cap, a.per_iteration, a.dim)
 
 
 if __name__ == "__main__":

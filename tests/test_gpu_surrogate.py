@@ -151,7 +151,7 @@ def test_ranked_edges_bad_arguments():
 
 
 def test_surrogate_turns_itself_off_where_ordering_cannot_save():
-    """With num_particles = N_0 = 4000 and stop probability 0, the first
+    """With num_particles = N_0 = 4000 and stop probability ~0, the first
     iteration of a slot checks every sample (it cannot hold num_particles
     collisions before its last sample), so ordering saves nothing: each slot
     checks in sample order from its second iteration on and the call
@@ -162,7 +162,7 @@ def test_surrogate_turns_itself_off_where_ordering_cannot_save():
     opt = csd.EizoOptions(num_particles=4000, mixing_steps=20, max_iterations=12)
     plain, cfg_plain, slots, starts, ends = run(None, opt)
     b = csd.BatchedEdgeInflator([S7.plant, S14.plant], opt, max_slots=6, face_capacity=400, autotune_iterations=0)
-    b.set_surrogate(bank, 0.0)
+    b.set_surrogate(bank, 1e-30)  # a slot that is decided inadmissible never stops early
     surr = b.inflate(slots, starts, ends, [DOMS[p] for p in slots])
     for P, R in zip(surr, plain):
         np.testing.assert_array_equal(P.A(), R.A())
