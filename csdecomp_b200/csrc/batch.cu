@@ -191,11 +191,19 @@ __global__ void __launch_bounds__(256, MINB) batch_sample_kernel(BatchArgs a) {
       __syncthreads();
       staged = slot;
     }
-    const float* src = fits ? smf : rows;
-    if (dim <= 8)
-      sample_region<8, KP>(G, src, P, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, gsa);
-    else
-      sample_region<16, KP>(G, src, P, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, gsa);
+    // separate calls for the staged and the global rows, so that the staged face loop reads shared memory
+    // with shared-memory loads (a pointer that may be either would make every load a generic one)
+    if (fits) {
+      if (dim <= 8)
+        sample_region<8, KP>(G, smf, P, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, gsa);
+      else
+        sample_region<16, KP>(G, smf, P, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, gsa);
+    } else {
+      if (dim <= 8)
+        sample_region<8, KP>(G, rows, P, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, gsa);
+      else
+        sample_region<16, KP>(G, rows, P, dim, ls, first, last, a.mixing, a.k0, a.k1, 0u, out, gsa);
+    }
     it = claim_item(&a.it->sample_next);
   }
 }

@@ -51,10 +51,9 @@ __device__ __forceinline__ float log_unit(float u) {
   uint32_t bits = __float_as_uint(u);
   int e = (int)(bits >> 23) - 127;
   float m = __uint_as_float((bits & 0x007fffffu) | 0x3f800000u);
-  if (m > 1.41421353816986083984375f) {
-    m = __fmul_rn(m, 0.5f);
-    e += 1;
-  }
+  const bool hi = m > 1.41421353816986083984375f;  // selects, not a branch (lanes draw different u)
+  m = hi ? __fmul_rn(m, 0.5f) : m;
+  e += hi ? 1 : 0;
   float s = __fdiv_rn(__fsub_rn(m, 1.0f), __fadd_rn(m, 1.0f));
   float s2 = __fmul_rn(s, s);
   float p = __fmaf_rn(s2, 0.0909090936183929443359375f, 0.111111111938953399658203125f);
@@ -91,12 +90,10 @@ __device__ __forceinline__ void sincos_2pi(float v, float* sn, float* cs) {
   pc = __fmaf_rn(x2, pc, 4.1666666666666667e-02f);
   pc = __fmaf_rn(x2, pc, -0.5f);
   float c = __fmaf_rn(x2, pc, 1.0f);
-  switch (qd & 3) {
-    case 0: *sn = s; *cs = c; break;
-    case 1: *sn = c; *cs = -s; break;
-    case 2: *sn = -s; *cs = -c; break;
-    default: *sn = -c; *cs = s; break;
-  }
+  // quadrant qd: (sin, cos) = (s, c), (c, -s), (-s, -c), (-c, s), by selects
+  const float ss = (qd & 1) ? c : s, cc = (qd & 1) ? s : c;
+  *sn = (qd & 2) ? -ss : ss;
+  *cs = ((qd + 1) & 2) ? -cc : cc;
 }
 
 // Direction (dim Gaussians) and the theta uniform of one mixing step.

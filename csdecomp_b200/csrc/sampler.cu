@@ -73,11 +73,18 @@ __global__ void __launch_bounds__(256, 2) sample_region_kernel(const float* __re
     stage_pairs(rows, P, rs, smf);
     __syncthreads();
   }
-  const float* src = fits ? smf : rows;
-  if (dim <= 8)
-    sample_region<8, kRegionKP>(G, src, P, dim, start, first, last, mixing, k0, k1, stream, out, gsa);
-  else
-    sample_region<16, kRegionKP>(G, src, P, dim, start, first, last, mixing, k0, k1, stream, out, gsa);
+  // separate calls for staged and global rows (shared-memory loads in the staged face loop)
+  if (fits) {
+    if (dim <= 8)
+      sample_region<8, kRegionKP>(G, smf, P, dim, start, first, last, mixing, k0, k1, stream, out, gsa);
+    else
+      sample_region<16, kRegionKP>(G, smf, P, dim, start, first, last, mixing, k0, k1, stream, out, gsa);
+  } else {
+    if (dim <= 8)
+      sample_region<8, kRegionKP>(G, rows, P, dim, start, first, last, mixing, k0, k1, stream, out, gsa);
+    else
+      sample_region<16, kRegionKP>(G, rows, P, dim, start, first, last, mixing, k0, k1, stream, out, gsa);
+  }
 }
 
 csd_status_t launch_sample_region(const float* rows, const int* num_faces_dev, int dim, const float* start, int S,

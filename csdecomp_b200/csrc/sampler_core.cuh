@@ -128,12 +128,14 @@ __device__ __forceinline__ void put_faces(const float* __restrict__ A, const flo
   }
 }
 
-// theta bounds of one face (slack s, a . dir = ad): the reference's rule.
+// theta bounds of one face (slack s, a . dir = ad): the reference's rule
+// (ad < 0 raises theta_min to s / ad, ad > 0 lowers theta_max to s / ad, ad = 0
+// bounds nothing), as one IEEE division and two selects, so that lanes whose
+// faces point either way do not split into two division paths.
 __device__ __forceinline__ void theta_bound(float s, float ad, float& tmin, float& tmax) {
-  if (ad < 0.0f)
-    tmin = fmaxf(tmin, __fdiv_rn(s, ad));
-  else if (ad > 0.0f)
-    tmax = fminf(tmax, __fdiv_rn(s, ad));
+  const float q = __fdiv_rn(s, ad != 0.0f ? ad : 1.0f);
+  tmin = ad < 0.0f ? fmaxf(tmin, q) : tmin;
+  tmax = ad > 0.0f ? fminf(tmax, q) : tmax;
 }
 
 // Shared scratch of a group wider than a warp (G = 64, 128, 256 lanes): the
@@ -177,11 +179,14 @@ __device__ __forceinline__ bool run_chain_pairs(const float* __restrict__ rows, 
   constexpr int XL = (MAXD + G - 1) / G;         // position coordinates per lane
   static_assert(G <= 32 || R == 1, "wide groups draw in their first warp");
   const int npairs = (dim + 1) >> 1;
+  // a lane past the last pair in round j holds a copy of pair P - 1 there: its work is the same
+  // as that pair's owner's (so the group's lanes never diverge in the face loop) and a face seen
+  // twice changes no theta bound
   uint64_t s2[KP], a2[KP];
 #pragma unroll
   for (int j = 0; j < KP; ++j) {
-    const int p = gl + G * j;
-    s2[j] = p < P ? *reinterpret_cast<const uint64_t*>(rows + (size_t)p * RS + 2 * MAXD) : 0ull;
+    const int p = min(gl + G * j, P - 1);
+    s2[j] = P > 0 ? *reinterpret_cast<const uint64_t*>(rows + (size_t)p * RS + 2 * MAXD) : 0ull;
     a2[j] = 0ull;  // with nth = -0 the first update leaves every slack as it is
   }
   float nth = -0.0f;
@@ -192,25 +197,21 @@ __device__ __forceinline__ bool run_chain_pairs(const float* __restrict__ rows, 
     for (int r = 0; r < R; ++r) {
       c0[r] = 0.f;
       c1[r] = 0.f;
-      const int job = gl + r * G;
-      if (job <= npairs) {
-        const int word = 2 * job;
-        uint32_t w[4];
-        philox4x32_10((uint32_t)step, chain, stream, (uint32_t)(word >> 2), k0, k1, w);
-        const uint32_t wa = (word & 2) ? w[2] : w[0];
-        const uint32_t wb = (word & 2) ? w[3] : w[1];
-        if (job < npairs) {
-          float u = u01_open0(wa);
-          float v = u01_open1(wb);
-          float rad = __fsqrt_rn(__fmul_rn(-2.0f, log_unit(u)));
-          float sn, cs;
-          sincos_2pi(v, &sn, &cs);
-          c0[r] = __fmul_rn(rad, cs);
-          c1[r] = __fmul_rn(rad, sn);
-        } else {
-          c0[r] = u01_open0(wa);
-        }
-      }
+      // every lane evaluates its job slot without branching (lanes past the last job compute a
+      // value nobody reads), so the group's lanes stay convergent through the draws
+      const int job = min(gl + r * G, npairs);
+      const int word = 2 * job;
+      uint32_t w[4];
+      philox4x32_10((uint32_t)step, chain, stream, (uint32_t)(word >> 2), k0, k1, w);
+      const uint32_t wa = (word & 2) ? w[2] : w[0];
+      const uint32_t wb = (word & 2) ? w[3] : w[1];
+      const float u = u01_open0(wa);
+      const float rad = __fsqrt_rn(__fmul_rn(-2.0f, log_unit(u)));
+      float sn, cs;
+      sincos_2pi(u01_open1(wb), &sn, &cs);
+      const bool gauss = job < npairs;
+      c0[r] = gauss ? __fmul_rn(rad, cs) : u;
+      c1[r] = gauss ? __fmul_rn(rad, sn) : 0.f;
     }
     uint64_t dd[MAXD];  // (dir_k, dir_k)
     float ut;
@@ -246,27 +247,26 @@ __device__ __forceinline__ bool run_chain_pairs(const float* __restrict__ rows, 
     const uint64_t nth2 = f2_pack(nth, nth);
 #pragma unroll
     for (int j = 0; j < KP; ++j) {
-      const int p = gl + G * j;
-      if (p < P) {
-        const uint64_t s = f2_fma(nth2, a2[j], s2[j]);  // the previous step's slack update
-        s2[j] = s;
-        const ulonglong2* row = reinterpret_cast<const ulonglong2*>(rows + (size_t)p * RS);
-        uint64_t acc = 0ull;
+      if (G * j >= P) break;  // no lane of the group holds pair j (uniform across the group)
+      const int p = min(gl + G * j, P - 1);
+      const uint64_t s = f2_fma(nth2, a2[j], s2[j]);  // the previous step's slack update
+      s2[j] = s;
+      const ulonglong2* row = reinterpret_cast<const ulonglong2*>(rows + (size_t)p * RS);
+      uint64_t acc = 0ull;
 #pragma unroll
-        for (int q = 0; q < MAXD / 2; ++q) {
-          if (2 * q < dim) {
-            const ulonglong2 v = row[q];  // coordinates 2q and 2q + 1 of both faces
-            acc = q == 0 ? f2_mul(v.x, dd[0]) : f2_fma(v.x, dd[2 * q], acc);
-            if (2 * q + 1 < dim) acc = f2_fma(v.y, dd[2 * q + 1], acc);
-          }
+      for (int q = 0; q < MAXD / 2; ++q) {
+        if (2 * q < dim) {
+          const ulonglong2 v = row[q];  // coordinates 2q and 2q + 1 of both faces
+          acc = q == 0 ? f2_mul(v.x, dd[0]) : f2_fma(v.x, dd[2 * q], acc);
+          if (2 * q + 1 < dim) acc = f2_fma(v.y, dd[2 * q + 1], acc);
         }
-        a2[j] = acc;
-        float sa, sb, aa, ab;
-        f2_unpack(s, &sa, &sb);
-        f2_unpack(acc, &aa, &ab);
-        theta_bound(sa, aa, tmin, tmax);
-        theta_bound(sb, ab, tmin, tmax);
       }
+      a2[j] = acc;
+      float sa, sb, aa, ab;
+      f2_unpack(s, &sa, &sb);
+      f2_unpack(acc, &aa, &ab);
+      theta_bound(sa, aa, tmin, tmax);
+      theta_bound(sb, ab, tmin, tmax);
     }
     if constexpr (G <= 32) {
 #pragma unroll

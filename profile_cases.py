@@ -5,7 +5,7 @@
       configurations of the 7-DOF arm (80 spheres + 4 capsules) in 200 world
       primitives (with --no-cull every pair is evaluated: the full sweep)
   python profile_cases.py batch [--slots S] [--iterations I] [--dim {7,14}]
-      [--sample-variant V] [--check-item-cap C] [--per-iteration]
+      [--sample-variant V] [--check-item-cap C] [--per-iteration] [--surrogate]
       S inflations of the batched EI-ZO workload (first S scenes), at most I
       iterations, launched stage by stage (profiling mode) with the given
       sampler variant and check work-item cap (defaults: the shapes the
@@ -87,7 +87,7 @@ def check_points(n: int, cull: bool = True) -> None:
 
 
 def batch(slots: int, iterations: int, sample_variant: int, check_item_cap: int, per_iteration: bool = False,
-          dim: int = 0) -> None:
+          dim: int = 0, surrogate: bool = False) -> None:
     import csdecomp_b200 as csd
     from csdecomp_b200 import scenes
     eizo = dict(num_particles=2000, mixing_steps=50, bisection_steps=9, max_hyperplanes_per_iteration=10,
@@ -113,6 +113,12 @@ def batch(slots: int, iterations: int, sample_variant: int, check_item_cap: int,
     b = csd.BatchedEdgeInflator([sc.plant for sc in scs], csd.EizoOptions(**eizo), max_slots=len(scs),
                                 face_capacity=4000, autotune_iterations=0)
     b.set_shapes(sample_variant, check_item_cap)
+    if surrogate:  # one net per scene, 16,384 exact labels each, 2 epochs (the benchmark trains 6)
+        from csdecomp_b200.surrogate import CollisionSurrogate, training_set
+        data = [training_set(sc, [e], 16384, seed=5000 + i) for i, (sc, e) in enumerate(zip(scs, edges))]
+        bank = CollisionSurrogate([sc.dim for sc in scs], seed=5000)
+        bank.train([x for x, _ in data], [y for _, y in data], batch=512, epochs=2, lr=2e-3)
+        b.set_surrogate(bank, 0.01)
     b.set_profiling(True)
     b.inflate(list(range(len(scs))), [e[0] for e in edges], [e[1] for e in edges], doms)
     out = {"case": "batch", "slots": len(scs), "stage_ms": b.stage_ms(), "iterations": b.last_iterations.tolist(),
@@ -364,6 +370,7 @@ def main() -> None:
     ap.add_argument("--check-item-cap", type=int, default=128)
     ap.add_argument("--per-iteration", action="store_true", help="batch: stage times and active slots per iteration")
     ap.add_argument("--dim", type=int, default=0, choices=[0, 7, 14], help="batch: only 7-DOF or 14-DOF scenes")
+    ap.add_argument("--surrogate", action="store_true", help="batch: surrogate-ordered checks (nets trained first)")
     ap.add_argument("--nets", type=int, default=64, help="mlp: nets in the bank")
     ap.add_argument("--rows", type=int, default=16384, help="mlp: rows per net")
     ap.add_argument("--train-steps", type=int, default=32, help="mlp: Adam steps")
@@ -387,7 +394,7 @@ def main() -> None:
     elif a.case == "mlp":
         mlp(a.nets, a.rows, a.train_steps)
     else:
-        batch(a.slots, a.iterations, a.sample_variant, a.check_item_cap, a.per_iteration, a.dim)
+        batch(a.slots, a.iterations, a.sample_variant, a.check_item_cap, a.per_iteration, a.dim, a.surrogate)
 
 
 if __name__ == "__main__":
