@@ -312,7 +312,7 @@ def roofline_point_check(csd, scene, torch, dev, flush):
 # DRAM bytes per launch from ncu captures (profiles/): the full-sweep checker
 # launch (2^20 configurations) and the sampler's launches of one 256-slot step.
 CHECKER_TRAFFIC_BYTES = 29.5e6
-SAMPLER_TRAFFIC_BYTES_PER_STEP = None
+SAMPLER_TRAFFIC_BYTES_PER_STEP = 205.8e6   # 147 launches, 120.0 MB read + 85.8 MB written
 
 
 def check_workloads(csd, torch, dev, flush, cpu: bool):
@@ -580,6 +580,10 @@ def main():
     batched.set_profiling(False)
     sampler_roofline = {"bound": "fp32", "achieved": s_flop / (s_ms * 1e-3) / 1e12, "peak": None, "unit": "TFLOP/s",
                         "frac": None, "traffic": SAMPLER_TRAFFIC_BYTES_PER_STEP,
+                        "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum summed over the sampler "
+                                          "launches of one timed step, one ncu capture "
+                                          "(profiles/batch_sample_kernel_dram_traffic_one_step.md); step basis, "
+                                          "as achieved",
                         "kernel": "batch_sample_kernel (hit-and-run, G lanes per chain, faces staged in shared memory; "
                                   "autotuned variant " + tuned_plain["sample_variant"] + "; regions beyond its "
                                   "staging: " + tuned_plain["large_region_variant"] + ")",
