@@ -89,7 +89,7 @@ EXPORTS = (
     "csd_last_error", "csd_version", "csd_plant_create", "csd_plant_destroy", "csd_plant_info", "csd_plant_status", "csd_plant_wait_selftest", "csd_fk",
     "csd_check_points", "csd_check_edges", "csd_check_edges_ranked", "csd_visibility_graph", "csd_pair_collision_free", "csd_uniform_sample_hpolyhedra",
     "csd_inflator_create", "csd_inflator_inflate", "csd_inflator_points_post_bisection", "csd_inflator_destroy", "csd_eizo", "csd_eizo_noalloc", "csd_edit_regions", "csd_batch_create", "csd_batch_inflate", "csd_batch_configs_checked",
-    "csd_batch_set_profiling", "csd_batch_stage_ms", "csd_batch_iteration_profile", "csd_batch_sample_flops", "csd_batch_last_launches",
+    "csd_batch_set_profiling", "csd_batch_stage_ms", "csd_batch_iteration_profile", "csd_batch_iteration_variants", "csd_batch_sample_flops", "csd_batch_last_launches",
     "csd_batch_autotune", "csd_batch_tuning", "csd_batch_set_shapes", "csd_batch_sample_variants", "csd_batch_shape_counts", "csd_batch_set_surrogate",
     "csd_batch_set_surrogate_rounds",    "csd_batch_destroy",
     "csd_num_samples_unadaptive", "csd_fp32_fma_probe", "csd_plant_flops", "csd_plant_set_culling",

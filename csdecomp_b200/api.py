@@ -725,6 +725,17 @@ class BatchedEdgeInflator:
                                                     ctypes.byref(cnt)))
         return ms, act
 
+    def iteration_variants(self):
+        """(sampler variant index [iterations], most faces of an active region
+        [iterations]) of the last inflate in profiling mode."""
+        cnt = ctypes.c_int32(0)
+        C.check(C.lib().csd_batch_iteration_variants(self._handle, 0, None, None, ctypes.byref(cnt)))
+        var = np.zeros(cnt.value, np.int32)
+        faces = np.zeros(cnt.value, np.int32)
+        C.check(C.lib().csd_batch_iteration_variants(self._handle, cnt.value, C.ptr(var), C.ptr(faces),
+                                                     ctypes.byref(cnt)))
+        return var, faces
+
     def sample_flops(self) -> float:
         """Sampler FLOPs of the last inflate in profiling mode (SAMPLE_FLOP_RULE)."""
         v = ctypes.c_double(0)

@@ -742,6 +742,8 @@ struct csd_batch_s {
   double stage_ms[csd::kStages] = {};
   std::vector<float> iter_ms;   // profiling mode: [iteration][kStages] of the last inflate
   std::vector<int> iter_active; // slots active at the start of each iteration
+  std::vector<int> iter_variant;  // sampler variant each iteration ran
+  std::vector<int> iter_faces;    // most faces of an active slot when each iteration started
   double sample_flop = 0.0;     // profiling mode: sampler FLOPs of the last inflate ((2 d + 4) F per chain step)
   ~csd_batch_s() {
     for (cudaEvent_t e : ev)
@@ -1148,6 +1150,8 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
   }
   h->iter_ms.clear();
   h->iter_active.clear();
+  h->iter_variant.clear();
+  h->iter_faces.clear();
   h->sample_flop = 0.0;
   std::vector<SlotState> prof_slots;
   if (h->profile) prof_slots = slots;  // the records as uploaded: faces of the domain
@@ -1218,10 +1222,15 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
         h->iter_ms.push_back(ms);
       }
       h->iter_active.push_back(active_now);
+      h->iter_variant.push_back(h->run_variant);
       // sampler work of this iteration, from the records before it ran
+      int most = 0;
       for (const SlotState& S : prof_slots)
-        if (!S.done)
+        if (!S.done) {
           h->sample_flop += (double)h->n_tab[S.k] * h->opt.mixing_steps * (2.0 * S.dim + 4.0) * S.nf;
+          most = std::max(most, S.nf);
+        }
+      h->iter_faces.push_back(most);
       CSD_CUDA_TRY(cudaMemcpyAsync(prof_slots.data(), h->slots_dev.ptr, ns * sizeof(SlotState),
                                    cudaMemcpyDeviceToHost, st));
     } else {
@@ -1444,6 +1453,18 @@ csd_status_t csd_batch_iteration_profile(csd_batch_t h, int32_t cap, float* stag
   for (int i = 0; i < std::min(n, (int)cap); ++i) {
     active[i] = h->iter_active[i];
     for (int j = 0; j < kStages; ++j) stage_ms[i * kStages + j] = h->iter_ms[(size_t)i * kStages + j];
+  }
+  return CSD_OK;
+}
+
+csd_status_t csd_batch_iteration_variants(csd_batch_t h, int32_t cap, int32_t* variant, int32_t* max_faces,
+                                          int32_t* count) {
+  CSD_CHECK(h && count && (cap == 0 || (variant && max_faces)), CSD_ERR_INVALID, "null argument");
+  const int n = (int)h->iter_variant.size();
+  *count = n;
+  for (int i = 0; i < std::min(n, (int)cap); ++i) {
+    variant[i] = h->iter_variant[i];
+    max_faces[i] = h->iter_faces[i];
   }
   return CSD_OK;
 }

@@ -245,9 +245,12 @@ static __device__ __forceinline__ void own_sphere(const DevPlant& p, const float
 // Link-level culling of one configuration. Lane k (< num_slots) places its
 // slot's bounding sphere in the world; `link` (lane k) has bit j set when the
 // spheres of slots k and j overlap, `stat` (lane g) has bit i set when static
-// 32 g + i overlaps some slot sphere. The spheres are padded on the host, so a
-// culled pair is separated by at least 1e-4 m. With culling off every bit is
-// set.
+// 32 g + i overlaps some slot sphere. Statics are tested in groups of 32: the
+// slots whose spheres overlap the group's sphere are found by one ballot, and
+// each static of the group is tested against those slots only (none: the
+// group is culled without a static test). The spheres are padded on the host
+// (the group spheres once more), so a culled pair is separated by at least
+// 1e-4 m. With culling off every bit is set.
 struct Cull {
   uint32_t link;
   uint32_t stat;
@@ -258,7 +261,8 @@ static __device__ __forceinline__ Cull broad_phase(const DevPlant& p, const floa
   // the staged region continues after the aligned boxes: static spheres, slot spheres, geometry slots
   const float4* sbs = aabb + 2 * p.num_sabox;
   const float4* slb = sbs + p.num_static;
-  Cull c{~0u, ~0u, reinterpret_cast<const uint8_t*>(slb + p.num_slots)};
+  const float4* gbs = slb + p.num_slots;
+  Cull c{~0u, ~0u, reinterpret_cast<const uint8_t*>(gbs + (p.num_static + kWarp - 1) / kWarp)};
   if (!p.cull) return c;
   float cx = 0.f, cy = 0.f, cz = 0.f, cr = -1.f;
   if (lane < p.num_slots) {
@@ -280,17 +284,25 @@ static __device__ __forceinline__ Cull broad_phase(const DevPlant& p, const floa
   c.link = lw;
   uint32_t sw = 0;
   for (int g = 0; g * kWarp < p.num_static; ++g) {
-    const int st = g * kWarp + lane;
-    float4 S = make_float4(0.f, 0.f, 0.f, -1.f);
-    if (st < p.num_static) S = sbs[st];
-    bool near = false;
-    for (int k = 0; k < p.num_slots; ++k) {
-      const float kx = __shfl_sync(kFull, cx, k), ky = __shfl_sync(kFull, cy, k), kz = __shfl_sync(kFull, cz, k);
-      const float kr = __shfl_sync(kFull, cr, k);
-      const float dx = kx - S.x, dy = ky - S.y, dz = kz - S.z, t = kr + S.w;
-      near |= kr >= 0.f && S.w >= 0.f && !(fmaf(dz, dz, fmaf(dy, dy, dx * dx)) > t * t);
+    const float4 B = gbs[g];
+    const float bx = cx - B.x, by = cy - B.y, bz = cz - B.z, bt = cr + B.w;
+    uint32_t km = __ballot_sync(kFull, cr >= 0.f && B.w >= 0.f && !(fmaf(bz, bz, fmaf(by, by, bx * bx)) > bt * bt));
+    uint32_t bits = 0u;
+    if (km) {  // uniform across the warp
+      const int st = g * kWarp + lane;
+      float4 S = make_float4(0.f, 0.f, 0.f, -1.f);
+      if (st < p.num_static) S = sbs[st];
+      bool near = false;
+      while (km) {
+        const int k = __ffs(km) - 1;
+        km &= km - 1u;
+        const float kx = __shfl_sync(kFull, cx, k), ky = __shfl_sync(kFull, cy, k), kz = __shfl_sync(kFull, cz, k);
+        const float kr = __shfl_sync(kFull, cr, k);
+        const float dx = kx - S.x, dy = ky - S.y, dz = kz - S.z, t = kr + S.w;
+        near |= S.w >= 0.f && !(fmaf(dz, dz, fmaf(dy, dy, dx * dx)) > t * t);
+      }
+      bits = __ballot_sync(kFull, near);
     }
-    const uint32_t bits = __ballot_sync(kFull, near);
     if (lane == g) sw = bits;
   }
   c.stat = sw;
@@ -538,6 +550,53 @@ static __device__ bool generic_segment(const DevPlant& p, const float4* stat, co
   return false;
 }
 
+// One moving-moving segment by link-pair runs: lane r takes run r of a chunk
+// of 32 and reads the overlap bit of its two slots; the warp then sweeps the
+// pairs of each stretch of consecutive overlapping runs (adjacent in the pair
+// list) as one range, one pair per lane. A run of culled slots costs no
+// pair-index load and no per-pair test; with culling off a chunk is one range.
+template <int TA, int TB>
+static __device__ bool generic_runs(const DevPlant& p, const float* pose, const GenSeg& sg, int lane,
+                                    const Cull& cu) {
+  for (int r0 = sg.run_begin; r0 < sg.run_end; r0 += kWarp) {
+    const int r = r0 + lane;
+    PairRun pr{0, 0, 0, 0};
+    if (r < sg.run_end) pr = p.runs[r];
+    const bool keep = ((__shfl_sync(kFull, cu.link, pr.sa & 31) >> (pr.sb & 31)) & 1u) && r < sg.run_end;
+    uint32_t km = __ballot_sync(kFull, keep);
+    while (km) {
+      const int j = __ffs(km) - 1;
+      const uint32_t t = km >> j;  // the stretch of set bits from j
+      const int len = t == 0xffffffffu ? kWarp : __ffs(~t) - 1;
+      km = len == kWarp ? 0u : km & ~(((1u << len) - 1u) << j);
+      const int b0 = __shfl_sync(kFull, pr.begin, j), b1 = __shfl_sync(kFull, pr.end, j + len - 1);
+      for (int base = b0; base < b1; base += kWarp) {
+        const int k = base + lane;
+        bool hit = false;
+        if (k < b1) {
+          const GenericPair gp = p.generic[k];
+          float A[Words<TA>::n], B[Words<TB>::n];
+          const float4* pa = reinterpret_cast<const float4*>(pose + pose_offset(p, (int)gp.a));
+#pragma unroll
+          for (int i = 0; i < Words<TA>::n / 4; ++i) {
+            float4 v = pa[i];
+            A[4 * i] = v.x; A[4 * i + 1] = v.y; A[4 * i + 2] = v.z; A[4 * i + 3] = v.w;
+          }
+          const float4* pb = reinterpret_cast<const float4*>(pose + pose_offset(p, (int)gp.b));
+#pragma unroll
+          for (int i = 0; i < Words<TB>::n / 4; ++i) {
+            float4 v = pb[i];
+            B[4 * i] = v.x; B[4 * i + 1] = v.y; B[4 * i + 2] = v.z; B[4 * i + 3] = v.w;
+          }
+          hit = pair_hit(TA, A, TB, B);
+        }
+        if (__any_sync(kFull, hit)) return true;
+      }
+    }
+  }
+  return false;
+}
+
 // Capsule x box segment with a broad phase: a lane tests its pair's capsule
 // bounding sphere (centre, radius + half length) against the box; pairs that
 // pass are compacted into a warp-wide batch (lane r of the batch holds the
@@ -625,15 +684,15 @@ static __device__ bool sweep_generic(const DevPlant& p, const float4* stat, cons
     bool h = false;
     switch (key) {
       // moving-moving
-      case G_SPHERE * 4 + G_CAPSULE: h = generic_segment<G_SPHERE, G_CAPSULE, false>(p, stat, pose, sg, lane, cu); break;
-      case G_SPHERE * 4 + G_BOX: h = generic_segment<G_SPHERE, G_BOX, false>(p, stat, pose, sg, lane, cu); break;
-      case G_CAPSULE * 4 + G_CAPSULE: h = generic_segment<G_CAPSULE, G_CAPSULE, false>(p, stat, pose, sg, lane, cu); break;
+      case G_SPHERE * 4 + G_CAPSULE: h = generic_runs<G_SPHERE, G_CAPSULE>(p, pose, sg, lane, cu); break;
+      case G_SPHERE * 4 + G_BOX: h = generic_runs<G_SPHERE, G_BOX>(p, pose, sg, lane, cu); break;
+      case G_CAPSULE * 4 + G_CAPSULE: h = generic_runs<G_CAPSULE, G_CAPSULE>(p, pose, sg, lane, cu); break;
       case G_CAPSULE * 4 + G_BOX: h = cap_box_segment<false>(p, stat, pose, sg, lane, cu); break;
-      case G_BOX * 4 + G_BOX: h = generic_segment<G_BOX, G_BOX, false>(p, stat, pose, sg, lane, cu); break;
-      case G_BOX * 4 + G_SPHERE: h = generic_segment<G_BOX, G_SPHERE, false>(p, stat, pose, sg, lane, cu); break;
-      case G_BOX * 4 + G_CAPSULE: h = generic_segment<G_BOX, G_CAPSULE, false>(p, stat, pose, sg, lane, cu); break;
-      case G_CAPSULE * 4 + G_SPHERE: h = generic_segment<G_CAPSULE, G_SPHERE, false>(p, stat, pose, sg, lane, cu); break;
-      case G_SPHERE * 4 + G_SPHERE: h = generic_segment<G_SPHERE, G_SPHERE, false>(p, stat, pose, sg, lane, cu); break;
+      case G_BOX * 4 + G_BOX: h = generic_runs<G_BOX, G_BOX>(p, pose, sg, lane, cu); break;
+      case G_BOX * 4 + G_SPHERE: h = generic_runs<G_BOX, G_SPHERE>(p, pose, sg, lane, cu); break;
+      case G_BOX * 4 + G_CAPSULE: h = generic_runs<G_BOX, G_CAPSULE>(p, pose, sg, lane, cu); break;
+      case G_CAPSULE * 4 + G_SPHERE: h = generic_runs<G_CAPSULE, G_SPHERE>(p, pose, sg, lane, cu); break;
+      case G_SPHERE * 4 + G_SPHERE: h = generic_runs<G_SPHERE, G_SPHERE>(p, pose, sg, lane, cu); break;
       // moving-static
       case 16 + G_CAPSULE * 4 + G_SPHERE: h = generic_segment<G_CAPSULE, G_SPHERE, true>(p, stat, pose, sg, lane, cu); break;
       case 16 + G_CAPSULE * 4 + G_BOX: h = cap_box_segment<true>(p, stat, pose, sg, lane, cu); break;

@@ -66,7 +66,13 @@ struct GenericPair {  // a: moving index; b: bit 31 set = static geometry, low b
 
 struct GenSeg {       // generic pairs [begin, end) share (type a, type b, b static)
   int begin, end, ta, tb;
-  int b_static, pad0, pad1, pad2;
+  int b_static;
+  int run_begin, run_end;  // moving-moving segments: link-pair runs [run_begin, run_end) of the segment
+  int pad0;
+};
+
+struct PairRun {      // generic pairs [begin, end) whose moving geometries lie on slots sa and sb
+  int begin, end, sa, sb;
 };
 
 struct TileInfo {     // moving spheres [32*t, 32*t+32) against static geometries
@@ -104,8 +110,10 @@ struct DevPlant {
   const MovingGeom* moving;
   const float4* statics;       // [num_static][4] float4 (WG format); followed by aabb
   const float4* aabb;          // [num_sabox][2]: [p 0 | h 0] of axis-aligned static boxes; followed by
-                               // [num_static] static bounding spheres (world centre, radius), then the
-                               // slot spheres and the geometry slots below (one staged region)
+                               // [num_static] static bounding spheres (world centre, radius), the slot
+                               // spheres, [ceil(num_static / 32)] group spheres (each enclosing the
+                               // bounding spheres of statics 32 g .. 32 g + 31) and the geometry slots
+                               // below (one staged region)
   const float4* slot_bs;       // [num_slots] bounding sphere of each slot's geometry (slot frame); radius < 0: none
   const uint8_t* moving_slot;  // [num_moving] slot of each moving geometry
   const int* static_type;      // [num_static]
@@ -113,6 +121,7 @@ struct DevPlant {
   const TileEntry* entries;
   const GenericPair* generic;
   const GenSeg* segs;
+  const PairRun* runs;
   const int* link_slot;        // [num_links] slot of each reference link (-1 world, -2 unreachable)
   const float* link_fixed;     // [num_links][12] slot->link (R col-major 9, t 3); world links: world pose
   int* status;                 // device error word: nonzero after a bounded wait gave up

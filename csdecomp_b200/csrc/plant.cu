@@ -53,6 +53,17 @@ int device_sm_count() {
 
 namespace {
 
+// Bits 0..9 of v spread to bits 0, 3, 6, ..., 27 (one coordinate of a 30-bit
+// Morton code).
+uint32_t spread10(uint32_t v) {
+  v &= 1023u;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
 struct X4 {  // rigid transform in FP64: R column-major, t
   double R[9];
   double t[3];
@@ -332,6 +343,30 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   std::vector<int> mov_order(mov_sph);
   mov_order.insert(mov_order.end(), mov_cap.begin(), mov_cap.end());
   mov_order.insert(mov_order.end(), mov_box.begin(), mov_box.end());
+  // Statics of each class in the Morton order of their world positions, so
+  // that the broad phase's groups of 32 consecutive statics are spatially
+  // compact and a group sphere far from every link culls the whole group.
+  // (Which static comes first changes no verdict: a configuration collides
+  // if any pair does.)
+  {
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (const std::vector<int>* lst : {&st_sph, &st_box, &st_cap})
+      for (int g : *lst)
+        for (int a = 0; a < 3; ++a) {
+          lo[a] = std::min(lo[a], gX[g].t[a]);
+          hi[a] = std::max(hi[a], gX[g].t[a]);
+        }
+    auto code = [&](int g) {
+      uint32_t c = 0;
+      for (int a = 0; a < 3; ++a) {
+        const double u = hi[a] > lo[a] ? (gX[g].t[a] - lo[a]) / (hi[a] - lo[a]) : 0.0;
+        c |= spread10((uint32_t)std::min(1023.0, std::max(0.0, u * 1023.0))) << a;
+      }
+      return c;
+    };
+    for (std::vector<int>* lst : {&st_sph, &st_box, &st_cap})
+      std::stable_sort(lst->begin(), lst->end(), [&](int x, int y) { return code(x) < code(y); });
+  }
   // world boxes whose axes are exactly the world axes get the aligned fast path
   std::vector<int> st_abox, st_rbox;
   for (int g : st_box) {
@@ -445,6 +480,7 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
     return slot_of_ref(x.b) < slot_of_ref(y.b);
   });
   std::vector<GenSeg> segs;
+  std::vector<PairRun> runs;  // moving-moving segments split where the (slot a, slot b) pair changes
   for (size_t i = 0; i < generic.size();) {
     size_t j = i;
     while (j < generic.size() && seg_key(generic[j]) == seg_key(generic[i])) ++j;
@@ -454,6 +490,16 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
     sg.ta = type_of_ref(generic[i].a);
     sg.tb = type_of_ref(generic[i].b);
     sg.b_static = (int)(generic[i].b >> 31);
+    sg.run_begin = (int)runs.size();
+    if (!sg.b_static)
+      for (size_t r = i; r < j;) {
+        size_t e = r;
+        const int sa = slot_of_ref(generic[r].a), sb = slot_of_ref(generic[r].b);
+        while (e < j && slot_of_ref(generic[e].a) == sa && slot_of_ref(generic[e].b) == sb) ++e;
+        runs.push_back({(int)r, (int)e, sa, sb});
+        r = e;
+      }
+    sg.run_end = (int)runs.size();
     segs.push_back(sg);
     i = j;
   }
@@ -572,6 +618,26 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
     for (int a = 0; a < 3; ++a) static_bs[4 * st + a] = (float)c[a];
     static_bs[4 * st + 3] = (float)(rad * (1 + 1e-6) + 1e-4);
   }
+  // group spheres: one per 32 consecutive statics, enclosing their bounding
+  // spheres (FP64, padded again by a relative 1e-6 and 1e-4 m)
+  const int NG = (S + kWarp - 1) / kWarp;
+  std::vector<float> group_bs((size_t)std::max(NG, 0) * 4, 0.f);
+  for (int g = 0; g < NG; ++g) {
+    const int s0 = g * kWarp, s1 = std::min(S, s0 + kWarp);
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300}, c[3], rad = 0;
+    for (int st = s0; st < s1; ++st)
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = std::min(lo[a], (double)static_bs[4 * st + a] - static_bs[4 * st + 3]);
+        hi[a] = std::max(hi[a], (double)static_bs[4 * st + a] + static_bs[4 * st + 3]);
+      }
+    for (int a = 0; a < 3; ++a) c[a] = 0.5 * (lo[a] + hi[a]);
+    for (int st = s0; st < s1; ++st) {
+      const double dx = static_bs[4 * st] - c[0], dy = static_bs[4 * st + 1] - c[1], dz = static_bs[4 * st + 2] - c[2];
+      rad = std::max(rad, std::sqrt(dx * dx + dy * dy + dz * dz) + static_bs[4 * st + 3]);
+    }
+    for (int a = 0; a < 3; ++a) group_bs[4 * g + a] = (float)c[a];
+    group_bs[4 * g + 3] = (float)(rad * (1 + 1e-6) + 1e-4);
+  }
   std::vector<uint8_t> moving_slot(std::max<size_t>(hp.moving.size(), 1), 0);
   for (size_t m = 0; m < hp.moving.size(); ++m) moving_slot[m] = (uint8_t)hp.moving[m].slot;
 
@@ -593,16 +659,19 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   };
   size_t o_fk = section(fk.size() * sizeof(FkJoint));
   size_t o_mv = section(hp.moving.size() * sizeof(MovingGeom));
-  // staged region: statics | aligned boxes | static spheres | slot spheres | geometry slots (16-byte padded)
+  // staged region: statics | aligned boxes | static spheres | slot spheres | group spheres | geometry slots
+  // (16-byte padded)
   const size_t ms_bytes = (moving_slot.size() + 15) & ~size_t(15);
   const size_t static_bytes = hp.statics.size() * sizeof(float) + aabb.size() * sizeof(float) +
-                              static_bs.size() * sizeof(float) + slot_bs.size() * sizeof(float) + ms_bytes;
+                              static_bs.size() * sizeof(float) + slot_bs.size() * sizeof(float) +
+                              group_bs.size() * sizeof(float) + ms_bytes;
   size_t o_st = section(static_bytes);
   size_t o_sty = section(hp.static_type.size() * sizeof(int));
   size_t o_ti = section(tiles.size() * sizeof(TileInfo));
   size_t o_en = section(entries.size() * sizeof(TileEntry));
   size_t o_ge = section(generic.size() * sizeof(GenericPair));
   size_t o_sg = section(segs.size() * sizeof(GenSeg));
+  size_t o_ru = section(runs.size() * sizeof(PairRun));
   size_t o_status = section(16);
   size_t o_ls = section(link_slot.size() * sizeof(int));
   size_t o_lf = section(link_fixed.size() * sizeof(float));
@@ -616,15 +685,18 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   put(o_st + hp.statics.size() * sizeof(float), aabb.data(), aabb.size() * sizeof(float));
   const size_t o_sph = o_st + (hp.statics.size() + aabb.size()) * sizeof(float);
   const size_t o_slb = o_sph + static_bs.size() * sizeof(float);
-  const size_t o_msl = o_slb + slot_bs.size() * sizeof(float);
+  const size_t o_gbs = o_slb + slot_bs.size() * sizeof(float);
+  const size_t o_msl = o_gbs + group_bs.size() * sizeof(float);
   put(o_sph, static_bs.data(), static_bs.size() * sizeof(float));
   put(o_slb, slot_bs.data(), slot_bs.size() * sizeof(float));
+  put(o_gbs, group_bs.data(), group_bs.size() * sizeof(float));
   put(o_msl, moving_slot.data(), moving_slot.size());
   put(o_sty, hp.static_type.data(), hp.static_type.size() * sizeof(int));
   put(o_ti, tiles.data(), tiles.size() * sizeof(TileInfo));
   put(o_en, entries.data(), entries.size() * sizeof(TileEntry));
   put(o_ge, generic.data(), generic.size() * sizeof(GenericPair));
   put(o_sg, segs.data(), segs.size() * sizeof(GenSeg));
+  put(o_ru, runs.data(), runs.size() * sizeof(PairRun));
   put(o_ls, link_slot.data(), link_slot.size() * sizeof(int));
   put(o_lf, link_fixed.data(), link_fixed.size() * sizeof(float));
   CSD_CUDA_TRY(cudaMalloc(&h->blob, off));
@@ -667,6 +739,7 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   dp.entries = (const TileEntry*)(base + o_en);
   dp.generic = (const GenericPair*)(base + o_ge);
   dp.segs = (const GenSeg*)(base + o_sg);
+  dp.runs = (const PairRun*)(base + o_ru);
   dp.status = (int*)(base + o_status);
   dp.link_slot = (const int*)(base + o_ls);
   dp.link_fixed = (const float*)(base + o_lf);

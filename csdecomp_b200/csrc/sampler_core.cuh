@@ -197,8 +197,12 @@ __device__ __forceinline__ bool run_chain_pairs(const float* __restrict__ rows, 
     for (int r = 0; r < R; ++r) {
       c0[r] = 0.f;
       c1[r] = 0.f;
-      // every lane evaluates its job slot without branching (lanes past the last job compute a
-      // value nobody reads), so the group's lanes stay convergent through the draws
+      // rounds past the last job are skipped and wide groups draw in their first warp (both
+      // uniform across a warp); within a round every lane evaluates its job slot without
+      // branching (lanes past the last job compute a value nobody reads), so the group's lanes
+      // stay convergent through the draws
+      if (r > 0 && r * G > npairs) continue;
+      if (G > 32 && gl >= 32) continue;
       const int job = min(gl + r * G, npairs);
       const int word = 2 * job;
       uint32_t w[4];

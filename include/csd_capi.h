@@ -364,6 +364,11 @@ csd_status_t csd_batch_tuning(csd_batch_t h, int32_t* sample_variant, int32_t* c
  * receives the number of iterations (at most cap are written). */
 csd_status_t csd_batch_iteration_profile(csd_batch_t h, int32_t cap, float* stage_ms, int32_t* active,
                                          int32_t* count);
+/* Profiling mode, last csd_batch_inflate: per iteration the sampler variant
+ * it ran (index as in csd_batch_set_shapes) and the most faces of a region
+ * active when it started; *count receives the number of iterations. */
+csd_status_t csd_batch_iteration_variants(csd_batch_t h, int32_t cap, int32_t* variant, int32_t* max_faces,
+                                          int32_t* count);
 /* Profiling mode, last csd_batch_inflate: algorithmic FLOPs of the sampling
  * stage, (2 d + 4) F per chain and mixing step (a . dir, the slack update and
  * the two theta-bound compares per face; FMA = 2, division not counted),

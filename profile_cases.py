@@ -9,7 +9,8 @@
       S inflations of the batched EI-ZO workload (first S scenes), at most I
       iterations, launched stage by stage (profiling mode) with the given
       sampler variant and check work-item cap (defaults: the shapes the
-      autotuner picks on a B200)
+      autotuner picks on a B200; --sample-variant -1: autotuned over the first
+      4 iterations, with the variant switch on region growth)
 
   python profile_cases.py point_check [--configs N]
       config 1: 7-DOF arm, 40 spheres, 20 world boxes; N uniform configurations
@@ -111,8 +112,9 @@ def batch(slots: int, iterations: int, sample_variant: int, check_item_cap: int,
         d.MakeBox(sc.lower(), sc.upper())
         doms.append(d)
     b = csd.BatchedEdgeInflator([sc.plant for sc in scs], csd.EizoOptions(**eizo), max_slots=len(scs),
-                                face_capacity=4000, autotune_iterations=0)
-    b.set_shapes(sample_variant, check_item_cap)
+                                face_capacity=4000, autotune_iterations=0 if sample_variant >= 0 else 4)
+    if sample_variant >= 0:
+        b.set_shapes(sample_variant, check_item_cap)
     if surrogate:  # one net per scene, 16,384 exact labels each, 2 epochs (the benchmark trains 6)
         from csdecomp_b200.surrogate import CollisionSurrogate, training_set
         data = [training_set(sc, [e], 16384, seed=5000 + i) for i, (sc, e) in enumerate(zip(scs, edges))]
@@ -122,11 +124,14 @@ def batch(slots: int, iterations: int, sample_variant: int, check_item_cap: int,
     b.set_profiling(True)
     b.inflate(list(range(len(scs))), [e[0] for e in edges], [e[1] for e in edges], doms)
     out = {"case": "batch", "slots": len(scs), "stage_ms": b.stage_ms(), "iterations": b.last_iterations.tolist(),
-           "sample_flop": b.sample_flops(), "sample_variant": b.SAMPLE_VARIANTS[sample_variant]}
+           "sample_flop": b.sample_flops(),
+           "sample_variant": b.SAMPLE_VARIANTS[sample_variant] if sample_variant >= 0 else b.tuning()}
     if per_iteration:
         ms, act = b.iteration_profile()
+        var, faces = b.iteration_variants()
         out["per_iteration"] = {"active": act.tolist(), "total_ms": ms.sum(1).round(3).tolist(),
-                                "stages": list(b.STAGES), "stage_ms": ms.round(3).tolist()}
+                                "stages": list(b.STAGES), "stage_ms": ms.round(3).tolist(),
+                                "variant": var.tolist(), "max_faces": faces.tolist()}
     print(json.dumps(out))
 
 
@@ -366,7 +371,7 @@ def main() -> None:
     ap.add_argument("--collisions", type=int, default=512, help="edit_regions: collisions per region")
     ap.add_argument("--voxels", type=int, default=10000, help="voxel_check: voxels")
     ap.add_argument("--iterations", type=int, default=12)
-    ap.add_argument("--sample-variant", type=int, default=1)  # index into BatchedEdgeInflator.SAMPLE_VARIANTS
+    ap.add_argument("--sample-variant", type=int, default=1)  # index into SAMPLE_VARIANTS; -1: autotune
     ap.add_argument("--check-item-cap", type=int, default=128)
     ap.add_argument("--per-iteration", action="store_true", help="batch: stage times and active slots per iteration")
     ap.add_argument("--dim", type=int, default=0, choices=[0, 7, 14], help="batch: only 7-DOF or 14-DOF scenes")
