@@ -138,12 +138,17 @@ __device__ __forceinline__ void theta_bound(float s, float ad, float& tmin, floa
   tmax = ad > 0.0f ? fminf(tmax, q) : tmax;
 }
 
+// Steps whose draws a group computes at once (when its drawing lanes hold
+// that many steps' jobs).
+constexpr int kDrawSteps = 4;
+
 // Shared scratch of a group wider than a warp (G = 64, 128, 256 lanes): the
-// step's direction and theta uniform, and each warp's partial theta bounds,
-// double buffered by step parity (a warp cannot run two steps ahead of the
-// group's barriers).
+// directions and theta uniforms of a batch of drawn steps (coordinates 0..15,
+// the uniform at 16), double buffered by batch parity, and each warp's
+// partial theta bounds, double buffered by step parity (a warp cannot run two
+// steps, or two batches, ahead of the group's barriers).
 struct GroupScratch {
-  float dir[2][17];
+  float dir[2][kDrawSteps][17];
   float red[2][8][2];
 };
 constexpr int kMaxWideGroups = 4;  // 256 threads / 64 lanes
@@ -162,23 +167,37 @@ __host__ __device__ __forceinline__ int pair_group_width(int g, int P, int KP) {
 // One chain run by a group of G lanes over a region of P face pairs (staged in
 // shared memory or read from global memory). Lane gl holds pairs gl + G j
 // (j < KP) and their slacks and a . dir values in registers, and coordinates
-// gl + G r of the position (xl). The draws are the serial chain's: job j <
-// ceil(dim/2) is Gaussian pair j, job ceil(dim/2) the theta uniform, lane gl
-// drawing jobs gl, gl + G, ...; the direction is broadcast by shuffles (G <=
-// 32) or through GroupScratch (wider groups, named barrier bar_id). The theta
-// bounds are max/min reductions, which do not depend on the order, so every
-// chain ends bit for bit where the oracle's serial chain ends whatever G.
-// A chain whose line search fails keeps stepping without moving (the group's
-// lanes stay convergent) and returns false.
+// gl + G r of the position (xl). The draws are the serial chain's: a step has
+// J = ceil(dim/2) + 1 jobs (job j < ceil(dim/2) is Gaussian pair j, the last
+// the theta uniform). The group's drawing lanes (all of a group of up to 32,
+// the first warp of a wider one) draw S = min(kDrawSteps, lanes / J) steps at
+// once: slot q = gl + r lanes is job q % J of step offset q / J, so Gaussian
+// pair p of offset t lies on lane t J + p of round 0. The direction reaches
+// the group by shuffles (G <= 32) or through GroupScratch (wider groups, named
+// barrier bar_id). The theta bounds are max/min reductions, which do not
+// depend on the order, so every chain ends bit for bit where the oracle's
+// serial chain ends whatever G. A chain whose line search fails keeps stepping
+// without moving (the group's lanes stay convergent) and returns false.
 template <int MAXD, int G, int KP>
 __device__ __forceinline__ bool run_chain_pairs(const float* __restrict__ rows, int P, int dim, int mixing,
                                                 uint32_t k0, uint32_t k1, uint32_t chain, uint32_t stream,
                                                 float* xl, int gl, GroupScratch* gs, int bar_id) {
   constexpr int RS = 2 * MAXD + 4;
-  constexpr int R = (MAXD / 2 + 1 + G - 1) / G;  // job rounds per lane
-  constexpr int XL = (MAXD + G - 1) / G;         // position coordinates per lane
+  constexpr int GD = G < 32 ? G : 32;             // drawing lanes
+  constexpr int R = (MAXD / 2 + 1 + GD - 1) / GD;  // draw rounds per lane (one step's jobs)
+  constexpr int XL = (MAXD + G - 1) / G;           // position coordinates per lane
   static_assert(G <= 32 || R == 1, "wide groups draw in their first warp");
-  const int npairs = (dim + 1) >> 1;
+  static_assert(MAXD / 2 <= GD, "Gaussian pairs of one step fit in round 0");
+  const int npairs = (dim + 1) >> 1, J = npairs + 1;
+  const int S = min(kDrawSteps, max(1, GD / J));  // steps drawn at once (uniform)
+  // this lane's draw slots: step offset and job of slot gl + r GD
+  int tq[R], jq[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int q = gl + r * GD;
+    tq[r] = q / J;
+    jq[r] = q - tq[r] * J;
+  }
   // a lane past the last pair in round j holds a copy of pair P - 1 there: its work is the same
   // as that pair's owner's (so the group's lanes never diverge in the face loop) and a face seen
   // twice changes no theta bound
@@ -191,55 +210,65 @@ __device__ __forceinline__ bool run_chain_pairs(const float* __restrict__ rows, 
   }
   float nth = -0.0f;
   bool ok = true;
+  float c0[R], c1[R];
+  int t = 0, batch = -1;  // step offset within the drawn batch, batch parity
   for (int step = 0; step < mixing; ++step) {
-    float c0[R], c1[R];
+    if (t == 0) {
+      ++batch;
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      c0[r] = 0.f;
-      c1[r] = 0.f;
-      // rounds past the last job are skipped and wide groups draw in their first warp (both
-      // uniform across a warp); within a round every lane evaluates its job slot without
-      // branching (lanes past the last job compute a value nobody reads), so the group's lanes
-      // stay convergent through the draws
-      if (r > 0 && r * G > npairs) continue;
-      if (G > 32 && gl >= 32) continue;
-      const int job = min(gl + r * G, npairs);
-      const int word = 2 * job;
-      uint32_t w[4];
-      philox4x32_10((uint32_t)step, chain, stream, (uint32_t)(word >> 2), k0, k1, w);
-      const uint32_t wa = (word & 2) ? w[2] : w[0];
-      const uint32_t wb = (word & 2) ? w[3] : w[1];
-      const float u = u01_open0(wa);
-      const float rad = __fsqrt_rn(__fmul_rn(-2.0f, log_unit(u)));
-      float sn, cs;
-      sincos_2pi(u01_open1(wb), &sn, &cs);
-      const bool gauss = job < npairs;
-      c0[r] = gauss ? __fmul_rn(rad, cs) : u;
-      c1[r] = gauss ? __fmul_rn(rad, sn) : 0.f;
+      for (int r = 0; r < R; ++r) {
+        c0[r] = 0.f;
+        c1[r] = 0.f;
+        // rounds past the batch's last slot are skipped and wide groups draw in their first warp
+        // (both uniform across a warp); within a round every lane evaluates its slot without
+        // branching (lanes past the last slot compute a value nobody reads), so the group's lanes
+        // stay convergent through the draws
+        if (r > 0 && r * GD >= S * J) continue;
+        if (G > 32 && gl >= 32) continue;
+        const int job = jq[r];
+        const int word = 2 * job;
+        uint32_t w[4];
+        philox4x32_10((uint32_t)(step + tq[r]), chain, stream, (uint32_t)(word >> 2), k0, k1, w);
+        const uint32_t wa = (word & 2) ? w[2] : w[0];
+        const uint32_t wb = (word & 2) ? w[3] : w[1];
+        const float u = u01_open0(wa);
+        const float rad = __fsqrt_rn(__fmul_rn(-2.0f, log_unit(u)));
+        float sn, cs;
+        sincos_2pi(u01_open1(wb), &sn, &cs);
+        const bool gauss = job < npairs;
+        c0[r] = gauss ? __fmul_rn(rad, cs) : u;
+        c1[r] = gauss ? __fmul_rn(rad, sn) : 0.f;
+      }
+      if constexpr (G > 32) {
+        if (gl < S * J) {  // the first warp's lanes (S J <= 32)
+          float* db = gs->dir[batch & 1][tq[0]];
+          if (jq[0] < npairs) {
+            db[2 * jq[0]] = c0[0];
+            db[2 * jq[0] + 1] = c1[0];
+          } else {
+            db[16] = c0[0];
+          }
+        }
+      }
     }
-    uint64_t dd[MAXD];  // (dir_k, dir_k)
+    const int base = t * J;  // lane of this step's Gaussian pair 0
+    uint64_t dd[MAXD];       // (dir_k, dir_k)
     float ut;
     if constexpr (G <= 32) {
 #pragma unroll
       for (int k = 0; k < MAXD; ++k) {
-        const int p = k >> 1;
-        const float dk = __shfl_sync(0xffffffffu, (k & 1) ? c1[p / G] : c0[p / G], p % G, G);
+        const float dk = __shfl_sync(0xffffffffu, (k & 1) ? c1[0] : c0[0], base + (k >> 1), G);
         dd[k] = f2_pack(dk, dk);
       }
+      const int q = base + npairs;  // the theta uniform's slot
       float utv = c0[0];
 #pragma unroll
       for (int r = 1; r < R; ++r)
-        if (npairs / G == r) utv = c0[r];
-      ut = __shfl_sync(0xffffffffu, utv, npairs % G, G);
+        if (q / G == r) utv = c0[r];
+      ut = __shfl_sync(0xffffffffu, utv, q % G, G);
     } else {
-      float* db = gs->dir[step & 1];
-      if (gl < npairs) {
-        db[2 * gl] = c0[0];
-        db[2 * gl + 1] = c1[0];
-      } else if (gl == npairs) {
-        db[16] = c0[0];
-      }
-      group_bar(bar_id, G);
+      const float* db = gs->dir[batch & 1][t];
+      if (t == 0) group_bar(bar_id, G);  // the batch's draws are in scratch
 #pragma unroll
       for (int k = 0; k < MAXD; ++k) {
         const float dk = db[k];  // entries past dim are never used
@@ -299,22 +328,31 @@ __device__ __forceinline__ bool run_chain_pairs(const float* __restrict__ rows, 
       }
     }
     if (isinf(tmax) || isinf(tmin) || tmax < tmin) ok = false;
+    // this step's direction at the position coordinates the lane holds (coordinate k is half k & 1
+    // of Gaussian pair k >> 1: lane base + (k >> 1), round 0)
+    float dkl[XL];
+#pragma unroll
+    for (int r = 0; r < XL; ++r) {
+      const int k = min(gl + G * r, MAXD - 1);
+      if constexpr (G <= 32) {
+        const float v0 = __shfl_sync(0xffffffffu, c0[0], base + (k >> 1), G);
+        const float v1 = __shfl_sync(0xffffffffu, c1[0], base + (k >> 1), G);
+        dkl[r] = (k & 1) ? v1 : v0;
+      } else {
+        dkl[r] = gs->dir[batch & 1][t][k];
+      }
+    }
     nth = -0.0f;
     if (ok) {
       double th = __dadd_rn(__dmul_rn((double)ut, __dsub_rn(__dmul_rn(0.999999, (double)tmax), (double)tmin)),
                             (double)tmin);
       const float theta = __double2float_rn(th);
 #pragma unroll
-      for (int r = 0; r < XL; ++r) {
-        const int k = gl + G * r;
-        float dk = 0.f, hi;
-#pragma unroll
-        for (int kk = 0; kk < MAXD; ++kk)
-          if (kk == k) f2_unpack(dd[kk], &dk, &hi);
-        if (k < dim) xl[r] = __fmaf_rn(theta, dk, xl[r]);
-      }
+      for (int r = 0; r < XL; ++r)
+        if (gl + G * r < dim) xl[r] = __fmaf_rn(theta, dkl[r], xl[r]);
       nth = -theta;
     }
+    t = t + 1 == S ? 0 : t + 1;
   }
   return ok;
 }
