@@ -720,6 +720,10 @@ struct csd_batch_s {
   int tune_iters = 0;                               // iterations of the next inflate to tune on
   double tune_ms[csd::kNumSampleVariants + csd::kNumCheckVariants] = {};
   int tuned_iters = 0;
+  // large regions: the first time a region outgrows the tuned variant's staging, the next
+  // iteration times every sampler variant on its own inputs (kept until the next autotune)
+  bool large_pending = false, large_tuned = false;
+  double large_ms[csd::kNumSampleVariants] = {};
   std::vector<int> n_tab, m_tab;
   std::vector<float> thr_tab;
   csd::DevBuf plants_dev, slots_dev, tabs, fpool, bpool, iter, act, fin;
@@ -774,10 +778,11 @@ size_t slot_floats(const csd_batch_s* h) {
 // fastest by tuning time among those whose staging buffer holds them, else
 // the one with the most room (faces beyond it are read from global memory).
 int variant_for(const csd_batch_s* h, int nf8, int nf16) {
+  const double* ms = h->large_tuned ? h->large_ms : h->tune_ms;
   int best = -1;
   for (int v = 0; v < kNumSampleVariants; ++v) {
     const SampleVariant& cv = kSampleVariants[v];
-    if (cv.f8 >= nf8 && cv.f16 >= nf16 && (best < 0 || h->tune_ms[v] < h->tune_ms[best])) best = v;
+    if (cv.f8 >= nf8 && cv.f16 >= nf16 && (best < 0 || ms[v] < ms[best])) best = v;
   }
   if (best >= 0) return best;
   best = 0;
@@ -785,7 +790,7 @@ int variant_for(const csd_batch_s* h, int nf8, int nf16) {
     const SampleVariant &cv = kSampleVariants[v], &bv = kSampleVariants[best];
     const bool roomier = cv.f16 > bv.f16 || (cv.f16 == bv.f16 && cv.f8 > bv.f8);
     const bool same = cv.f16 == bv.f16 && cv.f8 == bv.f8;
-    if (roomier || (same && h->tune_ms[v] < h->tune_ms[best])) best = v;
+    if (roomier || (same && ms[v] < ms[best])) best = v;
   }
   return best;
 }
@@ -1158,7 +1163,39 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
   std::vector<int> fin;
   int active_now = ns;
   for (;;) {
-    if (h->tune_iters > 0) {
+    if (h->large_pending && h->tune_iters == 0) {
+      // regions outgrew the tuned variant's staging for the first time: every sampler variant
+      // on this iteration's inputs (the stage is idempotent), then the rest of the iteration;
+      // the fastest samples the large regions from here on
+      h->large_pending = false;
+      std::vector<cudaEvent_t> tev(2 * kNumSampleVariants);
+      for (cudaEvent_t& e : tev) CSD_CUDA_TRY(cudaEventCreate(&e));
+      for (int v = 0; v < kNumSampleVariants; ++v) {
+        cudaMemsetAsync(&a.it->sample_next, 0, sizeof(int), st);
+        cudaEventRecord(tev[2 * v], st);
+        kSampleVariants[v].fn<<<h->sample_grid[v], 256, kSampleVariants[v].smem, st>>>(a);
+        cudaEventRecord(tev[2 * v + 1], st);
+        ++h->launches;
+      }
+      h->launches += launch_iteration(h, ns, a, st, nullptr, true);
+      CSD_CUDA_TRY(cudaGetLastError());
+      CSD_CUDA_TRY(cudaStreamSynchronize(st));
+      int best = 0;
+      for (int v = 0; v < kNumSampleVariants; ++v) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, tev[2 * v], tev[2 * v + 1]);
+        h->large_ms[v] = ms;
+        if (ms < h->large_ms[best]) best = v;
+      }
+      for (cudaEvent_t& e : tev) cudaEventDestroy(e);
+      h->large_tuned = true;
+      h->large_variant = best;
+      h->run_variant = best;
+      if ((s = build_graph(h, ns, a))) return s;
+      if (h->profile)
+        CSD_CUDA_TRY(cudaMemcpyAsync(prof_slots.data(), h->slots_dev.ptr, ns * sizeof(SlotState),
+                                     cudaMemcpyDeviceToHost, st));
+    } else if (h->tune_iters > 0) {
       // every sampler variant and check item size on this iteration's inputs
       // (both stages are idempotent: a rerun writes the same samples and
       // verdicts), then the rest of the iteration as usual
@@ -1287,11 +1324,16 @@ csd_status_t csd_batch_inflate(csd_batch_t h, int32_t n, const int32_t* slot_pla
       a.mlp_wb = nullptr;
       if ((s = build_graph(h, ns, a))) return s;
     }
-    // a slot's region outgrew the staging buffer of the running variant: continue with the
-    // fastest variant that stages it (identical samples; the graph is captured again)
-    if (h->switch_large && h->tune_iters == 0) {
+    // a slot's region outgrew the staging buffer of the running variant: the first time, time
+    // every variant on the next iteration; after that, continue with the fastest variant (by
+    // those times) that stages it (identical samples; the graph is captured again)
+    if (h->switch_large && h->tune_iters == 0 && !h->large_pending) {
       const SampleVariant& rv = kSampleVariants[h->run_variant];
       if (h->host_iter->max_nf8 > rv.f8 || h->host_iter->max_nf16 > rv.f16) {
+        if (!h->large_tuned) {
+          h->large_pending = true;
+          continue;
+        }
         const int v = variant_for(h, h->host_iter->max_nf8, h->host_iter->max_nf16);
         if (v != h->run_variant) {
           h->run_variant = v;
@@ -1350,6 +1392,9 @@ csd_status_t csd_batch_autotune(csd_batch_t h, int32_t iterations) {
   h->tune_iters = iterations;
   h->tuned_iters = 0;
   for (double& x : h->tune_ms) x = 0.0;
+  h->large_tuned = false;
+  h->large_pending = false;
+  for (double& x : h->large_ms) x = 0.0;
   return CSD_OK;
 }
 

@@ -345,10 +345,13 @@ csd_status_t csd_batch_set_shapes(csd_batch_t h, int32_t sample_variant, int32_t
 /* Each sampler variant stages a slot's region (face-pair rows) in shared
  * memory up to a face count set by its blocks per SM (1: 5120 faces for dim
  * <= 8, 2844 above; 2: 2662 / 1478; 3: 1740 / 966); larger regions are read
- * from global memory through L1. After tuning, once an active slot outgrows
- * the running variant's staging, the iterations continue with the fastest
- * variant (by tuning time) that stages the largest active region, else the
- * roomiest (the graph is captured once more per switch). tuned / large /
+ * from global memory through L1. After tuning, the first time an active slot
+ * outgrows the running variant's staging, the next iteration times every
+ * variant on its own inputs and the fastest runs from then on (kept for later
+ * calls until csd_batch_autotune); when a region outgrows that variant's
+ * staging too, the iterations continue with the fastest variant (by those
+ * times) that stages the largest active region, else the roomiest (the graph
+ * is captured once more per switch). tuned / large /
  * last_run: the tuned variant, the one the last switch chose for large
  * regions (before any switch: the one it would choose), the one the last
  * iteration ran. */
