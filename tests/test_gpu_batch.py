@@ -147,3 +147,34 @@ def test_queued_inflations_refill_slots():
     # the handle serves a later call with fewer inflations than slots
     again = small.inflate(slots[:2], [e[0] for e in edges[:2]], [e[1] for e in edges[:2]], doms[:2])
     np.testing.assert_array_equal(again[0].A(), got[0].A())
+
+
+def test_large_region_variant_timing_keeps_regions():
+    """A two-arm inflation of the benchmark workload whose region grows past
+    1,000 faces (10 per iteration for about 126 iterations): an autotuned
+    batch times every sampler variant once the region outgrows the tuned
+    variant's staging and continues with the fastest, and the region stays
+    the one a batch with a fixed variant yields, bit for bit."""
+    i = 111  # the workload's two-arm scene whose seed edge (seed 3000 + 101 i) inflates longest
+    sc = scenes.batch_scene(i, scenes.batch_scene_seeds(4 * 64 + 64)[i])
+    e = scenes.seed_edges(sc, 1, 3000 + 101 * i, lambda q: csd.CheckCollisionFreeCuda(q.T, sc.plant),
+                          lambda a, b: csd.CheckEdgesCollisionFreeCuda(a.T, b.T, sc.plant))
+    assert e
+    opt = csd.EizoOptions(num_particles=2000, mixing_steps=50, bisection_steps=9, max_hyperplanes_per_iteration=10,
+                          epsilon=0.01, delta=0.05, tau=0.5, max_iterations=500, configuration_margin=0.01, seed=1337)
+    tuned = csd.BatchedEdgeInflator([sc.plant], opt, max_slots=1, face_capacity=4000, autotune_iterations=2)
+    tuned.set_profiling(True)
+    got = tuned.inflate([0], [e[0][0]], [e[0][1]], [box(sc)])[0]
+    var, faces = tuned.iteration_variants()
+    fixed = csd.BatchedEdgeInflator([sc.plant], opt, max_slots=1, face_capacity=4000, autotune_iterations=0)
+    fixed.set_shapes(2, 32)
+    ref = fixed.inflate([0], [e[0][0]], [e[0][1]], [box(sc)])[0]
+    np.testing.assert_array_equal(got.A(), ref.A())
+    np.testing.assert_array_equal(got.b(), ref.b())
+    assert int(tuned.last_iterations[0]) == int(fixed.last_iterations[0])
+    assert faces.max() > 1000 and got.A().shape[0] > 1000
+    t = tuned.tuning()
+    names = list(csd.BatchedEdgeInflator.SAMPLE_VARIANTS)
+    staged = {0: 2844, 1: 1478, 2: 966, 3: 2844, 4: 1478}  # faces each variant stages at dim > 8
+    if faces.max() > staged[names.index(t["sample_variant"])]:
+        assert len(set(var.tolist())) >= 2 and t["large_region_variant"] in names
