@@ -94,15 +94,15 @@ __device__ __forceinline__ uint64_t f2_fma(uint64_t a, uint64_t b, uint64_t c) {
 // face 2p + h at float 2k + h (k < MAXD, zero past dim), the two start slacks
 // at 2 MAXD and 2 MAXD + 1, then two unused floats: 2 MAXD + 4 floats, a
 // multiple of 16 bytes. A face that does not exist yet (the partner of the
-// last face of an odd count) is a zero row: its a . dir is zero, so it bounds
-// nothing and its slack never changes. One 16-byte load brings two
+// last face of an odd count) holds a copy of that face: it bounds theta
+// exactly as the face does, so it changes no bound. One 16-byte load brings two
 // coordinates of both faces, and one packed FMA (fma.rn.f32x2, each half an
 // IEEE round-to-nearest FMA) advances both faces' dot products.
 __host__ __device__ constexpr int pair_maxd(int dim) { return dim <= 8 ? 8 : 16; }
 __host__ __device__ constexpr int pair_stride(int dim) { return 2 * pair_maxd(dim) + 4; }
 
 // Writes face f (coordinates a[0..dim), offset b) of a region whose chains
-// start at x0. An even f also clears its partner half.
+// start at x0. An even f also fills its partner half with a copy of itself.
 __device__ __forceinline__ void put_face(float* __restrict__ rows, int dim, int f, const float* a, float b,
                                          const float* __restrict__ x0) {
   const int md = pair_maxd(dim), h = f & 1;
@@ -111,9 +111,9 @@ __device__ __forceinline__ void put_face(float* __restrict__ rows, int dim, int 
   for (int k = 1; k < dim; ++k) ax = __fmaf_rn(a[k], x0[k], ax);
   for (int k = 0; k < md; ++k) r[2 * k + h] = k < dim ? a[k] : 0.f;
   r[2 * md + h] = __fsub_rn(b, ax);
-  if (!h) {
-    for (int k = 0; k < md; ++k) r[2 * k + 1] = 0.f;
-    r[2 * md + 1] = 0.f;
+  if (!h) {  // until face f + 1 is written, its half repeats face f (a face seen twice bounds nothing new)
+    for (int k = 0; k < md; ++k) r[2 * k + 1] = r[2 * k];
+    r[2 * md + 1] = r[2 * md];
   }
 }
 
@@ -131,9 +131,12 @@ __device__ __forceinline__ void put_faces(const float* __restrict__ A, const flo
 // theta bounds of one face (slack s, a . dir = ad): the reference's rule
 // (ad < 0 raises theta_min to s / ad, ad > 0 lowers theta_max to s / ad, ad = 0
 // bounds nothing), as one IEEE division and two selects, so that lanes whose
-// faces point either way do not split into two division paths.
+// faces point either way do not split into two division paths. For ad = 0
+// (either sign) the quotient is infinite or NaN and neither select takes it;
+// the rows hold no zero faces (an unpaired face is repeated), so that case,
+// which takes the division's slow path, only arises when a . dir is exactly 0.
 __device__ __forceinline__ void theta_bound(float s, float ad, float& tmin, float& tmax) {
-  const float q = __fdiv_rn(s, ad != 0.0f ? ad : 1.0f);
+  const float q = __fdiv_rn(s, ad);
   tmin = ad < 0.0f ? fmaxf(tmin, q) : tmin;
   tmax = ad > 0.0f ? fminf(tmax, q) : tmax;
 }
