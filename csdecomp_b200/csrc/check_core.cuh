@@ -248,7 +248,9 @@ static __device__ __forceinline__ void own_sphere(const DevPlant& p, const float
 // 32 g + i overlaps some slot sphere. Statics are tested in groups of 32: the
 // slots whose spheres overlap the group's sphere are found by one ballot, and
 // each static of the group is tested against those slots only (none: the
-// group is culled without a static test). The spheres are padded on the host
+// group is culled without a static test); a slot that cannot reach any static
+// of the group in any configuration (host reach masks) is not among them. The
+// spheres are padded on the host
 // (the group spheres once more), so a culled pair is separated by at least
 // 1e-4 m. With culling off every bit is set.
 struct Cull {
@@ -262,7 +264,9 @@ static __device__ __forceinline__ Cull broad_phase(const DevPlant& p, const floa
   const float4* sbs = aabb + 2 * p.num_sabox;
   const float4* slb = sbs + p.num_static;
   const float4* gbs = slb + p.num_slots;
-  Cull c{~0u, ~0u, reinterpret_cast<const uint8_t*>(gbs + (p.num_static + kWarp - 1) / kWarp)};
+  const int ng = (p.num_static + kWarp - 1) / kWarp;
+  const uint32_t* gmk = reinterpret_cast<const uint32_t*>(gbs + ng);  // per group: slots that can reach it
+  Cull c{~0u, ~0u, reinterpret_cast<const uint8_t*>(gmk + ((ng + 3) & ~3))};
   if (!p.cull) return c;
   float cx = 0.f, cy = 0.f, cz = 0.f, cr = -1.f;
   if (lane < p.num_slots) {
@@ -286,7 +290,10 @@ static __device__ __forceinline__ Cull broad_phase(const DevPlant& p, const floa
   for (int g = 0; g * kWarp < p.num_static; ++g) {
     const float4 B = gbs[g];
     const float bx = cx - B.x, by = cy - B.y, bz = cz - B.z, bt = cr + B.w;
-    uint32_t km = __ballot_sync(kFull, cr >= 0.f && B.w >= 0.f && !(fmaf(bz, bz, fmaf(by, by, bx * bx)) > bt * bt));
+    // a slot that cannot reach the group is skipped (unless its pose is NaN, which is near everything)
+    const bool reach = ((gmk[g] >> lane) & 1u) || !(cx == cx && cy == cy && cz == cz);
+    uint32_t km = __ballot_sync(kFull, cr >= 0.f && B.w >= 0.f && reach &&
+                                           !(fmaf(bz, bz, fmaf(by, by, bx * bx)) > bt * bt));
     uint32_t bits = 0u;
     if (km) {  // uniform across the warp
       const int st = g * kWarp + lane;

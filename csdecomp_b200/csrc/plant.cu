@@ -638,6 +638,52 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
     for (int a = 0; a < 3; ++a) group_bs[4 * g + a] = (float)c[a];
     group_bs[4 * g + 3] = (float)(rad * (1 + 1e-6) + 1e-4);
   }
+  // Reach masks: for any configuration, slot k's bounding sphere stays within
+  // reach[k] of a world-fixed point root[k] (its chain's first joint origin; a
+  // child frame's origin lies |t| from its parent's, whatever the revolute
+  // angles; a prismatic joint's travel is unbounded, so its subtree gets no
+  // bound). A static whose sphere is farther from root[k] than reach[k] plus its
+  // radius can never be near slot k; group g's mask holds the slots that can
+  // reach some member, and the broad phase tests the others against no static
+  // of the group (padded as the spheres; verdicts unchanged).
+  std::vector<uint32_t> group_mask((size_t)std::max(NG, 0), 0u);
+  {
+    std::vector<double> reach(NSL, 0.0), root((size_t)NSL * 3, 0.0);
+    std::vector<char> bounded(NSL, 1);
+    for (int k = 0; k < NSL; ++k) {
+      const FkJoint& f = fk[k];
+      const double tl = std::sqrt((double)f.t[0] * f.t[0] + (double)f.t[1] * f.t[1] + (double)f.t[2] * f.t[2]);
+      if (f.parent < 0) {
+        for (int a = 0; a < 3; ++a) root[3 * k + a] = f.t[a];
+        reach[k] = 0.0;
+        bounded[k] = f.type != J_PRISMATIC;
+      } else {
+        for (int a = 0; a < 3; ++a) root[3 * k + a] = root[3 * f.parent + a];
+        reach[k] = reach[f.parent] + tl;
+        bounded[k] = bounded[f.parent] && f.type != J_PRISMATIC;
+      }
+    }
+    for (int g = 0; g < NG; ++g)
+      for (int st = g * kWarp; st < std::min(S, g * kWarp + kWarp); ++st)
+        for (int k = 0; k < NSL; ++k) {
+          if (slot_bs[4 * k + 3] < 0.f) continue;  // no geometry on the slot
+          if (!bounded[k]) {
+            group_mask[g] |= 1u << k;
+            continue;
+          }
+          const double ck = std::sqrt((double)slot_bs[4 * k] * slot_bs[4 * k] +
+                                      (double)slot_bs[4 * k + 1] * slot_bs[4 * k + 1] +
+                                      (double)slot_bs[4 * k + 2] * slot_bs[4 * k + 2]);
+          double d2 = 0.0;
+          for (int a = 0; a < 3; ++a) {
+            const double x = (double)static_bs[4 * st + a] - root[3 * k + a];
+            d2 += x * x;
+          }
+          const double lim = (reach[k] + ck + slot_bs[4 * k + 3] + static_bs[4 * st + 3]) * (1 + 1e-6) + 1e-4;
+          if (std::sqrt(d2) <= lim) group_mask[g] |= 1u << k;
+        }
+  }
+  const size_t gm_bytes = ((size_t)std::max(NG, 0) * sizeof(uint32_t) + 15) & ~size_t(15);
   std::vector<uint8_t> moving_slot(std::max<size_t>(hp.moving.size(), 1), 0);
   for (size_t m = 0; m < hp.moving.size(); ++m) moving_slot[m] = (uint8_t)hp.moving[m].slot;
 
@@ -659,12 +705,12 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   };
   size_t o_fk = section(fk.size() * sizeof(FkJoint));
   size_t o_mv = section(hp.moving.size() * sizeof(MovingGeom));
-  // staged region: statics | aligned boxes | static spheres | slot spheres | group spheres | geometry slots
-  // (16-byte padded)
+  // staged region: statics | aligned boxes | static spheres | slot spheres | group spheres | group reach
+  // masks | geometry slots (16-byte padded)
   const size_t ms_bytes = (moving_slot.size() + 15) & ~size_t(15);
   const size_t static_bytes = hp.statics.size() * sizeof(float) + aabb.size() * sizeof(float) +
                               static_bs.size() * sizeof(float) + slot_bs.size() * sizeof(float) +
-                              group_bs.size() * sizeof(float) + ms_bytes;
+                              group_bs.size() * sizeof(float) + gm_bytes + ms_bytes;
   size_t o_st = section(static_bytes);
   size_t o_sty = section(hp.static_type.size() * sizeof(int));
   size_t o_ti = section(tiles.size() * sizeof(TileInfo));
@@ -686,10 +732,12 @@ csd_status_t csd_plant_create(const csd_plant_desc_t* d, csd_plant_t* out) {
   const size_t o_sph = o_st + (hp.statics.size() + aabb.size()) * sizeof(float);
   const size_t o_slb = o_sph + static_bs.size() * sizeof(float);
   const size_t o_gbs = o_slb + slot_bs.size() * sizeof(float);
-  const size_t o_msl = o_gbs + group_bs.size() * sizeof(float);
+  const size_t o_gmk = o_gbs + group_bs.size() * sizeof(float);
+  const size_t o_msl = o_gmk + gm_bytes;
   put(o_sph, static_bs.data(), static_bs.size() * sizeof(float));
   put(o_slb, slot_bs.data(), slot_bs.size() * sizeof(float));
   put(o_gbs, group_bs.data(), group_bs.size() * sizeof(float));
+  put(o_gmk, group_mask.data(), group_mask.size() * sizeof(uint32_t));
   put(o_msl, moving_slot.data(), moving_slot.size());
   put(o_sty, hp.static_type.data(), hp.static_type.size() * sizeof(int));
   put(o_ti, tiles.data(), tiles.size() * sizeof(TileInfo));
