@@ -949,8 +949,7 @@ csd_status_t csd_batch_create(const csd_plant_t* plants, int32_t num_plants, int
   h->check_grid = g1;
   h->bisect_grid = g2;
   for (int v = 0; v < kNumSampleVariants; ++v) {
-    CSD_CUDA_TRY(cudaFuncSetAttribute(kSampleVariants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kSampleVariants[v].smem));
+    CSD_CUDA_TRY(raise_smem_limit(kSampleVariants[v].fn, (int)kSampleVariants[v].smem));
     int per_sm = 0;
     CSD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kSampleVariants[v].fn, 256,
                                                              kSampleVariants[v].smem));
@@ -1425,10 +1424,8 @@ csd_status_t csd_batch_set_surrogate(csd_batch_t h, csd_mlp_t mlp, float stop_pr
   if ((s = h->scores.reserve((size_t)h->max_slots * h->n_max * 4)) ||
       (s = h->order.reserve((size_t)h->max_slots * h->n_max * 4)))
     return s;
-  CSD_CUDA_TRY(cudaFuncSetAttribute(batch_score_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)mlp::kFwdSmem));
-  CSD_CUDA_TRY(cudaFuncSetAttribute(batch_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(kSortMax * sizeof(unsigned long long))));
+  CSD_CUDA_TRY(raise_smem_limit(batch_score_kernel, (int)mlp::kFwdSmem));
+  CSD_CUDA_TRY(raise_smem_limit(batch_sort_kernel, (int)(kSortMax * sizeof(unsigned long long))));
   h->mlp = mlp;
   h->stop_logit = std::log(stop_probability / (1.f - stop_probability));
   return CSD_OK;

@@ -921,7 +921,7 @@ static inline size_t smem_bytes(const csd_plant_s* p, int wpb) {
 template <typename K>
 static csd_status_t grid_for(K kernel, size_t smem, int64_t work_warps, int* grid, int wpb) {
   int per_sm = 0;
-  CSD_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CSD_CUDA_TRY(raise_smem_limit(kernel, (int)smem));
   CSD_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32 * wpb, smem));
   if (per_sm <= 0) {
     set_error("plant tables do not fit in shared memory");

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -150,6 +151,23 @@ csd_status_t launch_put_faces(const float* A, const float* b, int F, int dim, co
                               cudaStream_t st);
 
 int device_sm_count();
+
+// Raises a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes`, never lowering it: handles and calls with different plants
+// launch the same kernels with different shared-memory sizes, and a lower
+// limit set by one (another handle, another thread) would make the others'
+// launches fail.
+template <typename K>
+inline cudaError_t raise_smem_limit(K kernel, size_t bytes) {
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  cudaFuncAttributes fa{};
+  cudaError_t e = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(kernel));
+  if (e != cudaSuccess) return e;
+  if ((size_t)fa.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+  return cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)bytes);
+}
 
 // The surrogate bank's device tensors (mlp.cu): bf16 weights, f32 parameters,
 // input scale, and the input dimension of each net.

@@ -159,8 +159,7 @@ csd_status_t launch_gemm(const GemmArgs& g, int groups, cudaStream_t st) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 64 || !attr[dev]) {
-    CSD_CUDA_TRY(cudaFuncSetAttribute(gemm_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)gemm_smem<NT>()));
+    CSD_CUDA_TRY(raise_smem_limit(gemm_kernel<NT>, (int)gemm_smem<NT>()));
     if (dev < 64) attr[dev] = true;
   }
   dim3 grid((g.M + 127) / 128, (g.N + NT - 1) / NT, groups);
@@ -202,7 +201,7 @@ csd_status_t launch_forward(const FwdArgs& a, int groups, int max_rows, cudaStre
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 64 || !attr[dev]) {
-    CSD_CUDA_TRY(cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem));
+    CSD_CUDA_TRY(raise_smem_limit(mlp_forward_kernel, (int)kFwdSmem));
     if (dev < 64) attr[dev] = true;
   }
   if (groups <= 0 || max_rows <= 0) return CSD_OK;

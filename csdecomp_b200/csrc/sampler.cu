@@ -95,8 +95,7 @@ csd_status_t launch_sample_region(const float* rows, const int* num_faces_dev, i
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 64 || !attr_set[dev]) {
-    CSD_CUDA_TRY(cudaFuncSetAttribute(sample_region_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kRegionStageBytes));
+    CSD_CUDA_TRY(raise_smem_limit(sample_region_kernel, (int)kRegionStageBytes));
     if (dev < 64) attr_set[dev] = true;
   }
   const int sms = device_sm_count();

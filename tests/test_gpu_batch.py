@@ -58,6 +58,42 @@ def test_batch_matches_single_inflations():
     np.testing.assert_array_equal(got2[1].A(), got[1].A())
 
 
+def test_batches_with_different_plants_coexist():
+    """Two batches whose plants need different amounts of shared memory per
+    block: creating the smaller one after the larger one leaves the larger
+    one's launches valid (a kernel's shared-memory limit only rises), also when
+    the two run at once from two threads, and each region equals its single
+    inflation."""
+    import threading
+    big = scenes.arm_scene(41, num_spheres=80, num_capsules=4, num_world_boxes=150, num_world_spheres=150,
+                           keepout=0.8)
+    small = scenes.arm_scene(42, num_spheres=20, num_world_boxes=5, num_world_spheres=5, keepout=0.8)
+    opt = csd.EizoOptions(num_particles=300, mixing_steps=10, max_iterations=8)
+    eb, es = free_edges(big, 2, 0.2, 3), free_edges(small, 2, 0.2, 4)
+    hb = csd.BatchedEdgeInflator([big.plant], opt, max_slots=2, face_capacity=200, autotune_iterations=2)
+    hs = csd.BatchedEdgeInflator([small.plant], opt, max_slots=2, face_capacity=200, autotune_iterations=2)
+    out = {}
+
+    def run(name, h, sc, e):
+        out[name] = h.inflate([0, 0], [x[0] for x in e], [x[1] for x in e], [box(sc)] * 2)
+
+    run("big", hb, big, eb)
+    run("small", hs, small, es)
+    threads = [threading.Thread(target=run, args=("big2", hb, big, eb)),
+               threading.Thread(target=run, args=("small2", hs, small, es))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for name, sc, e in (("big", big, eb), ("small", small, es)):
+        for i in range(2):
+            inf = csd.CudaEdgeInflator(sc.plant, sc.inspector.robot_geometry_ids, opt, box(sc), face_capacity=200)
+            ref = inf.inflateEdge(e[i][0], e[i][1], None, 0.0, verbose=False)
+            for got in (out[name][i], out[name + "2"][i]):
+                np.testing.assert_array_equal(got.A(), ref.A(), err_msg=f"{name} {i}")
+                np.testing.assert_array_equal(got.b(), ref.b(), err_msg=f"{name} {i}")
+
+
 def test_batch_rejects_segment_outside_domain():
     s7 = scenes.arm_scene(31, num_spheres=20, num_world_boxes=10, keepout=0.8)
     batch = csd.BatchedEdgeInflator([s7.plant], csd.EizoOptions(num_particles=100, max_iterations=5), 2, 100)
