@@ -142,7 +142,7 @@ static __device__ __forceinline__ int claim_item(int* counter) {
 template <int MINB>
 struct SampleStage {
   static constexpr size_t bytes = (MINB == 1 ? 200 : MINB == 2 ? 104 : 68) * size_t(1024);
-  static_assert(MINB * (bytes + 3072) <= 227 * 1024, "MINB staging buffers fit one SM");
+  static_assert(MINB * (bytes + 5120) <= 227 * 1024, "MINB staging buffers fit one SM");
 };
 
 // ------------------------------------------------------------------ kernels

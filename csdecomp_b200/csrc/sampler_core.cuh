@@ -143,7 +143,7 @@ __device__ __forceinline__ void theta_bound(float s, float ad, float& tmin, floa
 
 // Steps whose draws a group computes at once (when its drawing lanes hold
 // that many steps' jobs).
-constexpr int kDrawSteps = 4;
+constexpr int kDrawSteps = 8;
 
 // Shared scratch of a group wider than a warp (G = 64, 128, 256 lanes): the
 // directions and theta uniforms of a batch of drawn steps (coordinates 0..15,
@@ -170,37 +170,31 @@ __host__ __device__ __forceinline__ int pair_group_width(int g, int P, int KP) {
 // One chain run by a group of G lanes over a region of P face pairs (staged in
 // shared memory or read from global memory). Lane gl holds pairs gl + G j
 // (j < KP) and their slacks and a . dir values in registers, and coordinates
-// gl + G r of the position (xl). The draws are the serial chain's: a step has
-// J = ceil(dim/2) + 1 jobs (job j < ceil(dim/2) is Gaussian pair j, the last
-// the theta uniform). The group's drawing lanes (all of a group of up to 32,
-// the first warp of a wider one) draw S = min(kDrawSteps, lanes / J) steps at
-// once: slot q = gl + r lanes is job q % J of step offset q / J, so Gaussian
-// pair p of offset t lies on lane t J + p of round 0. The direction reaches
-// the group by shuffles (G <= 32) or through GroupScratch (wider groups, named
-// barrier bar_id). The theta bounds are max/min reductions, which do not
-// depend on the order, so every chain ends bit for bit where the oracle's
-// serial chain ends whatever G. A chain whose line search fails keeps stepping
-// without moving (the group's lanes stay convergent) and returns false.
+// gl + G r of the position (xl). The draws are the serial chain's: step s
+// reads words 0 .. 2 ceil(dim/2) of its stream (Gaussian pair j from words 2j
+// and 2j + 1, the theta uniform from word 2 ceil(dim/2)), four words per
+// Philox block. A drawing slot is one block: both its Box-Muller pairs (or a
+// pair and the theta uniform). A step has JB = ceil(dim/2) / 2 + 1 blocks; the
+// group's drawing lanes (all of a group of up to 32, the first warp of a wider
+// one) draw S = min(kDrawSteps, lanes / JB) steps at once, slot q = gl holding
+// block q % JB of step offset q / JB, so Gaussian pair p of offset t lies on
+// lane t JB + p / 2. The direction reaches the group by shuffles (G <= 32) or
+// through GroupScratch (wider groups, named barrier bar_id). The theta bounds
+// are max/min reductions, which do not depend on the order, so every chain
+// ends bit for bit where the oracle's serial chain ends whatever G. A chain
+// whose line search fails keeps stepping without moving (the group's lanes
+// stay convergent) and returns false.
 template <int MAXD, int G, int KP>
 __device__ __forceinline__ bool run_chain_pairs(const float* __restrict__ rows, int P, int dim, int mixing,
                                                 uint32_t k0, uint32_t k1, uint32_t chain, uint32_t stream,
                                                 float* xl, int gl, GroupScratch* gs, int bar_id) {
   constexpr int RS = 2 * MAXD + 4;
-  constexpr int GD = G < 32 ? G : 32;             // drawing lanes
-  constexpr int R = (MAXD / 2 + 1 + GD - 1) / GD;  // draw rounds per lane (one step's jobs)
-  constexpr int XL = (MAXD + G - 1) / G;           // position coordinates per lane
-  static_assert(G <= 32 || R == 1, "wide groups draw in their first warp");
-  static_assert(MAXD / 2 <= GD, "Gaussian pairs of one step fit in round 0");
-  const int npairs = (dim + 1) >> 1, J = npairs + 1;
-  const int S = min(kDrawSteps, max(1, GD / J));  // steps drawn at once (uniform)
-  // this lane's draw slots: step offset and job of slot gl + r GD
-  int tq[R], jq[R];
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const int q = gl + r * GD;
-    tq[r] = q / J;
-    jq[r] = q - tq[r] * J;
-  }
+  constexpr int GD = G < 32 ? G : 32;    // drawing lanes
+  constexpr int XL = (MAXD + G - 1) / G;  // position coordinates per lane
+  static_assert(MAXD / 4 + 1 <= GD, "one step's blocks fit the drawing lanes");
+  const int npairs = (dim + 1) >> 1, JB = (npairs >> 1) + 1;
+  const int S = min(kDrawSteps, GD / JB);  // steps drawn at once (uniform)
+  const int tq = gl / JB, bq = gl - tq * JB;  // this lane's slot: step offset, block
   // a lane past the last pair in round j holds a copy of pair P - 1 there: its work is the same
   // as that pair's owner's (so the group's lanes never diverge in the face loop) and a face seen
   // twice changes no theta bound
@@ -213,62 +207,62 @@ __device__ __forceinline__ bool run_chain_pairs(const float* __restrict__ rows, 
   }
   float nth = -0.0f;
   bool ok = true;
-  float c0[R], c1[R];
+  // this lane's block: pair 2 bq (c0a, c1a) and pair 2 bq + 1 (c0b, c1b); where a pair index
+  // reaches npairs its c0 holds the theta uniform instead
+  float c0a = 0.f, c1a = 0.f, c0b = 0.f, c1b = 0.f;
   int t = 0, batch = -1;  // step offset within the drawn batch, batch parity
   for (int step = 0; step < mixing; ++step) {
     if (t == 0) {
       ++batch;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        c0[r] = 0.f;
-        c1[r] = 0.f;
-        // rounds past the batch's last slot are skipped and wide groups draw in their first warp
-        // (both uniform across a warp); within a round every lane evaluates its slot without
-        // branching (lanes past the last slot compute a value nobody reads), so the group's lanes
-        // stay convergent through the draws
-        if (r > 0 && r * GD >= S * J) continue;
-        if (G > 32 && gl >= 32) continue;
-        const int job = jq[r];
-        const int word = 2 * job;
+      // wide groups draw in their first warp (uniform across a warp); every drawing lane
+      // evaluates its slot without branching (lanes past the batch's last slot compute values
+      // nobody reads), so the group's lanes stay convergent through the draws
+      if (G <= 32 || gl < 32) {
         uint32_t w[4];
-        philox4x32_10((uint32_t)(step + tq[r]), chain, stream, (uint32_t)(word >> 2), k0, k1, w);
-        const uint32_t wa = (word & 2) ? w[2] : w[0];
-        const uint32_t wb = (word & 2) ? w[3] : w[1];
-        const float u = u01_open0(wa);
-        const float rad = __fsqrt_rn(__fmul_rn(-2.0f, log_unit(u)));
-        float sn, cs;
-        sincos_2pi(u01_open1(wb), &sn, &cs);
-        const bool gauss = job < npairs;
-        c0[r] = gauss ? __fmul_rn(rad, cs) : u;
-        c1[r] = gauss ? __fmul_rn(rad, sn) : 0.f;
+        philox4x32_10((uint32_t)(step + tq), chain, stream, (uint32_t)bq, k0, k1, w);
+        const float ua = u01_open0(w[0]), ub = u01_open0(w[2]);
+        const float rada = __fsqrt_rn(__fmul_rn(-2.0f, log_unit(ua)));
+        const float radb = __fsqrt_rn(__fmul_rn(-2.0f, log_unit(ub)));
+        float sna, csa, snb, csb;
+        sincos_2pi(u01_open1(w[1]), &sna, &csa);
+        sincos_2pi(u01_open1(w[3]), &snb, &csb);
+        const bool ga = 2 * bq < npairs, gb = 2 * bq + 1 < npairs;
+        c0a = ga ? __fmul_rn(rada, csa) : ua;
+        c1a = __fmul_rn(rada, sna);
+        c0b = gb ? __fmul_rn(radb, csb) : ub;
+        c1b = __fmul_rn(radb, snb);
       }
       if constexpr (G > 32) {
-        if (gl < S * J) {  // the first warp's lanes (S J <= 32)
-          float* db = gs->dir[batch & 1][tq[0]];
-          if (jq[0] < npairs) {
-            db[2 * jq[0]] = c0[0];
-            db[2 * jq[0] + 1] = c1[0];
+        if (gl < S * JB) {  // the first warp's lanes (S JB <= 32)
+          float* db = gs->dir[batch & 1][tq];
+          if (2 * bq < npairs) {
+            db[4 * bq] = c0a;
+            db[4 * bq + 1] = c1a;
           } else {
-            db[16] = c0[0];
+            db[16] = c0a;
+          }
+          if (2 * bq + 1 < npairs) {
+            db[4 * bq + 2] = c0b;
+            db[4 * bq + 3] = c1b;
+          } else if (2 * bq + 1 == npairs) {
+            db[16] = c0b;
           }
         }
       }
     }
-    const int base = t * J;  // lane of this step's Gaussian pair 0
-    uint64_t dd[MAXD];       // (dir_k, dir_k)
+    const int base = t * JB;  // lane of this step's block 0
+    uint64_t dd[MAXD];        // (dir_k, dir_k)
     float ut;
     if constexpr (G <= 32) {
 #pragma unroll
       for (int k = 0; k < MAXD; ++k) {
-        const float dk = __shfl_sync(0xffffffffu, (k & 1) ? c1[0] : c0[0], base + (k >> 1), G);
+        // coordinate k: pair k >> 1 = block k >> 2, half (k >> 1) & 1, cosine or sine k & 1
+        const float v = ((k >> 1) & 1) ? ((k & 1) ? c1b : c0b) : ((k & 1) ? c1a : c0a);
+        const float dk = __shfl_sync(0xffffffffu, v, base + (k >> 2), G);
         dd[k] = f2_pack(dk, dk);
       }
-      const int q = base + npairs;  // the theta uniform's slot
-      float utv = c0[0];
-#pragma unroll
-      for (int r = 1; r < R; ++r)
-        if (q / G == r) utv = c0[r];
-      ut = __shfl_sync(0xffffffffu, utv, q % G, G);
+      const float utv = (npairs & 1) ? c0b : c0a;  // the theta uniform: block npairs / 2, half npairs & 1
+      ut = __shfl_sync(0xffffffffu, utv, base + (npairs >> 1), G);
     } else {
       const float* db = gs->dir[batch & 1][t];
       if (t == 0) group_bar(bar_id, G);  // the batch's draws are in scratch
@@ -331,16 +325,17 @@ __device__ __forceinline__ bool run_chain_pairs(const float* __restrict__ rows, 
       }
     }
     if (isinf(tmax) || isinf(tmin) || tmax < tmin) ok = false;
-    // this step's direction at the position coordinates the lane holds (coordinate k is half k & 1
-    // of Gaussian pair k >> 1: lane base + (k >> 1), round 0)
+    // this step's direction at the position coordinates the lane holds (coordinate k: block
+    // k >> 2 on lane base + (k >> 2), half (k >> 1) & 1, cosine or sine k & 1)
     float dkl[XL];
 #pragma unroll
     for (int r = 0; r < XL; ++r) {
       const int k = min(gl + G * r, MAXD - 1);
       if constexpr (G <= 32) {
-        const float v0 = __shfl_sync(0xffffffffu, c0[0], base + (k >> 1), G);
-        const float v1 = __shfl_sync(0xffffffffu, c1[0], base + (k >> 1), G);
-        dkl[r] = (k & 1) ? v1 : v0;
+        const int src = base + (k >> 2);
+        const float va0 = __shfl_sync(0xffffffffu, c0a, src, G), va1 = __shfl_sync(0xffffffffu, c1a, src, G);
+        const float vb0 = __shfl_sync(0xffffffffu, c0b, src, G), vb1 = __shfl_sync(0xffffffffu, c1b, src, G);
+        dkl[r] = ((k >> 1) & 1) ? ((k & 1) ? vb1 : vb0) : ((k & 1) ? va1 : va0);
       } else {
         dkl[r] = gs->dir[batch & 1][t][k];
       }
