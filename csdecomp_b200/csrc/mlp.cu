@@ -14,6 +14,7 @@
 //     the ReLU mask and store bf16 row-major and transposed.
 // CUDA-core kernels: the output-layer gradient, bias reductions, Adam.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -155,7 +156,7 @@ template <int NT>
 csd_status_t launch_gemm(const GemmArgs& g, int groups, cudaStream_t st) {
   CSD_CHECK(g.lda % 8 == 0 && g.ldb % 8 == 0 && g.K % 8 == 0 && g.a_group % 8 == 0 && g.b_group % 8 == 0,
             CSD_ERR_INVALID, "GEMM operands need 16-byte aligned rows");
-  static bool attr[64] = {};
+  static std::atomic<bool> attr[64] = {};  // per device: limit raised (any thread)
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 64 || !attr[dev]) {
@@ -197,7 +198,7 @@ __global__ void __launch_bounds__(kThreads) mlp_forward_kernel(FwdArgs a) {
 }
 
 csd_status_t launch_forward(const FwdArgs& a, int groups, int max_rows, cudaStream_t st) {
-  static bool attr[64] = {};
+  static std::atomic<bool> attr[64] = {};  // per device: limit raised (any thread)
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 64 || !attr[dev]) {

@@ -10,6 +10,7 @@
 // registers (the reference keeps two float[4000] arrays per thread in local
 // memory) and draws from the counter-based stream of csd_rng.cuh.
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 
 #include "csd_internal.h"
@@ -91,7 +92,7 @@ csd_status_t launch_sample_region(const float* rows, const int* num_faces_dev, i
                                   int mixing, uint64_t seed, uint32_t stream, float* out, cudaStream_t st) {
   if (S <= 0) return CSD_OK;
   CSD_CHECK(dim >= 1 && dim <= kMaxDim, CSD_ERR_DIMENSION, "dimension must be in [1, 16]");
-  static bool attr_set[64] = {};
+  static std::atomic<bool> attr_set[64] = {};  // per device: limit raised (any thread)
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 64 || !attr_set[dev]) {
