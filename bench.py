@@ -312,7 +312,7 @@ def roofline_point_check(csd, scene, torch, dev, flush):
 # DRAM bytes per launch from ncu captures (profiles/): the full-sweep checker
 # launch (2^20 configurations) and the sampler's launches of one 256-slot step.
 CHECKER_TRAFFIC_BYTES = 29.5e6
-SAMPLER_TRAFFIC_BYTES_PER_STEP = 273.6e6   # 147 launches, 134.6 MB read + 139.0 MB written
+SAMPLER_TRAFFIC_BYTES_PER_STEP = 216.4e6   # 147 launches, 156.5 MB read + 60.0 MB written
 
 
 def check_workloads(csd, torch, dev, flush, cpu: bool):
