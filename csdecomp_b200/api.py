@@ -611,7 +611,7 @@ class BatchedEdgeInflator:
     SAMPLE_FLOP_RULE = ("(2 d + 4) F per chain and mixing step: a . dir (2 d), the carried-slack update (2) and the "
                         "two theta-bound compares (2) per face, FMA = 2, division not counted; summed over the slots "
                         "and iterations of the step")
-    CHECK_ITEM_CAPS = (32, 128, 512)
+    CHECK_ITEM_CAPS = (8, 16, 32, 128, 512)
 
     def __init__(self, plants: Sequence[MinimalPlant], options: EizoOptions, max_slots: int,
                  face_capacity: int = MAX_NUM_FACES, autotune_iterations: int = 4):

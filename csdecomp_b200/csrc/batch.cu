@@ -694,7 +694,7 @@ constexpr int kMinKP = 8;
 static_assert(2 * 256 * kMinKP >= kMaxRegionFaces, "every variant samples the largest region");
 constexpr int kNumSampleVariants = (int)(sizeof(kSampleVariants) / sizeof(kSampleVariants[0]));
 // Largest check work item (configurations) the autotuner chooses from.
-constexpr int kCheckItemCaps[] = {32, 128, 512};
+constexpr int kCheckItemCaps[] = {8, 16, 32, 128, 512};
 constexpr int kNumCheckVariants = (int)(sizeof(kCheckItemCaps) / sizeof(kCheckItemCaps[0]));
 // profiled stages: sample, score, sort, check, compact, bisect, faces, step
 constexpr int kStages = 8;
@@ -711,7 +711,7 @@ struct csd_batch_s {
   int static_floats = 0;
   size_t check_smem = 0;
   int check_grid = 0, bisect_grid = 0;
-  int cfg_max = 128, part_max = 64;
+  int cfg_max = 128, part_max = 8;  // bisection: one particle per warp per item (balance)
   int sample_variant = 0;     // tuned (or set) variant
   int large_variant = 1;      // variant chosen once a slot's faces exceeded the tuned variant's staging
   int run_variant = 0;        // variant of the current iterations

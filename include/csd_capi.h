@@ -314,11 +314,11 @@ csd_status_t csd_batch_stage_ms(csd_batch_t h, float* stage_ms /* [8] */);
 /* Autotuner: during the first `iterations` iterations of the next
  * csd_batch_inflate, every sampler variant (face pairs a lane holds at most x
  * resident blocks per SM: [8x1, 8x2, 8x3, 16x1, 16x2]) and every check
- * work-item cap ([32, 128, 512] configurations) is timed on that iteration's
+ * work-item cap ([8, 16, 32, 128, 512] configurations) is timed on that iteration's
  * own inputs; the fastest of each is kept for the graph and later calls. All
  * variants give identical samples. csd_batch_tuning reports the choice and
- * the summed time of each variant (variant_ms: 5 sampler entries, then 3 check
- * entries; *num_variants = 8). */
+ * the summed time of each variant (variant_ms: 5 sampler entries, then 5 check
+ * entries; *num_variants = 10). */
 csd_status_t csd_batch_autotune(csd_batch_t h, int32_t iterations);
 /* Surrogate-guided checking (mlp: one net per plant of the batch, same
  * dimensions; NULL turns it off). Each iteration then scores every sample
