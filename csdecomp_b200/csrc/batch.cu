@@ -711,7 +711,7 @@ struct csd_batch_s {
   int static_floats = 0;
   size_t check_smem = 0;
   int check_grid = 0, bisect_grid = 0;
-  int cfg_max = 128, part_max = 8;  // bisection: one particle per warp per item (balance)
+  int cfg_max = 128, part_max = 8;  // bisection: one particle per warp per item (every block busy)
   int sample_variant = 0;     // tuned (or set) variant
   int large_variant = 1;      // variant chosen once a slot's faces exceeded the tuned variant's staging
   int run_variant = 0;        // variant of the current iterations
